@@ -1,0 +1,309 @@
+"""Benchmark: DG residual + VJP DOF-updates/s on the 3D compressible-Euler workload.
+
+Workload (one "step"): the HLLC Euler operator on a periodic 32^3 hex grid,
+DG degree k=3 (Np=20 per variable, 5 variables, 3,276,800 DOFs), quadrature
+order 7 (4^3 volume / 4^2 face nodes), seeded synthetic state (see
+bosss_b200/problems.py). A step evaluates the residual R(U) and the adjoint
+product J(U)^T W at the same state; DOF-updates per step = 2 x 3,276,800.
+
+* ``value``: device-resident throughput (inputs in HBM), CUDA events on the
+  launching stream around each step; L2 (126 MB) is flushed between steps by
+  writing a 512 MB buffer outside the timed events (the working set, 105 MB,
+  would otherwise stay L2-resident).
+* ``e2e``: the same steps through the host-buffer C-ABI entry points
+  (bosss_b200_evaluate / bosss_b200_vjp) from pinned host memory: every call copies
+  its inputs host->device and its result device->host inside the timed region.
+* ``roofline``: the residual kernel (the dominant launch) -- algorithmic bytes
+  (8 B x (inputs + outputs)) over its CUDA-event duration, against the measured HBM
+  copy bandwidth; the FP64 pipe figure is reported beside it (nominal peak).
+* ``cpu_baseline``: the CPU FP64 oracle (a C++/OpenMP restatement of the reference
+  evaluator; the reference's .NET code cannot run here) on the full workload:
+  residual + exact JVP (the reference has no VJP entry point; its adjoint needs the
+  assembled Jacobian).
+
+N > 1 GPUs: every rank evaluates its own independent instance (weak scaling, no
+data-path collective); time = max over ranks.
+
+``--impl reference`` times the CPU oracle alone on the host cores (rank 0).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DOF_PER_STEP_FACTOR = 2   # residual + VJP
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=32)
+    ap.add_argument("--k", type=int, default=3)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_json(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % os.getpid())
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(args):
+    """CPU oracle (C++ FP64 restatement of the reference evaluator), all host threads."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from bosss_b200 import problems as P
+    from oracle import oracle as orc
+    pr = P.euler3d(n=args.n, k=args.k, seed=2000)
+    opd, gd = pr.descs()
+    cores = orc.threads(os.cpu_count() or 1)
+    V = np.random.default_rng(9).uniform(-1, 1, pr.n_dofs)
+    for _ in range(max(args.warmup, 1) if args.warmup else 0):
+        orc.evaluate(opd, gd, pr.U)
+        orc.jvp(opd, gd, pr.U, V)
+    t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        orc.evaluate(opd, gd, pr.U)
+        orc.jvp(opd, gd, pr.U, V)
+        t.append(time.perf_counter() - t0)
+    total = float(np.sum(t))
+    v = DOF_PER_STEP_FACTOR * pr.n_dofs * args.steps / total
+    line = {
+        "impl": "reference", "metric": "dg_residual_vjp_dof_updates_per_s", "value": v, "unit": "DOF/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": pr.config["workload"] + "_residual+vjp", "dofs": pr.n_dofs},
+        "cpu_baseline": {"value": v, "unit": "DOF/s", "cores": cores, "kind": "port",
+                         "sample": "full workload per step: oracle residual + exact JVP (dual numbers), "
+                                   "OpenMP over %d host threads" % cores},
+        "e2e": {"value": v, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(pr):
+    """Bounded CPU sample: one residual + one JVP of the full workload on all host cores."""
+    from oracle import oracle as orc
+    opd, gd = pr.descs()
+    cores = orc.threads(os.cpu_count() or 1)
+    V = np.random.default_rng(9).uniform(-1, 1, pr.n_dofs)
+    orc.evaluate(opd, gd, pr.U)
+    reps, t = 0, 0.0
+    while reps < 3 and t < 20.0:
+        t0 = time.perf_counter()
+        orc.evaluate(opd, gd, pr.U)
+        orc.jvp(opd, gd, pr.U, V)
+        t += time.perf_counter() - t0
+        reps += 1
+    return {"value": DOF_PER_STEP_FACTOR * pr.n_dofs * reps / t, "unit": "DOF/s", "cores": cores, "kind": "port",
+            "sample": "%d x (residual + exact JVP) of the full %s workload, C++ FP64 oracle, OpenMP %d threads"
+                      % (reps, pr.config["workload"], cores)}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_env()
+    import torch
+    import torch.distributed as dist
+    import ctypes
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from bosss_b200 import _capi as C
+    from bosss_b200 import problems as P
+
+    pr = P.euler3d(n=args.n, k=args.k, seed=2000 + rank)
+    ev = pr.evaluator(device=local)
+    L = C.lib()
+    dev = torch.device("cuda", local)
+    n = pr.n_dofs
+    U = torch.from_numpy(pr.U).to(dev)
+    W = torch.from_numpy(np.random.default_rng(77 + rank).uniform(-1, 1, n)).to(dev)
+    R = torch.zeros(n, dtype=torch.float64, device=dev)
+    G = torch.zeros(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    h = ev.handle
+
+    def step():
+        C.check(L.bosss_b200_evaluate_device(h, 1.0, 0.0, C.ptr(U), C.ptr(R), 0.0, sptr))
+        C.check(L.bosss_b200_vjp_device(h, C.ptr(U), C.ptr(W), C.ptr(G), 0.0, sptr))
+
+    launches_per_step = 2
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev_m = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.fill_(float(i))           # evict L2 outside the timed events
+        ev_s[i].record(stream)
+        C.check(L.bosss_b200_evaluate_device(h, 1.0, 0.0, C.ptr(U), C.ptr(R), 0.0, sptr))
+        ev_m[i].record(stream)
+        C.check(L.bosss_b200_vjp_device(h, C.ptr(U), C.ptr(W), C.ptr(G), 0.0, sptr))
+        ev_e[i].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_res = [ev_s[i].elapsed_time(ev_m[i]) for i in range(args.steps)]
+    t_vjp = [ev_m[i].elapsed_time(ev_e[i]) for i in range(args.steps)]
+    total_ms = float(np.sum(t_res) + np.sum(t_vjp))
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * DOF_PER_STEP_FACTOR * n * args.steps / (total_ms * 1e-3)
+
+    # ---- end to end through the host-buffer C-ABI (pinned host memory)
+    Uh = torch.from_numpy(pr.U.copy()).pin_memory()
+    Wh = torch.from_numpy(W.cpu().numpy()).pin_memory()
+    Rh = torch.zeros(n, dtype=torch.float64).pin_memory()
+    Gh = torch.zeros(n, dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        C.check(L.bosss_b200_evaluate(h, 1.0, 0.0, C.ptr(Uh), C.ptr(Rh), 0.0))
+        C.check(L.bosss_b200_vjp(h, C.ptr(Uh), C.ptr(Wh), C.ptr(Gh), 0.0))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        C.check(L.bosss_b200_evaluate(h, 1.0, 0.0, C.ptr(Uh), C.ptr(Rh), 0.0))
+        C.check(L.bosss_b200_vjp(h, C.ptr(Uh), C.ptr(Wh), C.ptr(Gh), 0.0))
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * DOF_PER_STEP_FACTOR * n * args.steps / e2e_s
+    # residual: U in, R out; vjp: U and W in, result out
+    h2d = 8 * (n + 2 * n)
+    d2h = 8 * (n + n)
+    # the host-buffer path must agree with the device-resident one
+    assert np.allclose(Rh.numpy(), R.cpu().numpy(), rtol=0, atol=0)
+
+    # ---- roofline of the residual kernel
+    peaks = load_json(os.path.join(ROOT, "MEASURED_PEAKS.json"))
+    hbm_peak = peaks["hbm_gbs"] if peaks else 6650.0
+    t_r = float(np.mean(t_res)) * 1e-3
+    bytes_res = 8.0 * (n + n)
+    achieved = bytes_res / t_r / 1e9
+    prof = load_json(os.path.join(ROOT, "profiles", "traffic.json")) or {}
+    traffic = prof.get("euler3d_residual_bytes_per_launch")
+    flops = load_json(os.path.join(ROOT, "profiles", "flops.json")) or {}
+    fp64_flops = flops.get("euler3d_residual_fp64_flops_per_launch")
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": "dg_residual_vjp_dof_updates_per_s", "value": value, "unit": "DOF/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": pr.config["workload"] + "_residual+vjp", "dofs": n, "cells": pr.grid.NoOfCells,
+                       "k": args.k, "quad_nodes_1d": ev.quad_nodes_1d, "precision": "fp64",
+                       "l2": "flushed between steps (512 MB write outside the timed events)",
+                       "parallelism": "independent instance per rank" if world > 1 else "single GPU"},
+            "ms_residual": float(np.mean(t_res)), "ms_vjp": float(np.mean(t_vjp)),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": traffic,
+                         "kernel": "dg_cell_kernel<PhysEuler<3>,3,4,RES>",
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
+            "fp64": {"flops_per_launch": fp64_flops,
+                     "achieved_tflops": (fp64_flops / t_r / 1e12) if fp64_flops else None,
+                     "nominal_peak_tflops": 37.0},
+            "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk,
+        }
+        if world == 1:
+            line["cpu_baseline"] = cpu_baseline_sample(pr)
+        print(json.dumps(line), flush=True)
+    ev.Dispose()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

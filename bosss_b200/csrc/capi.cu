@@ -1,0 +1,696 @@
+// capi.cu -- implementation of the C-ABI declared in include/bosss_b200.h.
+//
+// create() is the device-side counterpart of DifferentialOperator.GetEvaluatorEx
+// (DifferentialOperator.cs:1013-1033): it checks the committed operator, maps each
+// registered equation component to a device functor (no CPU fallback: an unknown
+// component is an error, as the reference throws NotSupportedException for
+// unsupported evaluator configurations), evaluates the quadrature-order function
+// (QuadOrderFunc.cs) and picks the Gauss rule like RefElement.GetQuadratureRule
+// (RefElement.cs:844-874), tabulates the 1D basis once and binds the kernel instance.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/bosss_b200.h"
+#include "dg_kernel.cuh"
+#include "dg_registry.h"
+
+namespace bosss {
+
+std::map<KernelKey, KernelEntry>& kernel_registry() {
+    static std::map<KernelKey, KernelEntry> r;
+    return r;
+}
+
+static void ensure_registered() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        register_scalar2();
+        register_scalar3();
+        register_euler2();
+        register_euler3();
+    });
+}
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(call)                                                                            \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(BOSSS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+// ------------------------------------------------------------------ host tables
+// Gauss-Legendre rule with n nodes (Newton iteration on P_n in long double), ascending.
+static void gauss_rule(int n, double* x, double* w) {
+    const long double PI = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i < n; ++i) {
+        long double z = std::cos(PI * (i + 0.75L) / (n + 0.5L)), dp = 1.0L;
+        for (int it = 0; it < 60; ++it) {
+            long double p0 = 1.0L, p1 = z;
+            for (int m = 1; m < n; ++m) {
+                long double p2 = ((2 * m + 1) * z * p1 - m * p0) / (m + 1);
+                p0 = p1;
+                p1 = p2;
+            }
+            long double pn = (n == 1) ? z : p1, pm = (n == 1) ? 1.0L : p0;
+            dp = n * (z * pn - pm) / (z * z - 1.0L);
+            long double dz = pn / dp;
+            z -= dz;
+            if (std::fabs((double)dz) < 1e-19) {
+                // recompute the derivative at the converged node
+                p0 = 1.0L;
+                p1 = z;
+                for (int m = 1; m < n; ++m) {
+                    long double p2 = ((2 * m + 1) * z * p1 - m * p0) / (m + 1);
+                    p0 = p1;
+                    p1 = p2;
+                }
+                pn = (n == 1) ? z : p1;
+                pm = (n == 1) ? 1.0L : p0;
+                dp = n * (z * pn - pm) / (z * z - 1.0L);
+                break;
+            }
+        }
+        x[n - 1 - i] = (double)z;
+        w[n - 1 - i] = (double)(2.0L / ((1.0L - z * z) * dp * dp));
+    }
+    if (n % 2 == 1) x[n / 2] = 0.0;
+}
+
+// normalised Legendre L_a(x) = sqrt((2a+1)/2) P_a(x) and derivative, a = 0..K
+static void legendre(int K, long double x, long double* L, long double* dL) {
+    long double P[KMAX + 2], dP[KMAX + 2];
+    P[0] = 1.0L;
+    dP[0] = 0.0L;
+    if (K >= 1) {
+        P[1] = x;
+        dP[1] = 1.0L;
+    }
+    for (int m = 1; m < K; ++m) {
+        P[m + 1] = ((2 * m + 1) * x * P[m] - m * P[m - 1]) / (m + 1);
+        dP[m + 1] = dP[m - 1] + (2 * m + 1) * P[m];
+    }
+    for (int a = 0; a <= K; ++a) {
+        long double s = std::sqrt((2.0L * a + 1.0L) / 2.0L);
+        L[a] = s * P[a];
+        dL[a] = s * dP[a];
+    }
+}
+
+static void build_tables(int K, int Q, Tables1D& t) {
+    std::memset(&t, 0, sizeof(t));
+    double x[QMAX], w[QMAX];
+    gauss_rule(Q, x, w);
+    for (int q = 0; q < Q; ++q) {
+        long double L[KMAX + 1], dL[KMAX + 1];
+        legendre(K, x[q], L, dL);
+        for (int a = 0; a <= K; ++a) {
+            t.A[q][a] = (double)L[a];
+            t.dA[q][a] = (double)dL[a];
+        }
+        t.w[q] = w[q];
+        t.xq[q] = x[q];
+    }
+    for (int s = 0; s < 2; ++s) {
+        long double L[KMAX + 1], dL[KMAX + 1];
+        legendre(K, s ? 1.0L : -1.0L, L, dL);
+        for (int a = 0; a <= K; ++a) {
+            t.e[s][a] = (double)L[a];
+            t.de[s][a] = (double)dL[a];
+        }
+    }
+}
+
+// QuadOrderFunc.cs
+static int quad_order(const bosss_op_desc& op) {
+    int maxDom = 0, maxCod = 0;
+    for (int i = 0; i < op.n_domain; ++i) maxDom = std::max(maxDom, op.domain_degree[i]);
+    for (int i = 0; i < op.n_codomain; ++i) maxCod = std::max(maxCod, op.codomain_degree[i]);
+    switch (op.quad_kind) {
+        case BOSSS_QUAD_FIXED: return op.quad_param;
+        case BOSSS_QUAD_LINEAR: return maxDom + maxCod;
+        case BOSSS_QUAD_NONLINEAR: return maxDom * op.quad_param + maxCod;
+        case BOSSS_QUAD_MAXDEG_TIMES_TWO: return 2 * std::max(maxDom, maxCod);
+        case BOSSS_QUAD_SUM_OF_MAX_DEGREES: {
+            int o = maxDom * op.quad_param + maxCod;
+            return (o % 2) ? o + 1 : o;
+        }
+        default: return -1;
+    }
+}
+
+}  // namespace bosss
+
+using namespace bosss;
+
+struct bosss_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int phys = 0, D = 0, K = 0, Q = 0;
+    EvalArgs base{};
+    int64_t ndom = 0, ncod = 0;
+    KernelEntry kern[3]{};
+    bool check_nan = false;
+    // device staging for the host-buffer entry points
+    double* dU = nullptr;
+    double* dV = nullptr;
+    double* dOut = nullptr;
+    int* dFlag = nullptr;
+};
+
+struct bosss_bsr {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t nbr = 0, nbc = 0, nnzb = 0;
+    int br = 0, bc = 0;
+    int64_t* d_rowptr = nullptr;
+    int32_t* d_colidx = nullptr;
+    double* d_vals = nullptr;   // blocks stored column-major (coalesced row-lane loads)
+    double* dx = nullptr;
+    double* dy = nullptr;
+};
+
+namespace bosss {
+
+static int classify(const bosss_op_desc& op, int D, int& phys, PhysParams& ph) {
+    std::memset(&ph, 0, sizeof(ph));
+    if (op.n_components < 1 || op.n_components > BOSSS_MAX_COMPONENTS)
+        return fail(BOSSS_ERR_BAD_ARG, "operator has no equation components");
+    bool euler = false;
+    for (int c = 0; c < op.n_components; ++c) {
+        int t = op.components[c].type;
+        if (t == BOSSS_COMP_HLLC_DENSITY_FLUX || t == BOSSS_COMP_HLLC_MOMENTUM_FLUX || t == BOSSS_COMP_HLLC_ENERGY_FLUX)
+            euler = true;
+        else if (t != BOSSS_COMP_SCALAR_TRANSPORT_FLUX && t != BOSSS_COMP_SIP_LAPLACE && t != BOSSS_COMP_CONSTANT_SOURCE)
+            return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT,
+                        "equation component type " + std::to_string(t) + " has no device functor");
+    }
+    if (euler) {
+        const int NV = D + 2;
+        if (op.n_domain != NV || op.n_codomain != NV)
+            return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "HLLC operator needs D+2 domain and codomain variables");
+        std::vector<int> seen(NV, 0);
+        double gamma = 0, mach = 0;
+        for (int c = 0; c < op.n_components; ++c) {
+            const auto& cp = op.components[c];
+            if (cp.type != BOSSS_COMP_HLLC_DENSITY_FLUX && cp.type != BOSSS_COMP_HLLC_MOMENTUM_FLUX &&
+                cp.type != BOSSS_COMP_HLLC_ENERGY_FLUX)
+                return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "HLLC fluxes cannot be mixed with other components");
+            if (cp.n_args != NV) return fail(BOSSS_ERR_BAD_ARG, "HLLC flux needs D+2 arguments");
+            for (int a = 0; a < NV; ++a)
+                if (cp.args[a] != a)
+                    return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "HLLC arguments must be (rho, m_0..m_{D-1}, rhoE)");
+            int cod = (cp.type == BOSSS_COMP_HLLC_DENSITY_FLUX) ? 0
+                      : (cp.type == BOSSS_COMP_HLLC_ENERGY_FLUX) ? D + 1
+                                                                 : (int)cp.params[2] + 1;
+            if (cp.type == BOSSS_COMP_HLLC_MOMENTUM_FLUX && (cp.params[2] < 0 || cp.params[2] >= D))
+                return fail(BOSSS_ERR_BAD_ARG, "HLLC momentum component out of range");
+            if (cp.codomain != cod)
+                return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "HLLC flux registered on an unexpected codomain variable");
+            if (seen[cod]++) return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "duplicate HLLC flux");
+            if (c == 0) {
+                gamma = cp.params[0];
+                mach = cp.params[1];
+            } else if (gamma != cp.params[0] || mach != cp.params[1]) {
+                return fail(BOSSS_ERR_BAD_ARG, "HLLC fluxes with different material parameters");
+            }
+        }
+        for (int v = 0; v < NV; ++v)
+            if (!seen[v]) return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "incomplete HLLC flux set");
+        if (!(gamma > 1.0) || !(mach > 0.0)) return fail(BOSSS_ERR_BAD_ARG, "bad gamma/Mach");
+        ph.gamma = gamma;
+        ph.mach = mach;
+        phys = PHYS_EULER;
+        return 0;
+    }
+    if (op.n_domain != 1 || op.n_codomain != 1)
+        return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "scalar components need one domain and one codomain variable");
+    int ntr = 0, nsip = 0, nsrc = 0;
+    for (int c = 0; c < op.n_components; ++c) {
+        const auto& cp = op.components[c];
+        if (cp.codomain != 0) return fail(BOSSS_ERR_BAD_ARG, "bad codomain index");
+        if (cp.type != BOSSS_COMP_CONSTANT_SOURCE && (cp.n_args != 1 || cp.args[0] != 0))
+            return fail(BOSSS_ERR_BAD_ARG, "scalar component must take the domain variable as its argument");
+        if (cp.type == BOSSS_COMP_SCALAR_TRANSPORT_FLUX) {
+            ++ntr;
+            ph.has_transport = 1;
+            for (int d = 0; d < 3; ++d) ph.vel[d] = d < D ? cp.params[d] : 0.0;
+        } else if (cp.type == BOSSS_COMP_SIP_LAPLACE) {
+            ++nsip;
+            ph.has_sip = 1;
+            ph.pen = cp.params[0];   // multiplied by the degree factor in create()
+            ph.nu0 = cp.params[1];
+            ph.nu2 = cp.params[2];
+            ph.dirichlet = (cp.params[3] == 0.0) ? 1 : 0;
+            ph.g0 = cp.params[4];
+            for (int d = 0; d < 3; ++d) {
+                ph.g1[d] = cp.params[5 + d];
+                ph.g2[d] = cp.params[8 + d];
+            }
+        } else {
+            ++nsrc;
+            ph.has_source = 1;
+            ph.src = cp.params[0];
+        }
+    }
+    if (ntr > 1 || nsip > 1 || nsrc > 1)
+        return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "at most one transport, one SIP and one source component");
+    phys = (nsip || nsrc) ? PHYS_SIP : PHYS_TRANSPORT;
+    return 0;
+}
+
+static int ensure_staging(bosss_handle* h) {
+    if (h->dU) return 0;
+    const int64_t n1 = std::max(h->ndom, h->ncod);
+    CUDA_TRY(cudaMalloc(&h->dU, sizeof(double) * std::max<int64_t>(h->ndom, 1)));
+    CUDA_TRY(cudaMalloc(&h->dV, sizeof(double) * std::max<int64_t>(n1, 1)));
+    CUDA_TRY(cudaMalloc(&h->dOut, sizeof(double) * std::max<int64_t>(n1, 1)));
+    return 0;
+}
+
+__global__ void nan_scan_kernel(const double* x, long long n, int* flag) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (!isfinite(x[i])) {
+            atomicExch(flag, 1);
+            return;
+        }
+}
+
+static int run_mode(bosss_handle* h, int mode, double alpha, double beta, const double* U, const double* V,
+                    double* out, double time, cudaStream_t s) {
+    EvalArgs a = h->base;
+    a.U = U;
+    a.V = V;
+    a.out = out;
+    a.alpha = alpha;
+    a.beta = beta;
+    a.time = time;
+    CUDA_TRY(cudaSetDevice(h->device));
+    if (h->base.g.J > 0) CUDA_TRY(h->kern[mode].launch(a, s));
+    return 0;
+}
+
+static int check_nan(bosss_handle* h, const double* out, int64_t n, cudaStream_t s) {
+    if (!h->check_nan) return 0;
+    if (!h->dFlag) CUDA_TRY(cudaMalloc(&h->dFlag, sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(h->dFlag, 0, sizeof(int), s));
+    nan_scan_kernel<<<592, 256, 0, s>>>(out, (long long)n, h->dFlag);
+    CUDA_TRY(cudaGetLastError());
+    int flag = 0;
+    CUDA_TRY(cudaMemcpyAsync(&flag, h->dFlag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (flag) return fail(BOSSS_ERR_NAN, "NaN or Inf in the operator output");
+    return 0;
+}
+
+// ------------------------------------------------------------------ block-sparse SpMV
+// One thread per scalar row; blocks are stored column-major so that the threads of a
+// block row read consecutive addresses for each block column.
+__global__ void bsr_spmv_kernel(long long nbr, int br, int bc, const long long* __restrict__ rowptr,
+                                const int* __restrict__ colidx, const double* __restrict__ vals,
+                                const double* __restrict__ x, double alpha, double beta, double* __restrict__ y) {
+    const long long nrows = nbr * br;
+    for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < nrows;
+         row += (long long)gridDim.x * blockDim.x) {
+        const long long i = row / br;
+        const int r = (int)(row - i * br);
+        double acc = 0.0;
+        for (long long b = rowptr[i]; b < rowptr[i + 1]; ++b) {
+            const double* blk = vals + b * (long long)br * bc;
+            const double* xb = x + (long long)colidx[b] * bc;
+            for (int c = 0; c < bc; ++c) acc += blk[(long long)c * br + r] * __ldg(xb + c);
+        }
+        y[row] = (beta == 0.0) ? alpha * acc : beta * y[row] + alpha * acc;
+    }
+}
+
+}  // namespace bosss
+
+extern "C" {
+
+int bosss_b200_version(int32_t* major, int32_t* minor, int32_t* patch) {
+    if (major) *major = BOSSS_B200_VERSION_MAJOR;
+    if (minor) *minor = BOSSS_B200_VERSION_MINOR;
+    if (patch) *patch = BOSSS_B200_VERSION_PATCH;
+    return BOSSS_OK;
+}
+
+int bosss_b200_last_error(char* buf, size_t len) {
+    if (!buf || len == 0) return BOSSS_ERR_BAD_ARG;
+    std::strncpy(buf, g_last_error.c_str(), len - 1);
+    buf[len - 1] = 0;
+    return BOSSS_OK;
+}
+
+int bosss_b200_device_count(int32_t* count) {
+    if (!count) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    *count = (e == cudaSuccess) ? n : 0;
+    if (e != cudaSuccess) cudaGetLastError();
+    return BOSSS_OK;
+}
+
+int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, const bosss_options* opt,
+                      bosss_handle** out) {
+    if (!op || !grid || !out) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    *out = nullptr;
+    const int D = grid->dim;
+    if (D != 2 && D != 3) return fail(BOSSS_ERR_BAD_ARG, "grid dimension must be 2 or 3");
+    long long J = 1;
+    for (int d = 0; d < D; ++d) {
+        if (grid->n[d] < 1) return fail(BOSSS_ERR_BAD_ARG, "grid needs at least one cell per direction");
+        if (!(grid->hi[d] > grid->lo[d])) return fail(BOSSS_ERR_BAD_ARG, "grid box has non-positive extent");
+        J *= grid->n[d];
+    }
+    if (J > 2000000000LL) return fail(BOSSS_ERR_BAD_ARG, "too many cells");
+    if (op->n_domain < 1 || op->n_domain > BOSSS_MAX_VARS || op->n_codomain < 1 || op->n_codomain > BOSSS_MAX_VARS)
+        return fail(BOSSS_ERR_BAD_ARG, "bad number of variables");
+    const int K = op->domain_degree[0];
+    for (int i = 0; i < op->n_domain; ++i)
+        if (op->domain_degree[i] != K) return fail(BOSSS_ERR_BAD_ARG, "device path needs one DG degree for all fields");
+    for (int i = 0; i < op->n_codomain; ++i)
+        if (op->codomain_degree[i] != K) return fail(BOSSS_ERR_BAD_ARG, "device path needs one DG degree for all fields");
+    if (K < 0 || K > KMAX) return fail(BOSSS_ERR_BAD_ARG, "DG degree outside 0..4");
+    int phys = 0;
+    PhysParams ph;
+    int rc = classify(*op, D, phys, ph);
+    if (rc) return rc;
+    if (phys == PHYS_EULER)
+        for (int d = 0; d < D; ++d)
+            if (!grid->periodic[d])
+                return fail(BOSSS_ERR_BAD_ARG, "HLLC fluxes need a boundary-condition map: only periodic grids");
+    if (phys == PHYS_SIP && ph.has_sip && K < 1)
+        return fail(BOSSS_ERR_BAD_ARG, "SIP needs DG degree >= 1 (IsValidDomainDegreeCombination)");
+    const int order = quad_order(*op);
+    if (order < 0) return fail(BOSSS_ERR_BAD_ARG, "bad quadrature-order function");
+    const int Q = std::max(1, (order + 2) / 2);   // smallest Gauss rule with 2Q-1 >= order
+    ensure_registered();
+    auto& reg = kernel_registry();
+    for (int m = 0; m < 3; ++m)
+        if (!reg.count(KernelKey(phys, D, K, Q, m)))
+            return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no device kernel for degree " + std::to_string(K) +
+                                                             " with " + std::to_string(Q) + " Gauss nodes");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(BOSSS_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    const int dev = opt ? opt->device : 0;
+    if (dev < 0 || dev >= ndev) return fail(BOSSS_ERR_BAD_ARG, "bad device ordinal");
+
+    bosss_handle* h = new bosss_handle();
+    h->device = dev;
+    h->phys = phys;
+    h->D = D;
+    h->K = K;
+    h->Q = Q;
+    h->check_nan = opt && opt->check_nan;
+    build_tables(K, Q, h->base.tab);
+    GridConst& g = h->base.g;
+    std::memset(&g, 0, sizeof(g));
+    g.D = D;
+    g.J = (int)J;
+    for (int d = 0; d < 3; ++d) {
+        g.n[d] = d < D ? grid->n[d] : 1;
+        g.periodic[d] = d < D ? (grid->periodic[d] ? 1 : 0) : 0;
+        g.lo[d] = d < D ? grid->lo[d] : 0.0;
+        g.h[d] = d < D ? (grid->hi[d] - grid->lo[d]) / grid->n[d] : 1.0;
+        g.twoh[d] = 2.0 / g.h[d];
+    }
+    if (grid->cell_order == BOSSS_CELLS_GLOBALID) {
+        g.stride[0] = 1;
+        g.stride[1] = g.n[0];
+        g.stride[2] = (long long)g.n[0] * g.n[1];
+    } else {
+        if (D == 2) {
+            g.stride[0] = g.n[1];
+            g.stride[1] = 1;
+            g.stride[2] = 0;
+        } else {
+            g.stride[0] = (long long)g.n[1] * g.n[2];
+            g.stride[1] = g.n[2];
+            g.stride[2] = 1;
+        }
+    }
+    g.detJ = 1.0;
+    for (int d = 0; d < D; ++d) g.detJ *= 0.5 * g.h[d];
+    g.scaling = 1.0 / std::sqrt(g.detJ);
+    for (int d = 0; d < D; ++d) {
+        double sg = 1.0;
+        for (int d2 = 0; d2 < D; ++d2)
+            if (d2 != d) sg *= 0.5 * g.h[d2];
+        g.faceSG[d] = sg;
+    }
+    if (ph.has_sip) {
+        // ipLaplace.cs CoefficientUpdate: max(triangle formula, (p+1)^2)
+        const double p = K;
+        ph.pen *= std::max((p + 1.0) * (p + D) / D, (p + 1.0) * (p + 1.0));
+    }
+    h->base.ph = ph;
+    const int NV = (phys == PHYS_EULER) ? D + 2 : 1;
+    h->ndom = (int64_t)J * NV * np_of(D, K);
+    h->ncod = h->ndom;
+    for (int m = 0; m < 3; ++m) h->kern[m] = reg[KernelKey(phys, D, K, Q, m)];
+    cudaError_t e = cudaSetDevice(dev);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete h;
+        return fail(BOSSS_ERR_CUDA, std::string("stream creation: ") + cudaGetErrorString(e));
+    }
+    *out = h;
+    return BOSSS_OK;
+}
+
+int bosss_b200_destroy(bosss_handle* h) {
+    if (!h) return BOSSS_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->dU);
+    cudaFree(h->dV);
+    cudaFree(h->dOut);
+    cudaFree(h->dFlag);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return BOSSS_OK;
+}
+
+int bosss_b200_get_sizes(const bosss_handle* h, int64_t* n_domain_dofs, int64_t* n_codomain_dofs,
+                         int32_t* quad_nodes_1d) {
+    if (!h) return fail(BOSSS_ERR_BAD_ARG, "null handle");
+    if (n_domain_dofs) *n_domain_dofs = h->ndom;
+    if (n_codomain_dofs) *n_codomain_dofs = h->ncod;
+    if (quad_nodes_1d) *quad_nodes_1d = h->Q;
+    return BOSSS_OK;
+}
+
+int bosss_b200_evaluate_device(bosss_handle* h, double alpha, double beta, const double* U_dev, double* out_dev,
+                               double time, void* stream) {
+    if (!h || !U_dev || !out_dev) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    int rc = run_mode(h, MODE_RES, alpha, beta, U_dev, nullptr, out_dev, time, s);
+    if (rc) return rc;
+    return check_nan(h, out_dev, h->ncod, s);
+}
+
+int bosss_b200_evaluate(bosss_handle* h, double alpha, double beta, const double* U, double* out, double time) {
+    if (!h || !U || !out) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    int rc = ensure_staging(h);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = h->stream;
+    CUDA_TRY(cudaMemcpyAsync(h->dU, U, sizeof(double) * h->ndom, cudaMemcpyHostToDevice, s));
+    if (beta != 0.0) CUDA_TRY(cudaMemcpyAsync(h->dOut, out, sizeof(double) * h->ncod, cudaMemcpyHostToDevice, s));
+    rc = run_mode(h, MODE_RES, alpha, beta, h->dU, nullptr, h->dOut, time, s);
+    if (rc) return rc;
+    rc = check_nan(h, h->dOut, h->ncod, s);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(out, h->dOut, sizeof(double) * h->ncod, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return BOSSS_OK;
+}
+
+int bosss_b200_jvp_device(bosss_handle* h, const double* U_dev, const double* V_dev, double* JV_dev, double time,
+                          void* stream) {
+    if (!h || !U_dev || !V_dev || !JV_dev) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    return run_mode(h, MODE_JVP, 1.0, 0.0, U_dev, V_dev, JV_dev, time, s);
+}
+
+int bosss_b200_vjp_device(bosss_handle* h, const double* U_dev, const double* W_dev, double* JTW_dev, double time,
+                          void* stream) {
+    if (!h || !U_dev || !W_dev || !JTW_dev) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    return run_mode(h, MODE_VJP, 1.0, 0.0, U_dev, W_dev, JTW_dev, time, s);
+}
+
+static int host_pair(bosss_handle* h, int mode, const double* U, const double* X, double* Y, double time) {
+    if (!h || !U || !X || !Y) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    int rc = ensure_staging(h);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = h->stream;
+    const int64_t nx = (mode == MODE_JVP) ? h->ndom : h->ncod;
+    const int64_t ny = (mode == MODE_JVP) ? h->ncod : h->ndom;
+    CUDA_TRY(cudaMemcpyAsync(h->dU, U, sizeof(double) * h->ndom, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(h->dV, X, sizeof(double) * nx, cudaMemcpyHostToDevice, s));
+    rc = run_mode(h, mode, 1.0, 0.0, h->dU, h->dV, h->dOut, time, s);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(Y, h->dOut, sizeof(double) * ny, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return BOSSS_OK;
+}
+
+int bosss_b200_jvp(bosss_handle* h, const double* U, const double* V, double* JV, double time) {
+    return host_pair(h, MODE_JVP, U, V, JV, time);
+}
+
+int bosss_b200_vjp(bosss_handle* h, const double* U, const double* W, double* JTW, double time) {
+    return host_pair(h, MODE_VJP, U, W, JTW, time);
+}
+
+int bosss_b200_synchronize(bosss_handle* h) {
+    if (!h) return fail(BOSSS_ERR_BAD_ARG, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BOSSS_OK;
+}
+
+// ---------------------------------------------------------------- block-sparse matrix
+int bosss_b200_bsr_create(int64_t n_block_rows, int64_t n_block_cols, int32_t row_block, int32_t col_block,
+                          const int64_t* row_ptr, const int32_t* col_idx, const double* values, int32_t device,
+                          bosss_bsr** out) {
+    if (!out || !row_ptr || n_block_rows < 0 || n_block_cols < 0 || row_block < 1 || col_block < 1)
+        return fail(BOSSS_ERR_BAD_ARG, "bad block-sparse matrix arguments");
+    *out = nullptr;
+    const int64_t nnzb = row_ptr[n_block_rows];
+    if (row_ptr[0] != 0 || nnzb < 0) return fail(BOSSS_ERR_BAD_ARG, "row_ptr must start at 0");
+    for (int64_t i = 0; i < n_block_rows; ++i)
+        if (row_ptr[i + 1] < row_ptr[i]) return fail(BOSSS_ERR_BAD_ARG, "row_ptr not monotone");
+    if (nnzb > 0 && (!col_idx || !values)) return fail(BOSSS_ERR_BAD_ARG, "missing col_idx/values");
+    for (int64_t b = 0; b < nnzb; ++b)
+        if (col_idx[b] < 0 || col_idx[b] >= n_block_cols) return fail(BOSSS_ERR_BAD_ARG, "column index out of range");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(BOSSS_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(BOSSS_ERR_BAD_ARG, "bad device ordinal");
+    bosss_bsr* A = new bosss_bsr();
+    A->device = device;
+    A->nbr = n_block_rows;
+    A->nbc = n_block_cols;
+    A->nnzb = nnzb;
+    A->br = row_block;
+    A->bc = col_block;
+    const size_t bs = (size_t)row_block * col_block;
+    std::vector<double> cm(std::max<size_t>(nnzb * bs, 1));
+    for (int64_t b = 0; b < nnzb; ++b)
+        for (int r = 0; r < row_block; ++r)
+            for (int c = 0; c < col_block; ++c) cm[b * bs + (size_t)c * row_block + r] = values[b * bs + (size_t)r * col_block + c];
+    auto cleanup = [&](cudaError_t e) {
+        bosss_b200_bsr_destroy(A);
+        return fail(BOSSS_ERR_CUDA, std::string("block-sparse upload: ") + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&A->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&A->d_rowptr, sizeof(int64_t) * (n_block_rows + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&A->d_colidx, sizeof(int32_t) * std::max<int64_t>(nnzb, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&A->d_vals, sizeof(double) * cm.size());
+    if (e == cudaSuccess) e = cudaMemcpy(A->d_rowptr, row_ptr, sizeof(int64_t) * (n_block_rows + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nnzb) e = cudaMemcpy(A->d_colidx, col_idx, sizeof(int32_t) * nnzb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(A->d_vals, cm.data(), sizeof(double) * cm.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cleanup(e);
+    *out = A;
+    return BOSSS_OK;
+}
+
+int bosss_b200_bsr_destroy(bosss_bsr* A) {
+    if (!A) return BOSSS_OK;
+    cudaSetDevice(A->device);
+    if (A->stream) cudaStreamSynchronize(A->stream);
+    cudaFree(A->d_rowptr);
+    cudaFree(A->d_colidx);
+    cudaFree(A->d_vals);
+    cudaFree(A->dx);
+    cudaFree(A->dy);
+    if (A->stream) cudaStreamDestroy(A->stream);
+    delete A;
+    return BOSSS_OK;
+}
+
+int bosss_b200_bsr_spmv_device(bosss_bsr* A, double alpha, const double* x_dev, double beta, double* y_dev,
+                               void* stream) {
+    if (!A || !x_dev || !y_dev) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(A->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : A->stream;
+    const long long nrows = A->nbr * A->br;
+    if (nrows == 0) return BOSSS_OK;
+    int grid = (int)std::min<long long>((nrows + 255) / 256, 148LL * 16);
+    bsr_spmv_kernel<<<grid, 256, 0, s>>>(A->nbr, A->br, A->bc, (const long long*)A->d_rowptr, A->d_colidx,
+                                          A->d_vals, x_dev, alpha, beta, y_dev);
+    CUDA_TRY(cudaGetLastError());
+    return BOSSS_OK;
+}
+
+int bosss_b200_bsr_spmv(bosss_bsr* A, double alpha, const double* x, double beta, double* y) {
+    if (!A || !x || !y) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(A->device));
+    const int64_t nx = A->nbc * A->bc, ny = A->nbr * A->br;
+    if (!A->dx) {
+        CUDA_TRY(cudaMalloc(&A->dx, sizeof(double) * std::max<int64_t>(nx, 1)));
+        CUDA_TRY(cudaMalloc(&A->dy, sizeof(double) * std::max<int64_t>(ny, 1)));
+    }
+    cudaStream_t s = A->stream;
+    CUDA_TRY(cudaMemcpyAsync(A->dx, x, sizeof(double) * nx, cudaMemcpyHostToDevice, s));
+    if (beta != 0.0) CUDA_TRY(cudaMemcpyAsync(A->dy, y, sizeof(double) * ny, cudaMemcpyHostToDevice, s));
+    int rc = bosss_b200_bsr_spmv_device(A, alpha, A->dx, beta, A->dy, s);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(y, A->dy, sizeof(double) * ny, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return BOSSS_OK;
+}
+
+int bosss_b200_bsr_get(const bosss_bsr* A, int64_t* n_block_rows, int64_t* n_block_cols, int32_t* row_block,
+                       int32_t* col_block, int64_t* nnz_blocks, int64_t* row_ptr, int32_t* col_idx, double* values) {
+    if (!A) return fail(BOSSS_ERR_BAD_ARG, "null matrix");
+    if (n_block_rows) *n_block_rows = A->nbr;
+    if (n_block_cols) *n_block_cols = A->nbc;
+    if (row_block) *row_block = A->br;
+    if (col_block) *col_block = A->bc;
+    if (nnz_blocks) *nnz_blocks = A->nnzb;
+    CUDA_TRY(cudaSetDevice(A->device));
+    CUDA_TRY(cudaStreamSynchronize(A->stream));
+    if (row_ptr) CUDA_TRY(cudaMemcpy(row_ptr, A->d_rowptr, sizeof(int64_t) * (A->nbr + 1), cudaMemcpyDeviceToHost));
+    if (col_idx && A->nnzb) CUDA_TRY(cudaMemcpy(col_idx, A->d_colidx, sizeof(int32_t) * A->nnzb, cudaMemcpyDeviceToHost));
+    if (values && A->nnzb) {
+        const size_t bs = (size_t)A->br * A->bc;
+        std::vector<double> cm(A->nnzb * bs);
+        CUDA_TRY(cudaMemcpy(cm.data(), A->d_vals, sizeof(double) * cm.size(), cudaMemcpyDeviceToHost));
+        for (int64_t b = 0; b < A->nnzb; ++b)
+            for (int r = 0; r < A->br; ++r)
+                for (int c = 0; c < A->bc; ++c) values[b * bs + (size_t)r * A->bc + c] = cm[b * bs + (size_t)c * A->br + r];
+    }
+    return BOSSS_OK;
+}
+
+int bosss_b200_compute_jacobian(bosss_handle* h, const double* U, double time, bosss_bsr** out) {
+    (void)h; (void)U; (void)time;
+    if (out) *out = nullptr;
+    return fail(BOSSS_ERR_BAD_ARG, "compute_jacobian: not available in this build");
+}
+
+}  // extern "C"

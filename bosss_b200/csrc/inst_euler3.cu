@@ -1,0 +1,9 @@
+// inst_euler3.cu -- explicit instances of the fused DG kernel (one translation unit per
+// physics family and dimension so that they compile in parallel).
+#include "dg_instantiate.cuh"
+
+namespace bosss {
+void register_euler3() {
+    reg_degrees<PhysEuler<3>>(PHYS_EULER, 1);
+}
+}  // namespace bosss

@@ -1,0 +1,408 @@
+"""Host-side mirror of BoSSS's operator registration and evaluator API.
+
+The names and argument meanings follow the reference so that a test (or a C#
+port of this file through P/Invoke) reads like the reference's own code:
+
+* ``DifferentialOperator(DomainVarNames, ParameterVarNames, CodomainVarNames,
+  QuadOrderFunc)`` -- ``DifferentialOperator.cs:452-490``;
+  ``op.EquationComponents[cod].Add(component)``; ``op.Commit()`` (``:658-670``);
+* ``op.GetEvaluatorEx(DomainFields, ParameterMap, CodomainVarMap)``
+  (``:1013-1033``) returns an evaluator with
+  ``Evaluate(alpha, beta, output)`` (``IEvaluator.cs:81-97``):
+  ``output = beta*output + alpha*Op(DomainFields)``;
+* equation components carry the reference class names (``ScalarTransportFlux``,
+  ``SIPLaplace``, ``OptimizedHLLCDensityFlux``, ...).
+
+Every evaluation runs through the C-ABI of ``libbosss_b200.so``; components
+without a device functor fail at ``GetEvaluatorEx`` with
+``BosssError(ERR_UNSUPPORTED_COMPONENT)`` -- there is no CPU fallback.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi as C
+
+# ----------------------------------------------------------------------------- quadrature orders
+
+
+class QuadOrderFunc:
+    """QuadOrderFunc.cs: each factory returns a (kind, parameter) descriptor."""
+
+    @staticmethod
+    def FixedOrder(order):
+        return (C.QUAD_FIXED, int(order))
+
+    @staticmethod
+    def Linear():
+        return (C.QUAD_LINEAR, 1)
+
+    @staticmethod
+    def NonLinear(NonLinDeg):
+        return (C.QUAD_NONLINEAR, int(NonLinDeg))
+
+    @staticmethod
+    def MaxDegTimesTwo():
+        return (C.QUAD_MAXDEG_TIMES_TWO, 0)
+
+    @staticmethod
+    def SumOfMaxDegrees(NonLinDeg=1, RoundUp=True):
+        return (C.QUAD_SUM_OF_MAX_DEGREES if RoundUp else C.QUAD_NONLINEAR, int(NonLinDeg))
+
+
+# ----------------------------------------------------------------------------- grids and fields
+
+
+class CartesianGrid:
+    """Uniform Cartesian grid as built by ``Grid2D.Cartesian2DGrid`` /
+    ``Grid3D.Cartesian3DGrid`` from ``linspace`` node vectors. Local cell order is the
+    generator's (x slowest, last axis fastest; ``Grid3D.cs:232-249``)."""
+
+    def __init__(self, nodes, periodic, cell_order=C.CELLS_GENERATOR):
+        self.dim = len(nodes)
+        if self.dim not in (2, 3):
+            raise ValueError("grid dimension must be 2 or 3")
+        self.n, self.lo, self.hi = [], [], []
+        for x in nodes:
+            x = np.asarray(x, dtype=np.float64)
+            if x.ndim != 1 or len(x) < 2:
+                raise ValueError("node vectors need at least two entries")
+            h = np.diff(x)
+            if not np.allclose(h, h[0], rtol=1e-12, atol=0):
+                raise ValueError("the device path supports uniform (linspace) node vectors only")
+            self.n.append(len(x) - 1)
+            self.lo.append(float(x[0]))
+            self.hi.append(float(x[-1]))
+        self.periodic = [bool(p) for p in periodic]
+        self.cell_order = cell_order
+
+    @property
+    def NoOfCells(self):
+        return int(np.prod(self.n))
+
+    def desc(self):
+        g = C.GridDesc()
+        g.dim = self.dim
+        for d in range(3):
+            g.n[d] = self.n[d] if d < self.dim else 1
+            g.lo[d] = self.lo[d] if d < self.dim else 0.0
+            g.hi[d] = self.hi[d] if d < self.dim else 1.0
+            g.periodic[d] = int(self.periodic[d]) if d < self.dim else 0
+        g.cell_order = self.cell_order
+        return g
+
+    def cell_ijk(self):
+        """(J, dim) integer cell indices in local order."""
+        J = self.NoOfCells
+        j = np.arange(J)
+        if self.cell_order == C.CELLS_GENERATOR:
+            idx = np.unravel_index(j, self.n)                 # x slowest
+        else:
+            idx = np.unravel_index(j, self.n[::-1])[::-1]     # x fastest
+        return np.stack(idx, axis=1)
+
+
+def Cartesian2DGrid(xNodes, yNodes, periodicX=False, periodicY=False, cell_order=C.CELLS_GENERATOR):
+    return CartesianGrid([xNodes, yNodes], [periodicX, periodicY], cell_order)
+
+
+def Cartesian3DGrid(xNodes, yNodes, zNodes, periodicX=False, periodicY=False, periodicZ=False,
+                    cell_order=C.CELLS_GENERATOR):
+    return CartesianGrid([xNodes, yNodes, zNodes], [periodicX, periodicY, periodicZ], cell_order)
+
+
+def np_of(dim, k):
+    return (k + 1) * (k + 2) // 2 if dim == 2 else (k + 1) * (k + 2) * (k + 3) // 6
+
+
+class DGField:
+    """A named DG field of a given degree on a grid (``SinglePhaseField``)."""
+
+    def __init__(self, grid, degree, name):
+        self.grid, self.degree, self.name = grid, int(degree), name
+
+    @property
+    def Np(self):
+        return np_of(self.grid.dim, self.degree)
+
+
+class CoordinateVector:
+    """Coefficients of several fields in the cell-major layout
+    ``j*N + fieldOffset[f] + n`` (``UnsetteledCoordinateMapping.cs:696-706``)."""
+
+    def __init__(self, fields, data=None):
+        self.fields = list(fields)
+        self.grid = self.fields[0].grid
+        self.per_cell = sum(f.Np for f in self.fields)
+        n = self.grid.NoOfCells * self.per_cell
+        self.data = np.zeros(n) if data is None else data
+        if self.data.shape[0] != n:
+            raise ValueError("coordinate vector has length %d, expected %d" % (self.data.shape[0], n))
+
+    def field_view(self, f):
+        """(J, Np) view of field f."""
+        off = sum(x.Np for x in self.fields[:f])
+        return self.data.reshape(self.grid.NoOfCells, self.per_cell)[:, off:off + self.fields[f].Np]
+
+
+# ----------------------------------------------------------------------------- components
+
+
+class _Component:
+    ctype = None
+    ArgumentOrdering = ()
+    ParameterOrdering = None
+
+    def params(self, dim):
+        return []
+
+    def fill(self, comp, cod_index, arg_index, dim):
+        comp.type = self.ctype
+        comp.codomain = cod_index
+        comp.n_args = len(self.ArgumentOrdering)
+        for i, a in enumerate(self.ArgumentOrdering):
+            comp.args[i] = arg_index[a]
+        for i, v in enumerate(self.params(dim)):
+            comp.params[i] = float(v)
+
+
+class ScalarTransportFlux(_Component):
+    """ScalarTransportFlux / ScalarTransportFlux3D (``TransportFlux.cs:29-191``), upwind,
+    with the velocity parameter fields constant (``velocity``)."""
+    ctype = C.COMP_SCALAR_TRANSPORT_FLUX
+
+    def __init__(self, velocity, ArgumentVarName="u"):
+        self.velocity = [float(v) for v in velocity]
+        self.ArgumentOrdering = (ArgumentVarName,)
+
+    def params(self, dim):
+        if len(self.velocity) != dim:
+            raise ValueError("velocity has wrong dimension")
+        return self.velocity
+
+
+class SIPLaplace(_Component):
+    """SIPLaplace (``ipLaplace.cs:30-269``) with ``Nu`` generalised to
+    ``nu(u) = nu0 + nu2*u^2``. ``dirichlet=True`` uses ``g_D(x) = g0 + g1.x + g2.x^2``
+    (componentwise squares) on every boundary edge, else Neumann with ``g_N = 0``."""
+    ctype = C.COMP_SIP_LAPLACE
+
+    def __init__(self, penalty_base, ArgumentVarName="u", nu0=1.0, nu2=0.0, dirichlet=True,
+                 g0=0.0, g1=(0.0, 0.0, 0.0), g2=(0.0, 0.0, 0.0)):
+        self.penalty_base, self.nu0, self.nu2 = float(penalty_base), float(nu0), float(nu2)
+        self.dirichlet = bool(dirichlet)
+        self.g0, self.g1, self.g2 = float(g0), list(g1) + [0.0] * (3 - len(g1)), list(g2) + [0.0] * (3 - len(g2))
+        self.ArgumentOrdering = (ArgumentVarName,)
+
+    def params(self, dim):
+        return ([self.penalty_base, self.nu0, self.nu2, 0.0 if self.dirichlet else 1.0, self.g0]
+                + self.g1[:3] + self.g2[:3])
+
+
+class ConstantSource(_Component):
+    """Constant volume source ``s * v`` (INonlinearSource)."""
+    ctype = C.COMP_CONSTANT_SOURCE
+
+    def __init__(self, value, ArgumentVarName="u"):
+        self.value = float(value)
+        self.ArgumentOrdering = (ArgumentVarName,)
+
+    def params(self, dim):
+        return [self.value]
+
+
+class Material:
+    """Ideal gas with ``HeatCapacityRatio`` gamma and reference ``MachNumber``."""
+
+    def __init__(self, gamma=1.4, Mach=None):
+        self.gamma = float(gamma)
+        self.Mach = float(Mach) if Mach is not None else 1.0 / np.sqrt(self.gamma)
+
+
+def _euler_args(dim):
+    return tuple(["rho"] + ["m%d" % d for d in range(dim)] + ["rhoE"])
+
+
+class OptimizedHLLCDensityFlux(_Component):
+    """``Convection/OptimizedHLLCDensityFlux.cs``"""
+    ctype = C.COMP_HLLC_DENSITY_FLUX
+
+    def __init__(self, material, dim=3):
+        self.material = material
+        self.ArgumentOrdering = _euler_args(dim)
+
+    def params(self, dim):
+        return [self.material.gamma, self.material.Mach, 0.0]
+
+
+class OptimizedHLLCMomentumFlux(OptimizedHLLCDensityFlux):
+    """``Convection/OptimizedHLLCMomentumFlux.cs``"""
+    ctype = C.COMP_HLLC_MOMENTUM_FLUX
+
+    def __init__(self, material, component, dim=3):
+        super().__init__(material, dim)
+        self.component = int(component)
+
+    def params(self, dim):
+        return [self.material.gamma, self.material.Mach, float(self.component)]
+
+
+class OptimizedHLLCEnergyFlux(OptimizedHLLCDensityFlux):
+    """``Convection/OptimizedHLLCEnergyFlux.cs``"""
+    ctype = C.COMP_HLLC_ENERGY_FLUX
+
+
+# ----------------------------------------------------------------------------- operator
+
+
+class _ComponentList(list):
+    def Add(self, comp):
+        self.append(comp)
+
+
+class DifferentialOperator:
+    def __init__(self, DomainVarNames, ParameterVarNames, CodomainVarNames, QuadOrderFunc_=None):
+        self.DomainVar = list(DomainVarNames)
+        self.ParameterVar = list(ParameterVarNames or [])
+        self.CodomainVar = list(CodomainVarNames)
+        self.QuadOrderFunction = QuadOrderFunc_ or QuadOrderFunc.NonLinear(2)
+        self.EquationComponents = {c: _ComponentList() for c in self.CodomainVar}
+        self.IsCommitted = False
+
+    def Commit(self):
+        if self.IsCommitted:
+            raise RuntimeError("operator is already committed")
+        for cod, comps in self.EquationComponents.items():
+            for c in comps:
+                for a in c.ArgumentOrdering:
+                    if a not in self.DomainVar:
+                        raise ValueError("component on '%s' uses unknown argument '%s'" % (cod, a))
+        self.IsCommitted = True
+
+    def descriptor(self, domain_degrees, codomain_degrees, dim):
+        if not self.IsCommitted:
+            raise RuntimeError("operator must be committed before an evaluator is created")
+        d = C.OpDesc()
+        d.n_domain = len(self.DomainVar)
+        d.n_codomain = len(self.CodomainVar)
+        for i, k in enumerate(domain_degrees):
+            d.domain_degree[i] = int(k)
+        for i, k in enumerate(codomain_degrees):
+            d.codomain_degree[i] = int(k)
+        d.quad_kind, d.quad_param = self.QuadOrderFunction
+        arg_index = {n: i for i, n in enumerate(self.DomainVar)}
+        n = 0
+        for ci, cod in enumerate(self.CodomainVar):
+            for comp in self.EquationComponents[cod]:
+                if n >= C.MAX_COMPONENTS:
+                    raise ValueError("too many components")
+                comp.fill(d.components[n], ci, arg_index, dim)
+                n += 1
+        d.n_components = n
+        return d
+
+    def GetEvaluatorEx(self, DomainFields, ParameterMap, CodomainVarMap, device=0,
+                       precision=C.PRECISION_FP64, check_nan=False):
+        """``DomainFields``: list of DGField (or a CoordinateVector); ``CodomainVarMap``:
+        list of DGField of the codomain. ``ParameterMap`` must be empty (parameters are
+        component constants on the device path)."""
+        if ParameterMap:
+            raise C.BosssError(C.ERR_BAD_ARG, "parameter fields are not supported by the device path")
+        dom = DomainFields.fields if isinstance(DomainFields, CoordinateVector) else list(DomainFields)
+        cod = CodomainVarMap.fields if isinstance(CodomainVarMap, CoordinateVector) else list(CodomainVarMap)
+        if len(dom) != len(self.DomainVar) or len(cod) != len(self.CodomainVar):
+            raise ValueError("mismatch between number of fields and operator variables")
+        grid = dom[0].grid
+        return Evaluator(self, grid, [f.degree for f in dom], [f.degree for f in cod],
+                         DomainFields if isinstance(DomainFields, CoordinateVector) else None,
+                         device, precision, check_nan)
+
+
+class Evaluator:
+    """``IEvaluatorNonLin`` backed by one ``bosss_handle``."""
+
+    def __init__(self, op, grid, dom_deg, cod_deg, bound, device, precision, check_nan):
+        self.op, self.grid = op, grid
+        self.desc = op.descriptor(dom_deg, cod_deg, grid.dim)
+        self.gdesc = grid.desc()
+        opt = C.Options()
+        opt.device, opt.precision, opt.check_nan = int(device), int(precision), int(bool(check_nan))
+        h = ctypes.c_void_p()
+        C.check(C.lib().bosss_b200_create(ctypes.byref(self.desc), ctypes.byref(self.gdesc), ctypes.byref(opt),
+                                          ctypes.byref(h)))
+        self.handle = h
+        nd, nc, nq = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+        C.check(C.lib().bosss_b200_get_sizes(h, ctypes.byref(nd), ctypes.byref(nc), ctypes.byref(nq)))
+        self.n_domain, self.n_codomain, self.quad_nodes_1d = nd.value, nc.value, nq.value
+        self.bound = bound
+        self.time = 0.0
+
+    # -- lifetime
+    def Dispose(self):
+        if self.handle:
+            C.lib().bosss_b200_destroy(self.handle)
+            self.handle = None
+
+    __del__ = Dispose
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.Dispose()
+
+    # -- evaluation
+    @staticmethod
+    def _is_cuda(a):
+        return hasattr(a, "is_cuda") and a.is_cuda
+
+    def _stream(self):
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def Evaluate(self, alpha, beta, output, U=None):
+        """``output = beta*output + alpha*Op(U)``; ``U`` defaults to the bound domain
+        fields. numpy arrays go through the host entry point, CUDA tensors through the
+        device-resident one (enqueued on the current torch stream)."""
+        if U is None:
+            if self.bound is None:
+                raise ValueError("no domain fields bound")
+            U = self.bound.data
+        out = output.data if isinstance(output, CoordinateVector) else output
+        if len(U) != self.n_domain or len(out) != self.n_codomain:
+            raise C.BosssError(C.ERR_BAD_ARG, "wrong vector length")   # DifferentialOperator.cs:1590-1591
+        if self._is_cuda(U):
+            C.check(C.lib().bosss_b200_evaluate_device(self.handle, alpha, beta, C.ptr(U), C.ptr(out),
+                                                       self.time, self._stream()))
+        else:
+            U = np.ascontiguousarray(U, dtype=np.float64)
+            C.check(C.lib().bosss_b200_evaluate(self.handle, alpha, beta, C.ptr(U), C.ptr(out), self.time))
+        return out
+
+    def jvp(self, U, V, out=None):
+        """J(U) V (directional derivative)."""
+        if self._is_cuda(U):
+            import torch
+            out = torch.empty(self.n_codomain, dtype=torch.float64, device=U.device) if out is None else out
+            C.check(C.lib().bosss_b200_jvp_device(self.handle, C.ptr(U), C.ptr(V), C.ptr(out), self.time,
+                                                  self._stream()))
+            return out
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        out = np.empty(self.n_codomain) if out is None else out
+        C.check(C.lib().bosss_b200_jvp(self.handle, C.ptr(U), C.ptr(V), C.ptr(out), self.time))
+        return out
+
+    def vjp(self, U, W, out=None):
+        """J(U)^T W (adjoint product)."""
+        if self._is_cuda(U):
+            import torch
+            out = torch.empty(self.n_domain, dtype=torch.float64, device=U.device) if out is None else out
+            C.check(C.lib().bosss_b200_vjp_device(self.handle, C.ptr(U), C.ptr(W), C.ptr(out), self.time,
+                                                  self._stream()))
+            return out
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        out = np.empty(self.n_domain) if out is None else out
+        C.check(C.lib().bosss_b200_vjp(self.handle, C.ptr(U), C.ptr(W), C.ptr(out), self.time))
+        return out

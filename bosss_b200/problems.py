@@ -1,0 +1,180 @@
+"""Seeded synthetic problems of the benchmark configurations.
+
+No public dataset is involved: every input is drawn from
+``numpy.random.Generator(PCG64(seed))`` with the distributions of the workload
+definitions below, and every builder returns the operator, the fields and the
+FP64 coefficient vector in the reference's cell-major layout.
+
+* :func:`transport2d`  -- 2D scalar linear advection, upwind, periodic [0,1]^2,
+  64x64 cells, k=2 (Np=6), Gauss order 2k+1, coefficients iid U[-1,1].
+* :func:`euler3d`      -- 3D compressible Euler with HLLC, periodic [0,1]^3, 32^3
+  hexes, k=3 (Np=20 per variable), order 7, gamma=1.4, Ma=1/sqrt(gamma); primitive
+  state rho=1+0.1U, u_d=0.3U, p=1+0.1U sampled at the volume nodes and
+  L2-projected onto the basis.
+* :func:`nonlinear_diffusion3d` -- -div((1+u^2) grad u) with SIP (penalty base 4,
+  degree factor (k+1)^2, cell length scale as in the reference), Dirichlet g=0,
+  [0,1]^3, 48^3 hexes, k=2..4, order 4k (NonLinear(3)); u sampled iid U[-1,1] at the
+  (k+1)^3 Gauss nodes of every cell and L2-projected (iid coefficients of the
+  orthonormal basis would give physical values ~ (2/h)^1.5, i.e. nu(u) ~ 1e6).
+* :func:`advection_diffusion3d` -- upwind transport (a ~ U[-1,1]^3) + SIP with
+  nu=0.01, periodic, order 2k (Linear()).
+"""
+import numpy as np
+from numpy.polynomial import legendre as npleg
+
+from . import operator as O
+
+
+def rng(seed):
+    return np.random.Generator(np.random.PCG64(seed))
+
+
+class Problem:
+    def __init__(self, name, op, grid, dom, cod, U, config):
+        self.name, self.op, self.grid, self.dom, self.cod, self.U, self.config = name, op, grid, dom, cod, U, config
+
+    def descs(self):
+        """(OpDesc, GridDesc) of the C-ABI -- also what the oracle consumes."""
+        return (self.op.descriptor([f.degree for f in self.dom], [f.degree for f in self.cod], self.grid.dim),
+                self.grid.desc())
+
+    def evaluator(self, **kw):
+        return self.op.GetEvaluatorEx(self.dom, None, self.cod, **kw)
+
+    @property
+    def n_dofs(self):
+        return len(self.U)
+
+
+def _linspace_nodes(n, lo=0.0, hi=1.0):
+    return np.linspace(lo, hi, n + 1)
+
+
+def transport2d(n=64, k=2, seed=1000, velocity=(1.0, 0.5), periodic=True):
+    g = O.Cartesian2DGrid(_linspace_nodes(n), _linspace_nodes(n), periodic, periodic)
+    op = O.DifferentialOperator(["u"], [], ["R"], O.QuadOrderFunc.FixedOrder(2 * k + 1))
+    op.EquationComponents["R"].Add(O.ScalarTransportFlux(velocity, "u"))
+    op.Commit()
+    u = O.DGField(g, k, "u")
+    r = O.DGField(g, k, "R")
+    U = rng(seed).uniform(-1.0, 1.0, g.NoOfCells * u.Np)
+    return Problem("transport2d", op, g, [u], [r], U,
+                   {"workload": "transport2d_upwind_%dx%d_k%d" % (n, n, k), "cells": g.NoOfCells, "k": k,
+                    "seed": seed})
+
+
+def _legendre_table(k, x):
+    """L_a(x) = sqrt((2a+1)/2) P_a(x), shape (len(x), k+1)."""
+    T = np.empty((len(x), k + 1))
+    for a in range(k + 1):
+        c = np.zeros(a + 1)
+        c[a] = 1.0
+        T[:, a] = np.sqrt((2 * a + 1) / 2.0) * npleg.legval(x, c)
+    return T
+
+
+def basis_modes(dim, k):
+    """Exponent tuples in the reference polynomial order."""
+    m = []
+    for deg in range(k + 1):
+        if dim == 2:
+            m += [(a, deg - a) for a in range(deg + 1)]
+        else:
+            m += [(a, b, deg - a - b) for a in range(deg + 1) for b in range(deg - a + 1)]
+    return m
+
+
+def volume_basis(dim, k, nq):
+    """Reference basis at the tensor Gauss nodes (reference node order), weights:
+    returns (phi[Q, Np], W[Q], xi[Q, dim])."""
+    x, w = npleg.leggauss(nq)
+    L = _legendre_table(k, x)
+    modes = basis_modes(dim, k)
+    if dim == 2:
+        qy, qx = np.meshgrid(np.arange(nq), np.arange(nq), indexing="ij")
+        qi = [qx.ravel(), qy.ravel()]
+    else:
+        qz, qy, qx = np.meshgrid(np.arange(nq), np.arange(nq), np.arange(nq), indexing="ij")
+        qi = [qx.ravel(), qy.ravel(), qz.ravel()]
+    phi = np.ones((len(qi[0]), len(modes)))
+    for n, e in enumerate(modes):
+        for d in range(dim):
+            phi[:, n] *= L[qi[d], e[d]]
+    W = np.ones(len(qi[0]))
+    for d in range(dim):
+        W *= w[qi[d]]
+    xi = np.stack([x[qi[d]] for d in range(dim)], axis=1)
+    return phi, W, xi
+
+
+def project_nodal(dim, k, nq, h, nodal):
+    """L2 projection of nodal values nodal[J, Q] onto the orthonormal basis
+    (coefficients of phi_n = phi_ref_n / sqrt(detJ))."""
+    phi, W, _ = volume_basis(dim, k, nq)
+    detJ = np.prod([0.5 * hd for hd in h])
+    scaling = 1.0 / np.sqrt(detJ)
+    return (nodal * W[None, :]) @ phi * (detJ * scaling)
+
+
+def euler3d(n=32, k=3, seed=2000, gamma=1.4, quad_order=7):
+    g = O.Cartesian3DGrid(_linspace_nodes(n), _linspace_nodes(n), _linspace_nodes(n), True, True, True)
+    names = ["rho", "m0", "m1", "m2", "rhoE"]
+    op = O.DifferentialOperator(names, [], ["R_" + s for s in names], O.QuadOrderFunc.FixedOrder(quad_order))
+    mat = O.Material(gamma)
+    op.EquationComponents["R_rho"].Add(O.OptimizedHLLCDensityFlux(mat, 3))
+    for d in range(3):
+        op.EquationComponents["R_m%d" % d].Add(O.OptimizedHLLCMomentumFlux(mat, d, 3))
+    op.EquationComponents["R_rhoE"].Add(O.OptimizedHLLCEnergyFlux(mat, 3))
+    op.Commit()
+    dom = [O.DGField(g, k, s) for s in names]
+    cod = [O.DGField(g, k, "R_" + s) for s in names]
+    nq = (quad_order + 2) // 2
+    J = g.NoOfCells
+    Q = nq ** 3
+    r = rng(seed)
+    rho = 1.0 + 0.1 * r.uniform(-1, 1, (J, Q))
+    vel = 0.3 * r.uniform(-1, 1, (3, J, Q))
+    p = 1.0 + 0.1 * r.uniform(-1, 1, (J, Q))
+    gMs = gamma * mat.Mach ** 2
+    E = p / (gamma - 1.0) + 0.5 * gMs * rho * (vel ** 2).sum(axis=0)
+    h = [1.0 / n] * 3
+    Np = dom[0].Np
+    U = np.empty((J, 5 * Np))
+    fields = [rho, rho * vel[0], rho * vel[1], rho * vel[2], E]
+    for f, val in enumerate(fields):
+        U[:, f * Np:(f + 1) * Np] = project_nodal(3, k, nq, h, val)
+    return Problem("euler3d", op, g, dom, cod, U.ravel(),
+                   {"workload": "euler3d_hllc_%d^3_k%d" % (n, k), "cells": J, "k": k, "seed": seed,
+                    "gamma": gamma, "quad_order": quad_order})
+
+
+def nonlinear_diffusion3d(n=48, k=2, seed=3000, penalty_base=4.0, source=0.0):
+    g = O.Cartesian3DGrid(_linspace_nodes(n), _linspace_nodes(n), _linspace_nodes(n), False, False, False)
+    op = O.DifferentialOperator(["u"], [], ["R"], O.QuadOrderFunc.NonLinear(3))
+    op.EquationComponents["R"].Add(O.SIPLaplace(penalty_base, "u", nu0=1.0, nu2=1.0, dirichlet=True))
+    if source:
+        op.EquationComponents["R"].Add(O.ConstantSource(source, "u"))
+    op.Commit()
+    u = O.DGField(g, k, "u")
+    r_ = O.DGField(g, k, "R")
+    nq = k + 1
+    nodal = rng(seed).uniform(-1.0, 1.0, (g.NoOfCells, nq ** 3))
+    U = project_nodal(3, k, nq, [1.0 / n] * 3, nodal).ravel()
+    return Problem("nonlinear_diffusion3d", op, g, [u], [r_], U,
+                   {"workload": "sip_nonlinear_%d^3_k%d" % (n, k), "cells": g.NoOfCells, "k": k, "seed": seed})
+
+
+def advection_diffusion3d(n=16, k=2, seed=5000, nu=0.01, penalty_base=4.0, velocity=None, periodic=True):
+    r = rng(seed)
+    a = r.uniform(-1, 1, 3) if velocity is None else np.asarray(velocity, dtype=float)
+    g = O.Cartesian3DGrid(_linspace_nodes(n), _linspace_nodes(n), _linspace_nodes(n), periodic, periodic, periodic)
+    op = O.DifferentialOperator(["u"], [], ["R"], O.QuadOrderFunc.Linear())
+    op.EquationComponents["R"].Add(O.ScalarTransportFlux(a, "u"))
+    op.EquationComponents["R"].Add(O.SIPLaplace(penalty_base, "u", nu0=nu, nu2=0.0, dirichlet=True))
+    op.Commit()
+    u = O.DGField(g, k, "u")
+    r_ = O.DGField(g, k, "R")
+    U = r.uniform(-1.0, 1.0, g.NoOfCells * u.Np)
+    return Problem("advection_diffusion3d", op, g, [u], [r_], U,
+                   {"workload": "advdiff_%d^3_k%d" % (n, k), "cells": g.NoOfCells, "k": k, "seed": seed,
+                    "velocity": list(map(float, a)), "nu": nu})

@@ -1,0 +1,210 @@
+/*
+ * bosss_b200.h -- C-ABI of the B200-native DG operator evaluator.
+ *
+ * This is the drop-in boundary below BoSSS's C# operator API. The C# side keeps
+ * its registration (`new DifferentialOperator(...)`, `EquationComponents[cod].Add(..)`,
+ * `Commit()`) and its evaluator interface (`GetEvaluatorEx(..).Evaluate(alpha, beta, out)`);
+ * a GPU evaluator class translates the committed operator into the plain
+ * descriptors below and calls these functions through P/Invoke.
+ *
+ * Conventions
+ *  - every entry point returns an int status: 0 = OK, negative = error;
+ *    `bosss_b200_last_error` returns the message of the last failing call of
+ *    the calling thread.
+ *  - all vectors are FP64 in the reference's cell-major DOF layout
+ *    `idx = j * N_per_cell + fieldOffset[f] + n`
+ *    (UnsetteledCoordinateMapping.cs:696-706), j = local cell index.
+ *  - host pointers are only read/written during the call (C# pins them with
+ *    `fixed`/GCHandle for the duration of the call) and are never retained.
+ *  - one handle = one CUDA stream; calls on one handle must be serialised by
+ *    the caller (the reference evaluators are not thread-safe either).
+ *  - there is no CPU fallback: a component with no device functor makes
+ *    `bosss_b200_create` fail with BOSSS_ERR_UNSUPPORTED_COMPONENT.
+ */
+#ifndef BOSSS_B200_H
+#define BOSSS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BOSSS_B200_VERSION_MAJOR 0
+#define BOSSS_B200_VERSION_MINOR 3
+#define BOSSS_B200_VERSION_PATCH 0
+
+#define BOSSS_MAX_VARS 8
+#define BOSSS_MAX_COMPONENTS 32
+#define BOSSS_MAX_PARAMS 24
+
+/* ---- status codes (DifferentialOperator.cs:1022-1023, 1590-1591 throw on the same conditions) ---- */
+enum bosss_status {
+    BOSSS_OK = 0,
+    BOSSS_ERR_BAD_ARG = -1,                 /* wrong sizes, unsupported option (e.g. SubGridBoundaryTreatment) */
+    BOSSS_ERR_UNSUPPORTED_COMPONENT = -2,   /* a registered equation component has no device functor */
+    BOSSS_ERR_CUDA = -3,                    /* a CUDA runtime call failed */
+    BOSSS_ERR_TIMEOUT = -4,                 /* a bounded device-side wait ran out */
+    BOSSS_ERR_NAN = -5,                     /* opt-in NaN/Inf check tripped */
+    BOSSS_ERR_NO_DEVICE = -6,               /* no CUDA device / library built without one */
+    BOSSS_ERR_OUT_OF_MEMORY = -7
+};
+
+/* ---- equation components with device functors ----
+ * Each value names the reference class whose pointwise semantics the device
+ * functor reproduces. Parameters are passed in `bosss_component.params`. */
+enum bosss_component_type {
+    /* ScalarTransportFlux (2D) / ScalarTransportFlux3D, ScalarTransport/TransportFlux.cs:29-191.
+     * INonlinearFlux, one argument; the velocity parameter fields are constant:
+     * params[0..D-1] = velocity. */
+    BOSSS_COMP_SCALAR_TRANSPORT_FLUX = 1,
+    /* SIPLaplace, NSECommon/ipLaplace.cs:30-269 (IVolumeForm + IEdgeForm), one argument.
+     * Nu(x, p) is generalised to nu(u) = params[1] + params[2]*u^2 (params[2] = 0 is the
+     * reference's constant-viscosity form).
+     * params[0] = penalty_base, params[3] = boundary kind (0 = Dirichlet, 1 = Neumann g_N=0),
+     * Dirichlet value g_D(x) = params[4] + sum_d params[5+d]*x_d + sum_d params[8+d]*x_d^2. */
+    BOSSS_COMP_SIP_LAPLACE = 2,
+    /* Constant volume source (INonlinearSource, NECQuadratureVolume.cs:465-489): params[0] = s,
+     * contributes  s * v. */
+    BOSSS_COMP_CONSTANT_SOURCE = 3,
+    /* OptimizedHLLC{Density,Momentum,Energy}Flux,
+     * CompressibleFlowCommon/Convection/OptimizedHLLC*Flux.cs; arguments = all D+2 conservative
+     * variables (rho, m_0..m_{D-1}, rhoE). params[0] = gamma, params[1] = Mach;
+     * momentum: params[2] = component index. Only periodic grids (no boundary-condition map). */
+    BOSSS_COMP_HLLC_DENSITY_FLUX = 10,
+    BOSSS_COMP_HLLC_MOMENTUM_FLUX = 11,
+    BOSSS_COMP_HLLC_ENERGY_FLUX = 12
+};
+
+/* ---- quadrature-order functions, QuadOrderFunc.cs ---- */
+enum bosss_quad_order_kind {
+    BOSSS_QUAD_FIXED = 0,          /* FixedOrder(order) */
+    BOSSS_QUAD_LINEAR = 1,         /* Linear() = SumOfMaxDegrees(1, false) */
+    BOSSS_QUAD_NONLINEAR = 2,      /* NonLinear(deg) = SumOfMaxDegrees(deg, false) */
+    BOSSS_QUAD_MAXDEG_TIMES_TWO = 3,
+    BOSSS_QUAD_SUM_OF_MAX_DEGREES = 4  /* SumOfMaxDegrees(deg, RoundUp = true) */
+};
+
+typedef struct bosss_component {
+    int32_t type;                      /* enum bosss_component_type */
+    int32_t codomain;                  /* EquationComponents[codomain].Add(..) */
+    int32_t n_args;                    /* length of ArgumentOrdering */
+    int32_t args[BOSSS_MAX_VARS];      /* ArgumentOrdering as domain-variable indices */
+    double params[BOSSS_MAX_PARAMS];
+} bosss_component;
+
+typedef struct bosss_op_desc {
+    int32_t n_domain;                          /* number of domain variables */
+    int32_t n_codomain;                        /* number of codomain variables */
+    int32_t domain_degree[BOSSS_MAX_VARS];     /* DG degree per domain field */
+    int32_t codomain_degree[BOSSS_MAX_VARS];   /* DG degree per codomain field */
+    int32_t quad_kind;                         /* enum bosss_quad_order_kind */
+    int32_t quad_param;                        /* order (FIXED) or nonlinear degree */
+    int32_t n_components;
+    bosss_component components[BOSSS_MAX_COMPONENTS];
+} bosss_op_desc;
+
+/* Uniform Cartesian grid, Grid2D.Cartesian2DGrid / Grid3D.Cartesian3DGrid with linspace nodes. */
+enum bosss_cell_order {
+    /* the generator's local order on one process: x slowest, last axis fastest
+     * (Grid3D.cs:232-249: j = (ix*nY + iy)*nZ + iz; Grid2D: j = ix*nY + iy) */
+    BOSSS_CELLS_GENERATOR = 0,
+    /* GlobalID order: x fastest (GlobalID = ix + iy*nX + iz*nX*nY) */
+    BOSSS_CELLS_GLOBALID = 1
+};
+
+typedef struct bosss_grid_desc {
+    int32_t dim;           /* 2 or 3 */
+    int32_t n[3];          /* cells per direction */
+    double lo[3];          /* domain lower corner */
+    double hi[3];          /* domain upper corner */
+    int32_t periodic[3];   /* 1 = periodic in that direction */
+    int32_t cell_order;    /* enum bosss_cell_order */
+} bosss_grid_desc;
+
+enum bosss_precision {
+    BOSSS_PRECISION_FP64 = 0,        /* plain FP64 path */
+    BOSSS_PRECISION_SPLIT_FP32 = 1   /* split-FP32 basis contractions, FP64 pointwise physics */
+};
+
+typedef struct bosss_options {
+    int32_t device;        /* CUDA device ordinal */
+    int32_t precision;     /* enum bosss_precision */
+    int32_t check_nan;     /* 1 = scan outputs for NaN/Inf, fail with BOSSS_ERR_NAN */
+    int32_t cells_per_block; /* 0 = autotuned */
+    int32_t reserved[8];
+} bosss_options;
+
+typedef struct bosss_handle bosss_handle;
+typedef struct bosss_bsr bosss_bsr;
+
+/* ---- library ---- */
+int bosss_b200_version(int32_t* major, int32_t* minor, int32_t* patch);
+/* Copies the last error message of the calling thread (NUL-terminated, truncated to len). */
+int bosss_b200_last_error(char* buf, size_t len);
+/* Number of CUDA devices visible (0 when none). */
+int bosss_b200_device_count(int32_t* count);
+
+/* ---- operator evaluator ----
+ * create: DifferentialOperator.GetEvaluatorEx (DifferentialOperator.cs:1013-1033) with
+ * CompileQuadratureRules (:205-216); uploads basis tables and grid constants once. */
+int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid,
+                      const bosss_options* opt, bosss_handle** out);
+int bosss_b200_destroy(bosss_handle* h);
+/* DOF counts of the domain and codomain mappings, and the quadrature nodes per direction. */
+int bosss_b200_get_sizes(const bosss_handle* h, int64_t* n_domain_dofs, int64_t* n_codomain_dofs,
+                         int32_t* quad_nodes_1d);
+
+/* EvaluatorNonLin.Evaluate (DifferentialOperator.cs:1584-1661):
+ *   out = beta*out + alpha*Op(U),  host buffers (copies in and out inside the call). */
+int bosss_b200_evaluate(bosss_handle* h, double alpha, double beta, const double* U,
+                        double* out, double time);
+/* Same, device-resident buffers (U, out are device pointers), enqueued on `stream`
+ * (cudaStream_t, NULL = the handle's stream); returns after enqueueing. */
+int bosss_b200_evaluate_device(bosss_handle* h, double alpha, double beta, const double* U_dev,
+                               double* out_dev, double time, void* stream);
+
+/* Directional derivative J(U)*V of the nonlinear operator; replaces the FD `dirder`
+ * of the matrix-free Newton-GMRES (Newton.cs:1450-1495). Host buffers. */
+int bosss_b200_jvp(bosss_handle* h, const double* U, const double* V, double* JV, double time);
+/* Adjoint product J(U)^T * W (transpose of the Jacobian that
+ * EvaluatorLinear.ComputeMatrix / FDJacobianBuilder assemble, DifferentialOperator.cs:1740-1838,
+ * 2558-2858). Host buffers. */
+int bosss_b200_vjp(bosss_handle* h, const double* U, const double* W, double* JTW, double time);
+int bosss_b200_jvp_device(bosss_handle* h, const double* U_dev, const double* V_dev, double* JV_dev,
+                          double time, void* stream);
+int bosss_b200_vjp_device(bosss_handle* h, const double* U_dev, const double* W_dev, double* JTW_dev,
+                          double time, void* stream);
+/* Blocks until all work enqueued on the handle's stream is done; reports device-side errors. */
+int bosss_b200_synchronize(bosss_handle* h);
+
+/* ---- block-sparse matrix (BlockMsrMatrix, BoSSS.Platform/LinAlg/BlockMsrMatrix.cs:186) ----
+ * Block rows = cells of the codomain mapping, block columns = cells of the domain mapping,
+ * every stored block dense (row_block x col_block), row-major within the block.
+ * row_ptr[n_block_rows+1], col_idx[nnz_blocks], values[nnz_blocks*row_block*col_block]. */
+int bosss_b200_bsr_create(int64_t n_block_rows, int64_t n_block_cols, int32_t row_block,
+                          int32_t col_block, const int64_t* row_ptr, const int32_t* col_idx,
+                          const double* values, int32_t device, bosss_bsr** out);
+int bosss_b200_bsr_destroy(bosss_bsr* A);
+/* BlockMsrMatrix.SpMV (BlockMsrMatrix.cs:2554-2990): y = beta*y + alpha*A*x, host buffers. */
+int bosss_b200_bsr_spmv(bosss_bsr* A, double alpha, const double* x, double beta, double* y);
+/* Device-resident variant on `stream` (NULL = the matrix's stream). */
+int bosss_b200_bsr_spmv_device(bosss_bsr* A, double alpha, const double* x_dev, double beta,
+                               double* y_dev, void* stream);
+/* Reads the matrix back (same layout as bosss_b200_bsr_create's inputs). row_ptr/col_idx/values
+ * may be NULL to query sizes only. */
+int bosss_b200_bsr_get(const bosss_bsr* A, int64_t* n_block_rows, int64_t* n_block_cols,
+                       int32_t* row_block, int32_t* col_block, int64_t* nnz_blocks,
+                       int64_t* row_ptr, int32_t* col_idx, double* values);
+
+/* Jacobian assembly of the operator at state U into a new block-sparse matrix
+ * (EvaluatorLinear.ComputeMatrix, LECVolumeQuadrature2.cs:132 / LECEdgeQuadrature2.cs:127 ->
+ * BlockMsrMatrix.AccBlock): exact linearisation, cell-block pattern = self + face neighbours. */
+int bosss_b200_compute_jacobian(bosss_handle* h, const double* U, double time, bosss_bsr** out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BOSSS_B200_H */

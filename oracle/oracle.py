@@ -1,0 +1,154 @@
+"""ctypes wrapper of the CPU FP64 oracle ``oracle/_build/libdg_oracle.so``.
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` -- never by the ``bosss_b200`` package. It
+takes the same descriptors as the C-ABI (``include/bosss_b200.h``).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libdg_oracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        P = ctypes.c_void_p
+        L.orc_evaluate.argtypes = [P, P, ctypes.c_double, ctypes.c_double, P, P]
+        L.orc_jvp.argtypes = [P, P, P, P, P]
+        L.orc_jacobian_blocks.argtypes = [P, P, P, P, P]
+        L.orc_sizes.argtypes = [P, P, P, P, P]
+        L.orc_gauss_rule.argtypes = [ctypes.c_int, P, P]
+        L.orc_basis_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P]
+        L.orc_basis_monomials.argtypes = [ctypes.c_int, ctypes.c_int, P, P]
+        L.orc_threads.argtypes = [ctypes.c_int]
+        L.orc_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(rc):
+    if rc != 0:
+        buf = ctypes.create_string_buffer(512)
+        lib().orc_last_error(buf, 512)
+        raise RuntimeError("oracle error %d: %s" % (rc, buf.value.decode()))
+
+
+def threads(n=0):
+    """Set (n > 0) and return the OpenMP thread count of the oracle."""
+    return lib().orc_threads(n)
+
+
+def sizes(opd, gd):
+    nd, nc, nq = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+    _check(lib().orc_sizes(ctypes.byref(opd), ctypes.byref(gd), ctypes.byref(nd), ctypes.byref(nc),
+                           ctypes.byref(nq)))
+    return nd.value, nc.value, nq.value
+
+
+def evaluate(opd, gd, U, alpha=1.0, beta=0.0, out=None):
+    nd, nc, _ = sizes(opd, gd)
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    assert U.shape == (nd,)
+    out = np.zeros(nc) if out is None else np.array(out, dtype=np.float64, copy=True)
+    _check(lib().orc_evaluate(ctypes.byref(opd), ctypes.byref(gd), alpha, beta, _p(U), _p(out)))
+    return out
+
+
+def jvp(opd, gd, U, V):
+    nd, nc, _ = sizes(opd, gd)
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    out = np.zeros(nc)
+    _check(lib().orc_jvp(ctypes.byref(opd), ctypes.byref(gd), _p(U), _p(V), _p(out)))
+    return out
+
+
+def jacobian_dense(opd, gd, U):
+    """Exact Jacobian (dense, small problems only) assembled from the oracle's
+    cell-block Jacobian."""
+    nd, nc, _ = sizes(opd, gd)
+    D = gd.dim
+    J = int(np.prod([gd.n[d] for d in range(D)]))
+    Nd, Nc = nd // J, nc // J
+    NB = 1 + 2 * D
+    blocks = np.zeros(J * NB * Nc * Nd)
+    nbr = np.zeros(J * NB, dtype=np.int32)
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    _check(lib().orc_jacobian_blocks(ctypes.byref(opd), ctypes.byref(gd), _p(U), _p(blocks), _p(nbr)))
+    blocks = blocks.reshape(J, NB, Nc, Nd)
+    nbr = nbr.reshape(J, NB)
+    A = np.zeros((nc, nd))
+    for j in range(J):
+        seen = set()
+        for b in range(NB):
+            jc = nbr[j, b]
+            if jc < 0 or jc in seen:
+                continue
+            seen.add(jc)
+            A[j * Nc:(j + 1) * Nc, jc * Nd:(jc + 1) * Nd] = blocks[j, b]
+    return A
+
+
+def jacobian_blocks(opd, gd, U):
+    """Cell-block Jacobian: (blocks[J, 1+2D, Nc, Nd], nbr[J, 1+2D])."""
+    nd, nc, _ = sizes(opd, gd)
+    D = gd.dim
+    J = int(np.prod([gd.n[d] for d in range(D)]))
+    Nd, Nc = nd // J, nc // J
+    NB = 1 + 2 * D
+    blocks = np.zeros(J * NB * Nc * Nd)
+    nbr = np.zeros(J * NB, dtype=np.int32)
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    _check(lib().orc_jacobian_blocks(ctypes.byref(opd), ctypes.byref(gd), _p(U), _p(blocks), _p(nbr)))
+    return blocks.reshape(J, NB, Nc, Nd), nbr.reshape(J, NB)
+
+
+def gauss_rule(n):
+    x, w = np.zeros(n), np.zeros(n)
+    lib().orc_gauss_rule(n, _p(x), _p(w))
+    return x, w
+
+
+def basis_eval(D, k, pts):
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, D)
+    npts = pts.shape[0]
+    from math import comb
+    Np = comb(k + D, D)
+    phi = np.zeros(Np * npts)
+    dphi = np.zeros(Np * npts * D)
+    lib().orc_basis_eval(D, k, npts, _p(pts), _p(phi), _p(dphi))
+    return phi.reshape(Np, npts), dphi.reshape(Np, npts, D)
+
+
+def basis_monomials(D, k):
+    """List per polynomial of (coef, exponents) terms of the oracle's basis."""
+    from math import comb
+    Np = comb(k + D, D)
+    T = (k + 1) ** D
+    coef = np.zeros(Np * T)
+    exps = np.zeros(Np * T * 3, dtype=np.int32)
+    lib().orc_basis_monomials(D, k, _p(coef), _p(exps))
+    coef = coef.reshape(Np, T)
+    exps = exps.reshape(Np, T, 3)
+    out = []
+    for p in range(Np):
+        out.append([(coef[p, t], tuple(exps[p, t, :D])) for t in range(T) if coef[p, t] != 0.0])
+    return out

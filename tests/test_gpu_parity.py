@@ -1,0 +1,218 @@
+"""GPU parity of the sm_100a path against the CPU FP64 oracle, through the C-ABI.
+
+Tolerances (FP64 plain path): relative L2 error <= 1e-12 against the oracle for
+residuals and JVPs; the VJP is checked against the transpose of the oracle's
+assembled Jacobian (small grids) and, at full size, through the adjoint identity
+w.(J v) = (J^T w).v.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from bosss_b200 import _capi as C
+from bosss_b200 import operator as O
+from bosss_b200 import problems as P
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+SMALL = [
+    ("transport2d_8x6_k2", lambda: P.transport2d(n=8, k=2, seed=21)),
+    ("transport2d_nonper_k3", lambda: P.transport2d(n=5, k=3, seed=22, periodic=False)),
+    ("euler3d_4_k1", lambda: P.euler3d(n=4, k=1, seed=23)),
+    ("euler3d_3_k3", lambda: P.euler3d(n=3, k=3, seed=24)),
+    ("sip3d_4_k2", lambda: P.nonlinear_diffusion3d(n=4, k=2, seed=25)),
+    ("sip3d_3_k3", lambda: P.nonlinear_diffusion3d(n=3, k=3, seed=26)),
+    ("sip3d_3_k4", lambda: P.nonlinear_diffusion3d(n=3, k=4, seed=27)),
+    ("sip3d_src_k2", lambda: P.nonlinear_diffusion3d(n=3, k=2, seed=28, source=1.5)),
+    ("advdiff3d_4_k2", lambda: P.advection_diffusion3d(n=4, k=2, seed=29)),
+    ("advdiff3d_3_k1_nonper", lambda: P.advection_diffusion3d(n=3, k=1, seed=30, periodic=False)),
+    ("advdiff3d_3_k4", lambda: P.advection_diffusion3d(n=3, k=4, seed=31)),
+]
+
+
+@pytest.mark.parametrize("name,make", SMALL, ids=[s[0] for s in SMALL])
+def test_residual_small(name, make):
+    pr = make()
+    ref = orc.evaluate(*pr.descs(), pr.U)
+    with pr.evaluator() as ev:
+        out = np.zeros(ev.n_codomain)
+        ev.Evaluate(1.0, 0.0, out, pr.U)
+    assert rel(out, ref) <= TOL, rel(out, ref)
+
+
+@pytest.mark.parametrize("name,make", SMALL, ids=[s[0] for s in SMALL])
+def test_jvp_small(name, make):
+    pr = make()
+    V = np.random.default_rng(1).uniform(-1, 1, pr.n_dofs)
+    ref = orc.jvp(*pr.descs(), pr.U, V)
+    with pr.evaluator() as ev:
+        out = ev.jvp(pr.U, V)
+    assert rel(out, ref) <= TOL, rel(out, ref)
+
+
+@pytest.mark.parametrize("name,make", SMALL, ids=[s[0] for s in SMALL])
+def test_vjp_is_transposed_jacobian(name, make):
+    pr = make()
+    opd, gd = pr.descs()
+    A = orc.jacobian_dense(opd, gd, pr.U)
+    W = np.random.default_rng(2).uniform(-1, 1, A.shape[0])
+    ref = A.T @ W
+    with pr.evaluator() as ev:
+        out = ev.vjp(pr.U, W)
+    assert rel(out, ref) <= TOL, rel(out, ref)
+
+
+def test_alpha_beta_semantics():
+    pr = P.euler3d(n=3, k=2, seed=40)
+    r = np.random.default_rng(3)
+    out0 = r.uniform(-1, 1, pr.n_dofs)
+    ref = orc.evaluate(*pr.descs(), pr.U, alpha=-0.7, beta=0.3, out=out0)
+    with pr.evaluator() as ev:
+        out = out0.copy()
+        ev.Evaluate(-0.7, 0.3, out, pr.U)
+    assert rel(out, ref) <= TOL
+
+
+def test_globalid_cell_order():
+    """Same operator on the GlobalID cell numbering gives the permuted residual."""
+    a = P.advection_diffusion3d(n=4, k=2, seed=41, periodic=False)
+    g2 = O.Cartesian3DGrid(np.linspace(0, 1, 5), np.linspace(0, 1, 5), np.linspace(0, 1, 5),
+                           False, False, False, cell_order=C.CELLS_GLOBALID)
+    ijk1, ijk2 = a.grid.cell_ijk(), g2.cell_ijk()
+    pos = {tuple(t): i for i, t in enumerate(ijk1)}
+    perm = np.array([pos[tuple(t)] for t in ijk2])
+    Np = a.dom[0].Np
+    U2 = a.U.reshape(-1, Np)[perm].ravel()
+    dom2 = [O.DGField(g2, 2, "u")]
+    cod2 = [O.DGField(g2, 2, "R")]
+    with a.evaluator() as e1, a.op.GetEvaluatorEx(dom2, None, cod2) as e2:
+        r1 = np.zeros(e1.n_codomain)
+        r2 = np.zeros(e2.n_codomain)
+        e1.Evaluate(1.0, 0.0, r1, a.U)
+        e2.Evaluate(1.0, 0.0, r2, U2)
+    assert rel(r2, r1.reshape(-1, Np)[perm].ravel()) <= TOL
+
+
+FULL = [
+    ("C1_transport2d_64x64_k2", lambda: P.transport2d(n=64, k=2, seed=1000)),
+    ("C2_euler3d_32_k3", lambda: P.euler3d(n=32, k=3, seed=2000)),
+    ("C3_sip3d_48_k2", lambda: P.nonlinear_diffusion3d(n=48, k=2, seed=3000)),
+    ("C3_sip3d_24_k3", lambda: P.nonlinear_diffusion3d(n=24, k=3, seed=3001)),
+    ("C3_sip3d_16_k4", lambda: P.nonlinear_diffusion3d(n=16, k=4, seed=3002)),
+]
+
+
+@pytest.mark.parametrize("name,make", FULL, ids=[s[0] for s in FULL])
+def test_residual_full_size(name, make):
+    pr = make()
+    ref = orc.evaluate(*pr.descs(), pr.U)
+    with pr.evaluator() as ev:
+        out = np.zeros(ev.n_codomain)
+        ev.Evaluate(1.0, 0.0, out, pr.U)
+    assert rel(out, ref) <= TOL, rel(out, ref)
+
+
+@pytest.mark.parametrize("name,make", FULL[:3], ids=[s[0] for s in FULL[:3]])
+def test_adjoint_identity_full_size(name, make):
+    """w.(J v) == (J^T w).v at full size (size-independent property)."""
+    pr = make()
+    r = np.random.default_rng(4)
+    V = r.uniform(-1, 1, pr.n_dofs)
+    W = r.uniform(-1, 1, pr.n_dofs)
+    with pr.evaluator() as ev:
+        jv = ev.jvp(pr.U, V)
+        jtw = ev.vjp(pr.U, W)
+    a, b = W @ jv, jtw @ V
+    assert abs(a - b) <= 1e-11 * (np.linalg.norm(W) * np.linalg.norm(jv)), (a, b)
+
+
+def test_jvp_matches_central_fd_full_size():
+    pr = P.nonlinear_diffusion3d(n=48, k=2, seed=3000)
+    V = np.random.default_rng(5).uniform(-1, 1, pr.n_dofs)
+    eps = 1e-6
+    with pr.evaluator() as ev:
+        jv = ev.jvp(pr.U, V)
+        fp = np.zeros(ev.n_codomain)
+        fm = np.zeros(ev.n_codomain)
+        ev.Evaluate(1.0, 0.0, fp, pr.U + eps * V)
+        ev.Evaluate(1.0, 0.0, fm, pr.U - eps * V)
+    fd = (fp - fm) / (2 * eps)
+    assert rel(jv, fd) < 1e-7
+
+
+def test_device_resident_path_matches_host_path():
+    import torch
+    pr = P.euler3d(n=8, k=2, seed=42)
+    with pr.evaluator() as ev:
+        out_h = np.zeros(ev.n_codomain)
+        ev.Evaluate(1.0, 0.0, out_h, pr.U)
+        U = torch.from_numpy(pr.U).cuda()
+        out_d = torch.zeros(ev.n_codomain, dtype=torch.float64, device="cuda")
+        ev.Evaluate(1.0, 0.0, out_d, U)
+        torch.cuda.synchronize()
+    assert np.array_equal(out_d.cpu().numpy(), out_h)
+
+
+def test_check_nan_option():
+    pr = P.euler3d(n=3, k=1, seed=43)
+    U = pr.U.copy()
+    U[5] = np.nan
+    with pr.evaluator(check_nan=True) as ev:
+        out = np.zeros(ev.n_codomain)
+        with pytest.raises(C.BosssError) as ei:
+            ev.Evaluate(1.0, 0.0, out, U)
+        assert ei.value.code == C.ERR_NAN
+
+
+def _bsr_from_dense_blocks(blocks, nbr):
+    J, NB, Nc, Nd = blocks.shape
+    rowptr = [0]
+    cols, vals = [], []
+    for j in range(J):
+        seen = set()
+        for b in range(NB):
+            c = int(nbr[j, b])
+            if c < 0 or c in seen:
+                continue
+            seen.add(c)
+            cols.append(c)
+            vals.append(blocks[j, b])
+        rowptr.append(len(cols))
+    return (np.array(rowptr, dtype=np.int64), np.array(cols, dtype=np.int32),
+            np.ascontiguousarray(np.array(vals)).ravel())
+
+
+def test_block_sparse_spmv_matches_dense():
+    pr = P.nonlinear_diffusion3d(n=4, k=2, seed=44)
+    opd, gd = pr.descs()
+    blocks, nbr = orc.jacobian_blocks(opd, gd, pr.U)
+    rp, ci, vals = _bsr_from_dense_blocks(blocks, nbr)
+    Adense = orc.jacobian_dense(opd, gd, pr.U)
+    J, NB, Nc, Nd = blocks.shape
+    A = ctypes.c_void_p()
+    C.check(C.lib().bosss_b200_bsr_create(J, J, Nc, Nd, C.ptr(rp), C.ptr(ci), C.ptr(vals), 0, ctypes.byref(A)))
+    try:
+        r = np.random.default_rng(7)
+        x = r.uniform(-1, 1, J * Nd)
+        y0 = r.uniform(-1, 1, J * Nc)
+        y = y0.copy()
+        C.check(C.lib().bosss_b200_bsr_spmv(A, 0.5, C.ptr(x), -2.0, C.ptr(y)))
+        ref = 0.5 * Adense @ x - 2.0 * y0
+        assert rel(y, ref) <= TOL
+        # read back
+        nnzb = ctypes.c_int64()
+        C.check(C.lib().bosss_b200_bsr_get(A, None, None, None, None, ctypes.byref(nnzb), None, None, None))
+        v2 = np.zeros(nnzb.value * Nc * Nd)
+        C.check(C.lib().bosss_b200_bsr_get(A, None, None, None, None, None, None, None, C.ptr(v2)))
+        assert np.array_equal(v2, vals)
+    finally:
+        C.lib().bosss_b200_bsr_destroy(A)
