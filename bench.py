@@ -196,7 +196,8 @@ def main():
     R = torch.zeros(n, dtype=torch.float64, device=dev)
     G = torch.zeros(n, dtype=torch.float64, device=dev)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)          # all timed work and the events on one stream
+    torch.cuda.set_stream(stream)
     sptr = ctypes.c_void_p(stream.cuda_stream)
     h = ev.handle
 

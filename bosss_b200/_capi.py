@@ -41,6 +41,10 @@ QUAD_SUM_OF_MAX_DEGREES = 4
 CELLS_GENERATOR = 0
 CELLS_GLOBALID = 1
 
+# cudaStreamLegacy: the legacy default stream (a NULL stream argument selects the
+# handle's own stream)
+CUDA_STREAM_LEGACY = 1
+
 PRECISION_FP64 = 0
 PRECISION_SPLIT_FP32 = 1
 

@@ -322,6 +322,7 @@ class Evaluator:
     """``IEvaluatorNonLin`` backed by one ``bosss_handle``."""
 
     def __init__(self, op, grid, dom_deg, cod_deg, bound, device, precision, check_nan):
+        self.handle = None
         self.op, self.grid = op, grid
         self.desc = op.descriptor(dom_deg, cod_deg, grid.dim)
         self.gdesc = grid.desc()
@@ -357,8 +358,11 @@ class Evaluator:
         return hasattr(a, "is_cuda") and a.is_cuda
 
     def _stream(self):
+        """The current torch stream; torch's legacy default stream (handle 0) is passed as
+        cudaStreamLegacy, since a NULL stream selects the handle's own stream."""
         import torch
-        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        s = torch.cuda.current_stream().cuda_stream
+        return ctypes.c_void_p(s if s else C.CUDA_STREAM_LEGACY)
 
     def Evaluate(self, alpha, beta, output, U=None):
         """``output = beta*output + alpha*Op(U)``; ``U`` defaults to the bound domain

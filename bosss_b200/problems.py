@@ -8,7 +8,7 @@ FP64 coefficient vector in the reference's cell-major layout.
 * :func:`transport2d`  -- 2D scalar linear advection, upwind, periodic [0,1]^2,
   64x64 cells, k=2 (Np=6), Gauss order 2k+1, coefficients iid U[-1,1].
 * :func:`euler3d`      -- 3D compressible Euler with HLLC, periodic [0,1]^3, 32^3
-  hexes, k=3 (Np=20 per variable), order 7, gamma=1.4, Ma=1/sqrt(gamma); primitive
+  hexes, k=3 (Np=20 per variable), order 7 (= 2k+1), gamma=1.4, Ma=1/sqrt(gamma); primitive
   state rho=1+0.1U, u_d=0.3U, p=1+0.1U sampled at the volume nodes and
   L2-projected onto the basis.
 * :func:`nonlinear_diffusion3d` -- -div((1+u^2) grad u) with SIP (penalty base 4,
@@ -116,7 +116,8 @@ def project_nodal(dim, k, nq, h, nodal):
     return (nodal * W[None, :]) @ phi * (detJ * scaling)
 
 
-def euler3d(n=32, k=3, seed=2000, gamma=1.4, quad_order=7):
+def euler3d(n=32, k=3, seed=2000, gamma=1.4, quad_order=None):
+    quad_order = 2 * k + 1 if quad_order is None else quad_order
     g = O.Cartesian3DGrid(_linspace_nodes(n), _linspace_nodes(n), _linspace_nodes(n), True, True, True)
     names = ["rho", "m0", "m1", "m2", "rhoE"]
     op = O.DifferentialOperator(names, [], ["R_" + s for s in names], O.QuadOrderFunc.FixedOrder(quad_order))

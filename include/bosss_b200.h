@@ -18,6 +18,9 @@
  *    `fixed`/GCHandle for the duration of the call) and are never retained.
  *  - one handle = one CUDA stream; calls on one handle must be serialised by
  *    the caller (the reference evaluators are not thread-safe either).
+ *  - `stream` arguments of the *_device entry points: NULL selects the handle's own
+ *    (non-blocking) stream; pass cudaStreamLegacy ((void*)1) for the legacy default
+ *    stream.
  *  - there is no CPU fallback: a component with no device functor makes
  *    `bosss_b200_create` fail with BOSSS_ERR_UNSUPPORTED_COMPONENT.
  */
