@@ -135,12 +135,22 @@ def test_adjoint_identity_full_size(name, make):
     assert abs(a - b) <= 1e-11 * (np.linalg.norm(W) * np.linalg.norm(jv)), (a, b)
 
 
+def test_jvp_full_size_matches_oracle():
+    pr = P.nonlinear_diffusion3d(n=48, k=2, seed=3000)
+    V = np.random.default_rng(5).uniform(-1, 1, pr.n_dofs)
+    ref = orc.jvp(*pr.descs(), pr.U, V)
+    with pr.evaluator() as ev:
+        jv = ev.jvp(pr.U, V)
+    assert rel(jv, ref) <= TOL, rel(jv, ref)
+
+
 def test_jvp_matches_central_fd_full_size():
-    """Central FD with eps = 1e-6 at full size. The SIP penalty picks
-    nuMax = |nuA| > |nuB| ? nuA : nuB (ipLaplace.cs:181), a kink of the form: among the
-    ~8e6 face nodes of the 48^3 grid a few lie within eps of it, where FD is not a
-    derivative. So the check is entrywise: all but a tiny fraction of DOFs agree to
-    1e-6 of max|Jv|, and the median relative error is at FD-truncation level."""
+    """Central FD with eps = 1e-6 at full size, a sanity check of the linearisation.
+    Coefficients of the orthonormal basis carry the scaling (2/h)^1.5 ~ 940 on the
+    48^3 grid, so eps = 1e-6 moves u by ~1e-3 and central FD is accurate to ~1e-6
+    only; in addition the SIP penalty picks nuMax = |nuA| > |nuB| ? nuA : nuB
+    (ipLaplace.cs:181), a kink where FD is not a derivative. The exact comparison
+    is test_jvp_full_size_matches_oracle."""
     pr = P.nonlinear_diffusion3d(n=48, k=2, seed=3000)
     V = np.random.default_rng(5).uniform(-1, 1, pr.n_dofs)
     eps = 1e-6
@@ -151,10 +161,9 @@ def test_jvp_matches_central_fd_full_size():
         ev.Evaluate(1.0, 0.0, fp, pr.U + eps * V)
         ev.Evaluate(1.0, 0.0, fm, pr.U - eps * V)
     fd = (fp - fm) / (2 * eps)
-    err = np.abs(jv - fd)
-    scale = np.max(np.abs(jv))
-    assert np.mean(err > 1e-6 * scale) < 1e-4
-    assert np.median(err / np.maximum(np.abs(jv), 1e-3 * scale)) < 1e-7
+    err = np.abs(jv - fd) / np.maximum(np.abs(jv), 1e-3 * np.max(np.abs(jv)))
+    assert np.median(err) < 1e-5
+    assert np.mean(err > 1e-3) < 1e-4
 
 
 def test_device_resident_path_matches_host_path():
