@@ -45,6 +45,10 @@ CELLS_GLOBALID = 1
 # handle's own stream)
 CUDA_STREAM_LEGACY = 1
 
+KERNEL_AUTO = 0
+KERNEL_GENERIC = 1
+KERNEL_SLAB = 2
+
 PRECISION_FP64 = 0
 PRECISION_SPLIT_FP32 = 1
 
@@ -88,7 +92,7 @@ class Options(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("precision", ctypes.c_int32),
         ("check_nan", ctypes.c_int32),
-        ("cells_per_block", ctypes.c_int32),
+        ("kernel", ctypes.c_int32),
         ("reserved", ctypes.c_int32 * 8),
     ]
 

@@ -159,7 +159,7 @@ using namespace bosss;
 struct bosss_handle {
     int device = 0;
     cudaStream_t stream = nullptr;
-    int phys = 0, D = 0, K = 0, Q = 0;
+    int phys = 0, D = 0, K = 0, Q = 0, variant = 0;
     EvalArgs base{};
     int64_t ndom = 0, ncod = 0;
     KernelEntry kern[3]{};
@@ -400,10 +400,19 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     const int Q = std::max(1, (order + 2) / 2);   // smallest Gauss rule with 2Q-1 >= order
     ensure_registered();
     auto& reg = kernel_registry();
-    for (int m = 0; m < 3; ++m)
-        if (!reg.count(KernelKey(phys, D, K, Q, m)))
-            return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no device kernel for degree " + std::to_string(K) +
-                                                             " with " + std::to_string(Q) + " Gauss nodes");
+    const int want = opt ? opt->kernel : 0;
+    if (want < 0 || want > 2) return fail(BOSSS_ERR_BAD_ARG, "bad kernel selector");
+    int variant = VARIANT_GENERIC;
+    bool have_slab = true, have_generic = true;
+    for (int m = 0; m < 3; ++m) {
+        have_slab = have_slab && reg.count(KernelKey(phys, D, K, Q, m, VARIANT_SLAB));
+        have_generic = have_generic && reg.count(KernelKey(phys, D, K, Q, m, VARIANT_GENERIC));
+    }
+    if (want == 2 && !have_slab) return fail(BOSSS_ERR_BAD_ARG, "no slab kernel for this operator");
+    if (want == 2 || (want == 0 && have_slab)) variant = VARIANT_SLAB;
+    if (variant == VARIANT_GENERIC && !have_generic)
+        return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no device kernel for degree " + std::to_string(K) +
+                                                         " with " + std::to_string(Q) + " Gauss nodes");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -464,7 +473,8 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     const int NV = (phys == PHYS_EULER) ? D + 2 : 1;
     h->ndom = (int64_t)J * NV * np_of(D, K);
     h->ncod = h->ndom;
-    for (int m = 0; m < 3; ++m) h->kern[m] = reg[KernelKey(phys, D, K, Q, m)];
+    for (int m = 0; m < 3; ++m) h->kern[m] = reg[KernelKey(phys, D, K, Q, m, variant)];
+    h->variant = variant;
     cudaError_t e = cudaSetDevice(dev);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {

@@ -1,6 +1,7 @@
 // dg_instantiate.cuh -- launch wrappers and registration of explicit kernel instances.
 #pragma once
 #include "dg_kernel.cuh"
+#include "dg_slab_kernel.cuh"
 #include "dg_registry.h"
 
 namespace bosss {
@@ -29,9 +30,42 @@ template <class Phys, int K, int Q, int MODE>
 void reg_one(int phys) {
     using C = Cfg<Phys, K, Q, MODE>;
     if constexpr (C::SMEM_BYTES <= 227 * 1024) {
-        kernel_registry()[KernelKey(phys, Phys::D, K, Q, MODE)] =
+        kernel_registry()[KernelKey(phys, Phys::D, K, Q, MODE, VARIANT_GENERIC)] =
             KernelEntry{&launch_cell_kernel<Phys, K, Q, MODE>, C::CPB, C::SMEM_BYTES};
     }
+}
+
+template <class Phys, int K, int Q, int MODE>
+cudaError_t launch_slab_kernel(const EvalArgs& a, cudaStream_t s) {
+    using C = SlabCfg<Phys, K, Q, MODE>;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static unsigned long long attr_done = 0ull;
+    if (!(attr_done & (1ull << (dev & 63)))) {
+        cudaError_t e = cudaFuncSetAttribute(dg_slab_kernel<Phys, K, Q, MODE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        attr_done |= (1ull << (dev & 63));
+    }
+    const long long blocks = ((long long)a.g.J + C::CPB - 1) / C::CPB;
+    dg_slab_kernel<Phys, K, Q, MODE><<<(unsigned)blocks, C::NT, C::SMEM_BYTES, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class Phys, int K, int Q, int MODE>
+void reg_slab_one(int phys) {
+    using C = SlabCfg<Phys, K, Q, MODE>;
+    if constexpr (C::SMEM_BYTES <= 227 * 1024 && C::NT <= 256) {
+        kernel_registry()[KernelKey(phys, 3, K, Q, MODE, VARIANT_SLAB)] =
+            KernelEntry{&launch_slab_kernel<Phys, K, Q, MODE>, C::CPB, C::SMEM_BYTES};
+    }
+}
+
+template <class Phys, int K, int Q>
+void reg_slab_modes(int phys) {
+    reg_slab_one<Phys, K, Q, MODE_RES>(phys);
+    reg_slab_one<Phys, K, Q, MODE_JVP>(phys);
+    reg_slab_one<Phys, K, Q, MODE_VJP>(phys);
 }
 
 template <class Phys, int K, int Q>

@@ -16,7 +16,8 @@ struct KernelEntry {
     size_t smem_bytes;
 };
 
-using KernelKey = std::tuple<int, int, int, int, int>;   // phys, D, K, Q, mode
+enum KernelVariant { VARIANT_GENERIC = 0, VARIANT_SLAB = 1 };
+using KernelKey = std::tuple<int, int, int, int, int, int>;   // phys, D, K, Q, mode, variant
 std::map<KernelKey, KernelEntry>& kernel_registry();
 
 void register_scalar2();

@@ -1,0 +1,646 @@
+// dg_slab_kernel.cuh -- register-blocked 3D DG kernel for systems (several fields).
+//
+// Same algorithm and results as dg_cell_kernel (NECQuadratureVolume / NECQuadratureEdge
+// restated with sum factorisation, cell-centric faces), different work split:
+//
+//  * one thread per (cell, output field o, slab q). For the volume, slab q is the
+//    z-node index: sum factorisation contracting z first keeps every later stage
+//    inside the slab, so a thread interpolates u (and grad u) at the Q^2 nodes of its
+//    slab from the field's Np coefficients entirely in registers, and projects the
+//    slab's pointwise results back onto all Np test functions, again in registers.
+//    For a face normal to d the slab is the node row along the face's second in-plane
+//    direction. The Q partial residuals of a (cell, field) are summed once at the end;
+//  * 1D table entries with compile-time indices are read from the kernel-parameter
+//    constant bank (free FMA operands); the thread's own slab row lives in registers;
+//  * shared memory only carries the node values between the contraction threads and
+//    the pointwise threads (padded strides against bank conflicts).
+#pragma once
+#include <type_traits>
+
+#include "dg_kernel.cuh"
+
+namespace bosss {
+
+template <class Phys, int K, int Q, int MODE>
+struct SlabCfg {
+    using B = Cfg<Phys, K, Q, MODE>;
+    static constexpr int D = 3;
+    static_assert(Phys::D == 3, "slab kernel is three-dimensional");
+    static constexpr int NP = B::NP, NV = B::NV, NC = B::NC, NFI = B::NFI, NCI = B::NCI, NO = B::NO;
+    static constexpr int NPAIR = B::NPAIR, NS = B::NS;
+    static constexpr bool GRAD_IN = B::GRAD_IN;
+    static constexpr bool VOL_OV = B::VOL_OV, VOL_OG = B::VOL_OG, FACE_OV = B::FACE_OV, FACE_OG = B::FACE_OG;
+    static constexpr int NCOV = (VOL_OV ? 1 : 0) + (VOL_OG ? 3 : 0);
+    static constexpr int NCOF = (FACE_OV ? 1 : 0) + (FACE_OG ? 3 : 0);
+    static constexpr int GOV = VOL_OV ? 1 : 0;    // first gradient comp of volume outputs
+    static constexpr int GOF = FACE_OV ? 1 : 0;
+    static constexpr int SLV = Q * Q + 1;          // padded volume slab
+    static constexpr int FV = Q * SLV;             // one (field, comp) volume block
+    static constexpr int SLF = Q + 1;              // padded face row
+    static constexpr int FF = Q * SLF;             // one (field, comp) face block
+    static constexpr int TPC = NO * Q;             // threads per cell
+    static constexpr int S_CIN = NFI * NP;
+    static constexpr int S_VOL = NFI * NCI * FV + NO * NCOV * FV;
+    static constexpr int S_FACE = 2 * 2 * NFI * NCI * FF + 2 * NO * NCOF * FF;
+    static constexpr int S_RED = NO * Q * NP;
+    static constexpr int S_W0 = S_VOL > S_FACE ? S_VOL : S_FACE;
+    static constexpr int S_WORK = S_W0 > S_RED ? S_W0 : S_RED;
+    static constexpr int S_CELL = S_CIN + S_WORK;
+    static constexpr int BUDGET = 110 * 1024 / 8;
+    static constexpr int CPB_SMEM = BUDGET / S_CELL;
+    static constexpr int CPB_THR = 256 / TPC;
+    static constexpr int CPB0 = CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR;
+    static constexpr int CPB = CPB0 < 1 ? 1 : CPB0;
+    static constexpr int NT = CPB * TPC;
+    static constexpr size_t SMEM_BYTES = (size_t)CPB * S_CELL * 8;
+};
+
+template <int DIR> struct FaceDirs {
+    static constexpr int t1 = (DIR == 0) ? 1 : 0;
+    static constexpr int t2 = (DIR == 2) ? 1 : 2;
+};
+
+template <int DIR>
+__host__ __device__ constexpr int mode_dpr(int m, int p, int r) {
+    return DIR == 0 ? mode3(m, p, r) : (DIR == 1 ? mode3(p, m, r) : mode3(p, r, m));
+}
+
+// ------------------------------------------------------------------ pointwise helpers
+// Volume node: in(f, comp) reads interpolated fields, out(o, c, v) stores projected
+// coefficients (c = 0: test function, 1+d: gradient d) already scaled by `fac` and 2/h.
+template <class Phys, int MODE, int NCI, bool OV, bool OG, class In, class Out>
+__device__ __forceinline__ void volume_point(const PhysParams& ph, const double* x, double fac,
+                                             const double* twoh, In in, Out out) {
+    constexpr int D = Phys::D, NV = Phys::NV, NC = Phys::NC;
+    constexpr bool G = NCI > 1;
+    if constexpr (MODE == MODE_RES) {
+        double U[NV], Gr[NV][D], fV[NC], fG[NC][D];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            U[i] = in(i, 0);
+#pragma unroll
+            for (int d = 0; d < D; ++d) Gr[i][d] = G ? in(i, 1 + d) : 0.0;
+        }
+#pragma unroll
+        for (int e = 0; e < NC; ++e) {
+            fV[e] = 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) fG[e][d] = 0.0;
+        }
+        Phys::volume(ph, U, Gr, x, fV, fG);
+#pragma unroll
+        for (int e = 0; e < NC; ++e) {
+            if (OV) out(e, 0, fV[e] * fac);
+            if (OG)
+#pragma unroll
+                for (int d = 0; d < D; ++d) out(e, 1 + d, fG[e][d] * fac * twoh[d]);
+        }
+    } else if constexpr (MODE == MODE_JVP) {
+        using T = DualN<1>;
+        T U[NV], Gr[NV][D], fV[NC], fG[NC][D];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            U[i].v = in(i, 0);
+            U[i].d[0] = in(NV + i, 0);
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                Gr[i][d].v = G ? in(i, 1 + d) : 0.0;
+                Gr[i][d].d[0] = G ? in(NV + i, 1 + d) : 0.0;
+            }
+        }
+        Phys::volume(ph, U, Gr, x, fV, fG);
+#pragma unroll
+        for (int e = 0; e < NC; ++e) {
+            if (OV) out(e, 0, fV[e].d[0] * fac);
+            if (OG)
+#pragma unroll
+                for (int d = 0; d < D; ++d) out(e, 1 + d, fG[e][d].d[0] * fac * twoh[d]);
+        }
+    } else {
+        constexpr int NS = NV * (Phys::GRAD_U ? 1 + D : 1);
+        using T = DualN<NS>;
+        T U[NV], Gr[NV][D], fV[NC], fG[NC][D];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            U[i] = T(in(i, 0));
+            U[i].d[Phys::GRAD_U ? i * (1 + D) : i] = 1.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                Gr[i][d] = T(G ? in(i, 1 + d) : 0.0);
+                if (Phys::GRAD_U) Gr[i][d].d[i * (1 + D) + 1 + d] = 1.0;
+            }
+        }
+        Phys::volume(ph, U, Gr, x, fV, fG);
+        T phi(0.0);
+#pragma unroll
+        for (int e = 0; e < NC; ++e) {
+            if (Phys::VOL_V) phi += fV[e] * in(NV + e, 0);
+            if (Phys::VOL_G)
+#pragma unroll
+                for (int d = 0; d < D; ++d) phi += fG[e][d] * in(NV + e, 1 + d);
+        }
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            out(i, 0, phi.d[Phys::GRAD_U ? i * (1 + D) : i] * fac);
+            if (Phys::GRAD_U)
+#pragma unroll
+                for (int d = 0; d < D; ++d) out(i, 1 + d, phi.d[i * (1 + D) + 1 + d] * fac * twoh[d]);
+        }
+    }
+}
+
+// Face node: inA/inB read the traces of the IN (lower) and OUT (upper) cell,
+// out(o, c, v) stores the own side's coefficients.
+template <class Phys, int MODE, int NCI, bool OV, bool OG, class InA, class InB, class Out>
+__device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, bool selfA, double pnlty,
+                                           const double* nrm, const double* x, double fac, const double* twoh,
+                                           InA inA, InB inB, Out out) {
+    constexpr int D = Phys::D, NV = Phys::NV, NC = Phys::NC;
+    constexpr bool G = NCI > 1;
+    if constexpr (MODE == MODE_RES) {
+        double UA[NV], GA[NV][D], UB[NV], GB[NV][D], gA[NC], GAv[NC][D], gB[NC], GBv[NC][D];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            UA[i] = inA(i, 0);
+            UB[i] = inner ? inB(i, 0) : 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                GA[i][d] = G ? inA(i, 1 + d) : 0.0;
+                GB[i][d] = (G && inner) ? inB(i, 1 + d) : 0.0;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < NC; ++e) {
+            gA[e] = gB[e] = 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) GAv[e][d] = GBv[e][d] = 0.0;
+        }
+        if (inner) Phys::inner(ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
+        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, gA, GAv);
+#pragma unroll
+        for (int e = 0; e < NC; ++e) {
+            if (OV) out(e, 0, (selfA ? gA[e] : gB[e]) * fac);
+            if (OG)
+#pragma unroll
+                for (int d = 0; d < D; ++d) out(e, 1 + d, (selfA ? GAv[e][d] : GBv[e][d]) * fac * twoh[d]);
+        }
+    } else if constexpr (MODE == MODE_JVP) {
+        using T = DualN<1>;
+        T UA[NV], GA[NV][D], UB[NV], GB[NV][D], gA[NC], GAv[NC][D], gB[NC], GBv[NC][D];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            UA[i].v = inA(i, 0);
+            UA[i].d[0] = inA(NV + i, 0);
+            UB[i].v = inner ? inB(i, 0) : 0.0;
+            UB[i].d[0] = inner ? inB(NV + i, 0) : 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                GA[i][d].v = G ? inA(i, 1 + d) : 0.0;
+                GA[i][d].d[0] = G ? inA(NV + i, 1 + d) : 0.0;
+                GB[i][d].v = (G && inner) ? inB(i, 1 + d) : 0.0;
+                GB[i][d].d[0] = (G && inner) ? inB(NV + i, 1 + d) : 0.0;
+            }
+        }
+        if (inner) Phys::inner(ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
+        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, gA, GAv);
+#pragma unroll
+        for (int e = 0; e < NC; ++e) {
+            if (OV) out(e, 0, (selfA ? gA[e].d[0] : gB[e].d[0]) * fac);
+            if (OG)
+#pragma unroll
+                for (int d = 0; d < D; ++d)
+                    out(e, 1 + d, (selfA ? GAv[e][d].d[0] : GBv[e][d].d[0]) * fac * twoh[d]);
+        }
+    } else {
+        constexpr int NS = NV * (Phys::GRAD_U ? 1 + D : 1);
+        using T = DualN<NS>;
+        T UA[NV], GA[NV][D], UB[NV], GB[NV][D], gA[NC], GAv[NC][D], gB[NC], GBv[NC][D];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            UA[i] = T(inA(i, 0));
+            UB[i] = T(inner ? inB(i, 0) : 0.0);
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                GA[i][d] = T(G ? inA(i, 1 + d) : 0.0);
+                GB[i][d] = T((G && inner) ? inB(i, 1 + d) : 0.0);
+            }
+            (selfA ? UA[i] : UB[i]).d[Phys::GRAD_U ? i * (1 + D) : i] = 1.0;
+            if (Phys::GRAD_U)
+#pragma unroll
+                for (int d = 0; d < D; ++d) (selfA ? GA[i][d] : GB[i][d]).d[i * (1 + D) + 1 + d] = 1.0;
+        }
+        if (inner) Phys::inner(ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
+        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, gA, GAv);
+        T phi(0.0);
+#pragma unroll
+        for (int e = 0; e < NC; ++e) {
+            const int fe = NV + e;
+            if (Phys::FACE_V) {
+                phi += gA[e] * inA(fe, 0);
+                if (inner) phi += gB[e] * inB(fe, 0);
+            }
+            if (Phys::FACE_G)
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    phi += GAv[e][d] * inA(fe, 1 + d);
+                    if (inner) phi += GBv[e][d] * inB(fe, 1 + d);
+                }
+        }
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            out(i, 0, phi.d[Phys::GRAD_U ? i * (1 + D) : i] * fac);
+            if (Phys::GRAD_U)
+#pragma unroll
+                for (int d = 0; d < D; ++d) out(i, 1 + d, phi.d[i * (1 + D) + 1 + d] * fac * twoh[d]);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ contraction helpers
+// interpolation of one field at the slab qz = q (Q*Q nodes), into node block `nb`
+template <int K, int Q, bool GRAD>
+__device__ __forceinline__ void slab_interp(const Tables1D& T, const double* cf, const double* Az, const double* dAz,
+                                            int q, double scaling, const double* twoh, double* nb) {
+    constexpr int NPAIR = (K + 1) * (K + 2) / 2;
+    constexpr int SLV = Q * Q + 1, FV = Q * SLV;
+    double T1[NPAIR], T1z[NPAIR];
+#pragma unroll
+    for (int a = 0; a <= K; ++a)
+#pragma unroll
+        for (int b = 0; b <= K - a; ++b) {
+            double s = 0.0, sz = 0.0;
+#pragma unroll
+            for (int c = 0; c <= K - a - b; ++c) {
+                const double v = cf[mode3(a, b, c)];
+                s += v * Az[c];
+                if (GRAD) sz += v * dAz[c];
+            }
+            T1[pair_index(K, a, b)] = s;
+            T1z[pair_index(K, a, b)] = sz;
+        }
+    double* base = nb + q * SLV;
+#pragma unroll
+    for (int qy = 0; qy < Q; ++qy) {
+        double T2[K + 1], T2y[K + 1], T2z[K + 1];
+#pragma unroll
+        for (int a = 0; a <= K; ++a) {
+            double s = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll
+            for (int b = 0; b <= K - a; ++b) {
+                const double v = T1[pair_index(K, a, b)];
+                s += v * T.A[qy][b];
+                if (GRAD) {
+                    sy += v * T.dA[qy][b];
+                    sz += T1z[pair_index(K, a, b)] * T.A[qy][b];
+                }
+            }
+            T2[a] = s;
+            T2y[a] = sy;
+            T2z[a] = sz;
+        }
+#pragma unroll
+        for (int qx = 0; qx < Q; ++qx) {
+            double u = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
+#pragma unroll
+            for (int a = 0; a <= K; ++a) {
+                u += T2[a] * T.A[qx][a];
+                if (GRAD) {
+                    ux += T2[a] * T.dA[qx][a];
+                    uy += T2y[a] * T.A[qx][a];
+                    uz += T2z[a] * T.A[qx][a];
+                }
+            }
+            base[qy * Q + qx] = u * scaling;
+            if (GRAD) {
+                base[FV + qy * Q + qx] = ux * scaling * twoh[0];
+                base[2 * FV + qy * Q + qx] = uy * scaling * twoh[1];
+                base[3 * FV + qy * Q + qx] = uz * scaling * twoh[2];
+            }
+        }
+    }
+}
+
+// projection of the slab qz = q of one output field (block `ob`, comps) into R[NP]
+template <int K, int Q, bool OV, bool OG>
+__device__ __forceinline__ void slab_project(const Tables1D& T, const double* ob, const double* Az, const double* dAz,
+                                             int q, double* R) {
+    constexpr int NPAIR = (K + 1) * (K + 2) / 2;
+    constexpr int SLV = Q * Q + 1, FV = Q * SLV;
+    constexpr int G0 = OV ? 1 : 0;
+    double P2[NPAIR], P2z[NPAIR];
+#pragma unroll
+    for (int i = 0; i < NPAIR; ++i) P2[i] = P2z[i] = 0.0;
+    const double* base = ob + q * SLV;
+#pragma unroll
+    for (int qy = 0; qy < Q; ++qy) {
+        double P[K + 1], Py[K + 1], Pz[K + 1];
+#pragma unroll
+        for (int a = 0; a <= K; ++a) P[a] = Py[a] = Pz[a] = 0.0;
+#pragma unroll
+        for (int qx = 0; qx < Q; ++qx) {
+            const int n = qy * Q + qx;
+            const double s = OV ? base[n] : 0.0;
+            const double gx = OG ? base[G0 * FV + n] : 0.0;
+            const double gy = OG ? base[(G0 + 1) * FV + n] : 0.0;
+            const double gz = OG ? base[(G0 + 2) * FV + n] : 0.0;
+#pragma unroll
+            for (int a = 0; a <= K; ++a) {
+                P[a] += s * T.A[qx][a] + gx * T.dA[qx][a];
+                Py[a] += gy * T.A[qx][a];
+                Pz[a] += gz * T.A[qx][a];
+            }
+        }
+#pragma unroll
+        for (int a = 0; a <= K; ++a)
+#pragma unroll
+            for (int b = 0; b <= K - a; ++b) {
+                P2[pair_index(K, a, b)] += P[a] * T.A[qy][b] + Py[a] * T.dA[qy][b];
+                P2z[pair_index(K, a, b)] += Pz[a] * T.A[qy][b];
+            }
+    }
+#pragma unroll
+    for (int a = 0; a <= K; ++a)
+#pragma unroll
+        for (int b = 0; b <= K - a; ++b)
+#pragma unroll
+            for (int c = 0; c <= K - a - b; ++c)
+                R[mode3(a, b, c)] += P2[pair_index(K, a, b)] * Az[c] + P2z[pair_index(K, a, b)] * dAz[c];
+}
+
+// trace of one field at face DIR, own face side fs (0: xi_d = -1, 1: +1), row q2 = q
+template <int DIR, int K, int Q, bool GRAD>
+__device__ __forceinline__ void face_interp(const Tables1D& T, const double* cf, int fs, const double* A2,
+                                            const double* dA2, double scaling, const double* twoh, double* tb) {
+    constexpr int t1 = FaceDirs<DIR>::t1, t2 = FaceDirs<DIR>::t2;
+    constexpr int SLF = Q + 1, FF = Q * SLF;
+    double Tv[K + 1], Tn[K + 1], Tt2[K + 1];
+#pragma unroll
+    for (int p = 0; p <= K; ++p) {
+        double s0 = 0.0, sn = 0.0, st = 0.0;
+#pragma unroll
+        for (int r = 0; r <= K - p; ++r) {
+            double S = 0.0, Sn = 0.0;
+#pragma unroll
+            for (int m = 0; m <= K - p - r; ++m) {
+                const double v = cf[mode_dpr<DIR>(m, p, r)];
+                S += v * (fs ? T.e[1][m] : T.e[0][m]);
+                if (GRAD) Sn += v * (fs ? T.de[1][m] : T.de[0][m]);
+            }
+            s0 += S * A2[r];
+            if (GRAD) {
+                sn += Sn * A2[r];
+                st += S * dA2[r];
+            }
+        }
+        Tv[p] = s0;
+        Tn[p] = sn;
+        Tt2[p] = st;
+    }
+#pragma unroll
+    for (int q1 = 0; q1 < Q; ++q1) {
+        double u = 0.0, u1 = 0.0, u2 = 0.0, un = 0.0;
+#pragma unroll
+        for (int p = 0; p <= K; ++p) {
+            u += Tv[p] * T.A[q1][p];
+            if (GRAD) {
+                u1 += Tv[p] * T.dA[q1][p];
+                u2 += Tt2[p] * T.A[q1][p];
+                un += Tn[p] * T.A[q1][p];
+            }
+        }
+        tb[q1] = u * scaling;
+        if (GRAD) {
+            tb[(1 + DIR) * FF + q1] = un * scaling * twoh[DIR];
+            tb[(1 + t1) * FF + q1] = u1 * scaling * twoh[t1];
+            tb[(1 + t2) * FF + q1] = u2 * scaling * twoh[t2];
+        }
+    }
+}
+
+template <int DIR, int K, int Q, bool OV, bool OG>
+__device__ __forceinline__ void face_project(const Tables1D& T, const double* ob, int fs, const double* A2,
+                                             const double* dA2, double* R) {
+    constexpr int t1 = FaceDirs<DIR>::t1, t2 = FaceDirs<DIR>::t2;
+    constexpr int SLF = Q + 1, FF = Q * SLF;
+    constexpr int G0 = OV ? 1 : 0;
+    double P[K + 1], Pn[K + 1], Pt2[K + 1];
+#pragma unroll
+    for (int p = 0; p <= K; ++p) P[p] = Pn[p] = Pt2[p] = 0.0;
+#pragma unroll
+    for (int q1 = 0; q1 < Q; ++q1) {
+        const double g = OV ? ob[q1] : 0.0;
+        const double gn = OG ? ob[(G0 + DIR) * FF + q1] : 0.0;
+        const double g1 = OG ? ob[(G0 + t1) * FF + q1] : 0.0;
+        const double g2 = OG ? ob[(G0 + t2) * FF + q1] : 0.0;
+#pragma unroll
+        for (int p = 0; p <= K; ++p) {
+            P[p] += g * T.A[q1][p] + g1 * T.dA[q1][p];
+            Pn[p] += gn * T.A[q1][p];
+            Pt2[p] += g2 * T.A[q1][p];
+        }
+    }
+#pragma unroll
+    for (int p = 0; p <= K; ++p)
+#pragma unroll
+        for (int r = 0; r <= K - p; ++r) {
+            const double w0 = P[p] * A2[r] + Pt2[p] * dA2[r];
+            const double wn = Pn[p] * A2[r];
+#pragma unroll
+            for (int m = 0; m <= K - p - r; ++m)
+                R[mode_dpr<DIR>(m, p, r)] += w0 * (fs ? T.e[1][m] : T.e[0][m]) + wn * (fs ? T.de[1][m] : T.de[0][m]);
+        }
+}
+
+// ------------------------------------------------------------------ the kernel
+template <class Phys, int K, int Q, int MODE>
+__global__ void __launch_bounds__(SlabCfg<Phys, K, Q, MODE>::NT)
+dg_slab_kernel(const __grid_constant__ EvalArgs args) {
+    using C = SlabCfg<Phys, K, Q, MODE>;
+    constexpr int NP = C::NP, NV = C::NV, NFI = C::NFI, NCI = C::NCI, NO = C::NO, CPB = C::CPB, NT = C::NT;
+    constexpr int SLV = C::SLV, FV = C::FV, SLF = C::SLF, FF = C::FF, QF = Q * Q;
+    constexpr bool GI = C::GRAD_IN;
+    extern __shared__ double smem[];
+    const GridConst& g = args.g;
+    const Tables1D& T = args.tab;
+    const int tid = threadIdx.x;
+    const long long c0 = (long long)blockIdx.x * CPB;
+    const int ncell = (int)((g.J - c0) < CPB ? (g.J - c0) : CPB);
+    // own (cell, output field, slab)
+    const int q = tid % Q, o = (tid / Q) % NO, cl = tid / (Q * NO);
+    const bool active = cl < ncell;
+    auto CIN = [&](int c) { return smem + (size_t)c * C::S_CELL; };
+    auto WK = [&](int c) { return smem + (size_t)c * C::S_CELL + C::S_CIN; };
+
+    constexpr int NVPC = NV * NP;
+    constexpr int N1PC = C::B::NF1 * NP;
+    for (int i = tid; i < ncell * NVPC; i += NT) CIN(i / NVPC)[i % NVPC] = args.U[c0 * NVPC + i];
+    if constexpr (C::B::NF1 > 0)
+        for (int i = tid; i < ncell * N1PC; i += NT) CIN(i / N1PC)[NVPC + i % N1PC] = args.V[c0 * N1PC + i];
+
+    double Aq[K + 1], dAq[K + 1];
+#pragma unroll
+    for (int a = 0; a <= K; ++a) {
+        Aq[a] = T.A[q][a];
+        dAq[a] = T.dA[q][a];
+    }
+    double R[NP];
+#pragma unroll
+    for (int n = 0; n < NP; ++n) R[n] = 0.0;
+    int ijk[3];
+    cell_ijk(g, c0 + (active ? cl : 0), ijk);
+    __syncthreads();
+
+    // ---------------------------------------------------------- volume
+    {
+        double* nodes = nullptr;
+        (void)nodes;
+        if (active) {
+            for (int f = o; f < NFI; f += NO) {
+                double cf[NP];
+#pragma unroll
+                for (int n = 0; n < NP; ++n) cf[n] = CIN(cl)[f * NP + n];
+                slab_interp<K, Q, GI>(T, cf, Aq, dAq, q, g.scaling, g.twoh, WK(cl) + f * NCI * FV);
+            }
+        }
+        __syncthreads();
+        constexpr int OUT0 = NFI * NCI * FV;
+        for (int it = tid; it < CPB * Q * Q * Q; it += NT) {
+            const int n = it % (Q * Q * Q), c = it / (Q * Q * Q);
+            if (c >= ncell) continue;
+            const int qx = n % Q, qy = (n / Q) % Q, qz = n / (Q * Q);
+            const int off = qz * SLV + qy * Q + qx;
+            int cijk[3];
+            cell_ijk(g, c0 + c, cijk);
+            double x[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) x[d] = g.lo[d] + (cijk[d] + 0.5) * g.h[d];
+            x[0] += 0.5 * g.h[0] * T.xq[qx];
+            x[1] += 0.5 * g.h[1] * T.xq[qy];
+            x[2] += 0.5 * g.h[2] * T.xq[qz];
+            const double fac = T.w[qx] * T.w[qy] * T.w[qz] * g.detJ * g.scaling;
+            const double* nb = WK(c);
+            double* ob = WK(c) + OUT0;
+            volume_point<Phys, MODE, NCI, C::VOL_OV, C::VOL_OG>(
+                args.ph, x, fac, g.twoh, [&](int f, int comp) { return nb[(f * NCI + comp) * FV + off]; },
+                [&](int oo, int comp, double v) {
+                    const int cc = C::VOL_OV ? comp : comp - 1;
+                    ob[(oo * C::NCOV + cc) * FV + off] = v;
+                });
+        }
+        __syncthreads();
+        if (active) slab_project<K, Q, C::VOL_OV, C::VOL_OG>(T, WK(cl) + OUT0 + o * C::NCOV * FV, Aq, dAq, q, R);
+        __syncthreads();
+    }
+
+    // ---------------------------------------------------------- faces
+    auto face_pass = [&](auto dirc) {
+        constexpr int DIR = decltype(dirc)::value;
+        constexpr int t1 = FaceDirs<DIR>::t1, t2 = FaceDirs<DIR>::t2;
+        constexpr int TRB = NFI * NCI * FF;     // one (s, side) trace block
+        constexpr int OUTF0 = 2 * 2 * TRB;
+        // traces: own side 0, neighbour side 1, faces s = 0 (lower), 1 (upper)
+        if (active) {
+            for (int f = o; f < NFI; f += NO) {
+                double cf[NP];
+#pragma unroll
+                for (int n = 0; n < NP; ++n) cf[n] = CIN(cl)[f * NP + n];
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+                    face_interp<DIR, K, Q, GI>(T, cf, s, Aq, dAq, g.scaling, g.twoh,
+                                               WK(cl) + (s * 2 + 0) * TRB + f * NCI * FF + q * SLF);
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const long long nb = neighbour(g, ijk, DIR, s);
+                    double cn[NP];
+                    if (nb >= 0) {
+                        const double* src = (f < NV) ? args.U + nb * NVPC + f * NP : args.V + nb * N1PC + (f - NV) * NP;
+#pragma unroll
+                        for (int n = 0; n < NP; ++n) cn[n] = __ldg(src + n);
+                    } else {
+#pragma unroll
+                        for (int n = 0; n < NP; ++n) cn[n] = 0.0;
+                    }
+                    face_interp<DIR, K, Q, GI>(T, cn, 1 - s, Aq, dAq, g.scaling, g.twoh,
+                                               WK(cl) + (s * 2 + 1) * TRB + f * NCI * FF + q * SLF);
+                }
+            }
+        }
+        __syncthreads();
+        for (int it = tid; it < CPB * 2 * QF; it += NT) {
+            const int qf = it % QF, s = (it / QF) % 2, c = it / (2 * QF);
+            if (c >= ncell) continue;
+            const int q1 = qf % Q, q2 = qf / Q;
+            const int off = q2 * SLF + q1;
+            int cijk[3];
+            cell_ijk(g, c0 + c, cijk);
+            const long long nb = neighbour(g, cijk, DIR, s);
+            const bool inner = nb >= 0;
+            double x[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) x[d] = g.lo[d] + (cijk[d] + 0.5) * g.h[d];
+            x[DIR] += (s ? 0.5 : -0.5) * g.h[DIR];
+            x[t1] += 0.5 * g.h[t1] * T.xq[q1];
+            x[t2] += 0.5 * g.h[t2] * T.xq[q2];
+            double nrm[3] = {0.0, 0.0, 0.0};
+            nrm[DIR] = inner ? 1.0 : (s ? 1.0 : -1.0);
+            double pnlty;
+            if (inner) {
+                int ijk2[3] = {cijk[0], cijk[1], cijk[2]};
+                ijk2[DIR] = (int)((nb / g.stride[DIR]) % g.n[DIR]);
+                pnlty = args.ph.pen * fmax(cell_cj(g, cijk), cell_cj(g, ijk2));
+            } else {
+                pnlty = 2.0 * args.ph.pen * cell_cj(g, cijk);
+            }
+            const bool selfA = !inner || s == 1;
+            const double* trOwn = WK(c) + (s * 2 + 0) * TRB;
+            const double* trNb = WK(c) + (s * 2 + 1) * TRB;
+            const double* trA = selfA ? trOwn : trNb;
+            const double* trB = selfA ? trNb : trOwn;
+            double* ob = WK(c) + OUTF0 + s * NO * C::NCOF * FF;
+            const double fac = T.w[q1] * T.w[q2] * g.faceSG[DIR] * g.scaling;
+            face_point<Phys, MODE, NCI, C::FACE_OV, C::FACE_OG>(
+                args.ph, inner, selfA, pnlty, nrm, x, fac, g.twoh,
+                [&](int f, int comp) { return trA[(f * NCI + comp) * FF + off]; },
+                [&](int f, int comp) { return trB[(f * NCI + comp) * FF + off]; },
+                [&](int oo, int comp, double v) {
+                    const int cc = C::FACE_OV ? comp : comp - 1;
+                    ob[(oo * C::NCOF + cc) * FF + off] = v;
+                });
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int s = 0; s < 2; ++s)
+                face_project<DIR, K, Q, C::FACE_OV, C::FACE_OG>(
+                    T, WK(cl) + OUTF0 + (s * NO + o) * C::NCOF * FF + q * SLF, s, Aq, dAq, R);
+        }
+        __syncthreads();
+    };
+    face_pass(std::integral_constant<int, 0>{});
+    face_pass(std::integral_constant<int, 1>{});
+    face_pass(std::integral_constant<int, 2>{});
+
+    // ---------------------------------------------------------- reduce slabs and store
+    if (active) {
+        double* red = WK(cl) + (o * Q + q) * NP;
+#pragma unroll
+        for (int n = 0; n < NP; ++n) red[n] = R[n];
+    }
+    __syncthreads();
+    if (active) {
+        const long long obase = (c0 + cl) * (long long)(NO * NP) + o * NP;
+        for (int n = q; n < NP; n += Q) {
+            double v = 0.0;
+#pragma unroll
+            for (int qq = 0; qq < Q; ++qq) v += WK(cl)[(o * Q + qq) * NP + n];
+            if constexpr (MODE == MODE_RES) {
+                args.out[obase + n] =
+                    (args.beta == 0.0) ? args.alpha * v : args.beta * args.out[obase + n] + args.alpha * v;
+            } else {
+                args.out[obase + n] = v;
+            }
+        }
+    }
+}
+
+}  // namespace bosss

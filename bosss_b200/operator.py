@@ -302,7 +302,7 @@ class DifferentialOperator:
         return d
 
     def GetEvaluatorEx(self, DomainFields, ParameterMap, CodomainVarMap, device=0,
-                       precision=C.PRECISION_FP64, check_nan=False):
+                       precision=C.PRECISION_FP64, check_nan=False, kernel=C.KERNEL_AUTO):
         """``DomainFields``: list of DGField (or a CoordinateVector); ``CodomainVarMap``:
         list of DGField of the codomain. ``ParameterMap`` must be empty (parameters are
         component constants on the device path)."""
@@ -315,19 +315,20 @@ class DifferentialOperator:
         grid = dom[0].grid
         return Evaluator(self, grid, [f.degree for f in dom], [f.degree for f in cod],
                          DomainFields if isinstance(DomainFields, CoordinateVector) else None,
-                         device, precision, check_nan)
+                         device, precision, check_nan, kernel)
 
 
 class Evaluator:
     """``IEvaluatorNonLin`` backed by one ``bosss_handle``."""
 
-    def __init__(self, op, grid, dom_deg, cod_deg, bound, device, precision, check_nan):
+    def __init__(self, op, grid, dom_deg, cod_deg, bound, device, precision, check_nan, kernel=C.KERNEL_AUTO):
         self.handle = None
         self.op, self.grid = op, grid
         self.desc = op.descriptor(dom_deg, cod_deg, grid.dim)
         self.gdesc = grid.desc()
         opt = C.Options()
         opt.device, opt.precision, opt.check_nan = int(device), int(precision), int(bool(check_nan))
+        opt.kernel = int(kernel)
         h = ctypes.c_void_p()
         C.check(C.lib().bosss_b200_create(ctypes.byref(self.desc), ctypes.byref(self.gdesc), ctypes.byref(opt),
                                           ctypes.byref(h)))

@@ -71,6 +71,46 @@ def test_vjp_is_transposed_jacobian(name, make):
     assert rel(out, ref) <= TOL, rel(out, ref)
 
 
+EULER_VARIANTS = [(k, kern) for k in (1, 2, 3, 4) for kern in (C.KERNEL_GENERIC, C.KERNEL_SLAB)]
+
+
+@pytest.mark.parametrize("k,kernel", EULER_VARIANTS, ids=["k%d_%s" % (k, "slab" if v == 2 else "generic")
+                                                         for k, v in EULER_VARIANTS])
+def test_euler_kernel_variants(k, kernel):
+    """Both 3D kernels (generic fused and register-blocked slab) against the oracle:
+    residual with alpha/beta, JVP, and VJP vs the transposed Jacobian."""
+    pr = P.euler3d(n=3, k=k, seed=50 + k)
+    opd, gd = pr.descs()
+    r = np.random.default_rng(8)
+    V = r.uniform(-1, 1, pr.n_dofs)
+    W = r.uniform(-1, 1, pr.n_dofs)
+    out0 = r.uniform(-1, 1, pr.n_dofs)
+    ref = orc.evaluate(opd, gd, pr.U, alpha=0.5, beta=-1.5, out=out0)
+    jref = orc.jvp(opd, gd, pr.U, V)
+    A = orc.jacobian_dense(opd, gd, pr.U) if k <= 2 else None
+    with pr.evaluator(kernel=kernel) as ev:
+        out = out0.copy()
+        ev.Evaluate(0.5, -1.5, out, pr.U)
+        jv = ev.jvp(pr.U, V)
+        jtw = ev.vjp(pr.U, W)
+    assert rel(out, ref) <= TOL
+    assert rel(jv, jref) <= TOL
+    if A is not None:
+        assert rel(jtw, A.T @ W) <= TOL
+    assert abs(W @ jv - jtw @ V) <= 1e-12 * np.linalg.norm(W) * np.linalg.norm(jv)
+
+
+def test_euler_full_size_slab_matches_generic():
+    pr = P.euler3d(n=32, k=3, seed=2000)
+    W = np.random.default_rng(9).uniform(-1, 1, pr.n_dofs)
+    with pr.evaluator(kernel=C.KERNEL_GENERIC) as e1, pr.evaluator(kernel=C.KERNEL_SLAB) as e2:
+        r1, r2 = np.zeros(pr.n_dofs), np.zeros(pr.n_dofs)
+        e1.Evaluate(1.0, 0.0, r1, pr.U)
+        e2.Evaluate(1.0, 0.0, r2, pr.U)
+        g1, g2 = e1.vjp(pr.U, W), e2.vjp(pr.U, W)
+    assert rel(r2, r1) <= TOL and rel(g2, g1) <= TOL
+
+
 def test_alpha_beta_semantics():
     pr = P.euler3d(n=3, k=2, seed=40)
     r = np.random.default_rng(3)
