@@ -29,6 +29,12 @@ struct SlabCfg {
     static constexpr int NP = B::NP, NV = B::NV, NC = B::NC, NFI = B::NFI, NCI = B::NCI, NO = B::NO;
     static constexpr int NPAIR = B::NPAIR, NS = B::NS;
     static constexpr bool GRAD_IN = B::GRAD_IN;
+    // which interpolated groups actually need gradients: the state (and the JVP
+    // direction) only if the forms read grad u; the VJP adjoint only where test-function
+    // gradients enter (volume: VOL_G, faces: FACE_G)
+    static constexpr bool G_STATE = Phys::GRAD_U;
+    static constexpr bool G_SECOND_VOL = (MODE == MODE_VJP) ? Phys::VOL_G : Phys::GRAD_U;
+    static constexpr bool G_SECOND_FACE = (MODE == MODE_VJP) ? Phys::FACE_G : Phys::GRAD_U;
     static constexpr bool VOL_OV = B::VOL_OV, VOL_OG = B::VOL_OG, FACE_OV = B::FACE_OV, FACE_OG = B::FACE_OG;
     static constexpr int NCOV = (VOL_OV ? 1 : 0) + (VOL_OG ? 3 : 0);
     static constexpr int NCOF = (FACE_OV ? 1 : 0) + (FACE_OG ? 3 : 0);
@@ -499,7 +505,10 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
                 double cf[NP];
 #pragma unroll
                 for (int n = 0; n < NP; ++n) cf[n] = CIN(cl)[f * NP + n];
-                slab_interp<K, Q, GI>(T, cf, Aq, dAq, q, g.scaling, g.twoh, WK(cl) + f * NCI * FV);
+                if ((f < NV) ? C::G_STATE : C::G_SECOND_VOL)
+                    slab_interp<K, Q, GI>(T, cf, Aq, dAq, q, g.scaling, g.twoh, WK(cl) + f * NCI * FV);
+                else
+                    slab_interp<K, Q, false>(T, cf, Aq, dAq, q, g.scaling, g.twoh, WK(cl) + f * NCI * FV);
             }
         }
         __syncthreads();
@@ -544,10 +553,13 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
                 double cf[NP];
 #pragma unroll
                 for (int n = 0; n < NP; ++n) cf[n] = CIN(cl)[f * NP + n];
+                const bool fg = (f < NV) ? C::G_STATE : C::G_SECOND_FACE;
 #pragma unroll
-                for (int s = 0; s < 2; ++s)
-                    face_interp<DIR, K, Q, GI>(T, cf, s, Aq, dAq, g.scaling, g.twoh,
-                                               WK(cl) + (s * 2 + 0) * TRB + f * NCI * FF + q * SLF);
+                for (int s = 0; s < 2; ++s) {
+                    double* tb = WK(cl) + (s * 2 + 0) * TRB + f * NCI * FF + q * SLF;
+                    if (fg) face_interp<DIR, K, Q, GI>(T, cf, s, Aq, dAq, g.scaling, g.twoh, tb);
+                    else face_interp<DIR, K, Q, false>(T, cf, s, Aq, dAq, g.scaling, g.twoh, tb);
+                }
 #pragma unroll
                 for (int s = 0; s < 2; ++s) {
                     const long long nb = neighbour(g, ijk, DIR, s);
@@ -560,8 +572,9 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
 #pragma unroll
                         for (int n = 0; n < NP; ++n) cn[n] = 0.0;
                     }
-                    face_interp<DIR, K, Q, GI>(T, cn, 1 - s, Aq, dAq, g.scaling, g.twoh,
-                                               WK(cl) + (s * 2 + 1) * TRB + f * NCI * FF + q * SLF);
+                    double* tb = WK(cl) + (s * 2 + 1) * TRB + f * NCI * FF + q * SLF;
+                    if (fg) face_interp<DIR, K, Q, GI>(T, cn, 1 - s, Aq, dAq, g.scaling, g.twoh, tb);
+                    else face_interp<DIR, K, Q, false>(T, cn, 1 - s, Aq, dAq, g.scaling, g.twoh, tb);
                 }
             }
         }
