@@ -7,7 +7,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libbosss_b200.so")
+# BOSSS_B200_LIB selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("BOSSS_B200_LIB") or os.path.join(HERE, "libbosss_b200.so")
 
 MAX_VARS = 8
 MAX_COMPONENTS = 32

@@ -55,7 +55,7 @@ cudaError_t launch_slab_kernel(const EvalArgs& a, cudaStream_t s) {
 template <class Phys, int K, int Q, int MODE>
 void reg_slab_one(int phys) {
     using C = SlabCfg<Phys, K, Q, MODE>;
-    if constexpr (C::SMEM_BYTES <= 227 * 1024 && C::NT <= 256) {
+    if constexpr (C::SMEM_BYTES <= 227 * 1024 && C::NT <= 512) {
         kernel_registry()[KernelKey(phys, 3, K, Q, MODE, VARIANT_SLAB)] =
             KernelEntry{&launch_slab_kernel<Phys, K, Q, MODE>, C::CPB, C::SMEM_BYTES};
     }

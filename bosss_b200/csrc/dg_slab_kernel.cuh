@@ -26,39 +26,71 @@ struct SlabCfg {
     using B = Cfg<Phys, K, Q, MODE>;
     static constexpr int D = 3;
     static_assert(Phys::D == 3, "slab kernel is three-dimensional");
-    static constexpr int NP = B::NP, NV = B::NV, NC = B::NC, NFI = B::NFI, NCI = B::NCI, NO = B::NO;
+    static constexpr int NP = B::NP, NV = B::NV, NC = B::NC, NFI = B::NFI, NO = B::NO, NF1 = B::NF1;
     static constexpr int NPAIR = B::NPAIR, NS = B::NS;
-    static constexpr bool GRAD_IN = B::GRAD_IN;
-    // which interpolated groups actually need gradients: the state (and the JVP
-    // direction) only if the forms read grad u; the VJP adjoint only where test-function
-    // gradients enter (volume: VOL_G, faces: FACE_G)
+    static constexpr bool VOL_OV = B::VOL_OV, VOL_OG = B::VOL_OG, FACE_OV = B::FACE_OV, FACE_OG = B::FACE_OG;
+    // which interpolated groups need gradients: the state (and the JVP direction) only
+    // if the forms read grad u; the VJP adjoint only where test-function gradients enter
     static constexpr bool G_STATE = Phys::GRAD_U;
     static constexpr bool G_SECOND_VOL = (MODE == MODE_VJP) ? Phys::VOL_G : Phys::GRAD_U;
     static constexpr bool G_SECOND_FACE = (MODE == MODE_VJP) ? Phys::FACE_G : Phys::GRAD_U;
-    static constexpr bool VOL_OV = B::VOL_OV, VOL_OG = B::VOL_OG, FACE_OV = B::FACE_OV, FACE_OG = B::FACE_OG;
+    static constexpr int NCI0 = G_STATE ? 4 : 1;
+    static constexpr int NCI1V = G_SECOND_VOL ? 4 : 1;
+    static constexpr int NCI1F = G_SECOND_FACE ? 4 : 1;
     static constexpr int NCOV = (VOL_OV ? 1 : 0) + (VOL_OG ? 3 : 0);
     static constexpr int NCOF = (FACE_OV ? 1 : 0) + (FACE_OG ? 3 : 0);
-    static constexpr int GOV = VOL_OV ? 1 : 0;    // first gradient comp of volume outputs
-    static constexpr int GOF = FACE_OV ? 1 : 0;
     static constexpr int SLV = Q * Q + 1;          // padded volume slab
     static constexpr int FV = Q * SLV;             // one (field, comp) volume block
     static constexpr int SLF = Q + 1;              // padded face row
     static constexpr int FF = Q * SLF;             // one (field, comp) face block
-    static constexpr int TPC = NO * Q;             // threads per cell
+    // work split of a slab over SPLIT warp-uniform parts: volume rows qy = part mod SPLIT,
+    // faces: part s handles the lower (s=0) / upper (s=1) face. Measured on B200 (Euler
+    // k=3): the split pays for the register-heavy VJP (more resident warps), not for the
+    // residual/JVP
+    static constexpr int SPLIT = (MODE == MODE_VJP && Q >= 3) ? 2 : 1;
+    static constexpr int TPC = NO * Q * SPLIT;     // threads per cell
+    static constexpr int NODEV = (NV * NCI0 + NF1 * NCI1V) * FV;   // interpolated node values
     static constexpr int S_CIN = NFI * NP;
-    static constexpr int S_VOL = NFI * NCI * FV + NO * NCOV * FV;
-    static constexpr int S_FACE = 2 * 2 * NFI * NCI * FF + 2 * NO * NCOF * FF;
-    static constexpr int S_RED = NO * Q * NP;
+    static constexpr int S_VOL = NODEV + NO * NCOV * FV;
+    static constexpr int TRB = (NV * NCI0 + NF1 * NCI1F) * FF;      // one (face, side) trace block
+    static constexpr int S_FACE = 2 * 2 * TRB + 2 * NO * NCOF * FF;
+    static constexpr int S_RED = NO * SPLIT * Q * NP;
     static constexpr int S_W0 = S_VOL > S_FACE ? S_VOL : S_FACE;
     static constexpr int S_WORK = S_W0 > S_RED ? S_W0 : S_RED;
     static constexpr int S_CELL = S_CIN + S_WORK;
     static constexpr int BUDGET = 110 * 1024 / 8;
     static constexpr int CPB_SMEM = BUDGET / S_CELL;
-    static constexpr int CPB_THR = 256 / TPC;
-    static constexpr int CPB0 = CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR;
-    static constexpr int CPB = CPB0 < 1 ? 1 : CPB0;
+    // threads per block target and minimum resident blocks per SM (register budget):
+    // tuned on B200 for the Euler k=3 tile (profiles/)
+#ifndef BOSSS_SLAB_THREADS
+#define BOSSS_SLAB_THREADS 256
+#endif
+#ifndef BOSSS_SLAB_THREADS_VJP
+#define BOSSS_SLAB_THREADS_VJP 128
+#endif
+#ifndef BOSSS_SLAB_MINB
+#define BOSSS_SLAB_MINB 1
+#endif
+#ifndef BOSSS_SLAB_MINB_VJP
+#define BOSSS_SLAB_MINB_VJP 2
+#endif
+    static constexpr int CPB_THR = ((MODE == MODE_VJP) ? BOSSS_SLAB_THREADS_VJP : BOSSS_SLAB_THREADS) / TPC;
+    static constexpr int MINB = (MODE == MODE_VJP) ? BOSSS_SLAB_MINB_VJP : BOSSS_SLAB_MINB;
+    static constexpr int CPB_MAX = (CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR) < 1 ? 1
+                                   : (CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR);
+    // prefer a tile whose half-block is a whole number of warps (warp-uniform parts)
+    static constexpr int pick_cpb() {
+        for (int c = CPB_MAX; c >= 1; --c)
+            if ((c * NO * Q) % 32 == 0) return c;
+        return CPB_MAX;
+    }
+    static constexpr int CPB = pick_cpb();
+    static constexpr int HALF = CPB * NO * Q;
     static constexpr int NT = CPB * TPC;
     static constexpr size_t SMEM_BYTES = (size_t)CPB * S_CELL * 8;
+    // offset of field f's first comp block
+    __host__ __device__ static constexpr int vnode(int f) { return f < NV ? f * NCI0 * FV : (NV * NCI0 + (f - NV) * NCI1V) * FV; }
+    __host__ __device__ static constexpr int fnode(int f) { return f < NV ? f * NCI0 * FF : (NV * NCI0 + (f - NV) * NCI1F) * FF; }
 };
 
 template <int DIR> struct FaceDirs {
@@ -74,18 +106,17 @@ __host__ __device__ constexpr int mode_dpr(int m, int p, int r) {
 // ------------------------------------------------------------------ pointwise helpers
 // Volume node: in(f, comp) reads interpolated fields, out(o, c, v) stores projected
 // coefficients (c = 0: test function, 1+d: gradient d) already scaled by `fac` and 2/h.
-template <class Phys, int MODE, int NCI, bool OV, bool OG, class In, class Out>
+template <class Phys, int MODE, bool GS, bool G2, bool OV, bool OG, class In, class Out>
 __device__ __forceinline__ void volume_point(const PhysParams& ph, const double* x, double fac,
                                              const double* twoh, In in, Out out) {
     constexpr int D = Phys::D, NV = Phys::NV, NC = Phys::NC;
-    constexpr bool G = NCI > 1;
     if constexpr (MODE == MODE_RES) {
         double U[NV], Gr[NV][D], fV[NC], fG[NC][D];
 #pragma unroll
         for (int i = 0; i < NV; ++i) {
             U[i] = in(i, 0);
 #pragma unroll
-            for (int d = 0; d < D; ++d) Gr[i][d] = G ? in(i, 1 + d) : 0.0;
+            for (int d = 0; d < D; ++d) Gr[i][d] = GS ? in(i, 1 + d) : 0.0;
         }
 #pragma unroll
         for (int e = 0; e < NC; ++e) {
@@ -110,8 +141,8 @@ __device__ __forceinline__ void volume_point(const PhysParams& ph, const double*
             U[i].d[0] = in(NV + i, 0);
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                Gr[i][d].v = G ? in(i, 1 + d) : 0.0;
-                Gr[i][d].d[0] = G ? in(NV + i, 1 + d) : 0.0;
+                Gr[i][d].v = GS ? in(i, 1 + d) : 0.0;
+                Gr[i][d].d[0] = (GS && G2) ? in(NV + i, 1 + d) : 0.0;
             }
         }
         Phys::volume(ph, U, Gr, x, fV, fG);
@@ -132,7 +163,7 @@ __device__ __forceinline__ void volume_point(const PhysParams& ph, const double*
             U[i].d[Phys::GRAD_U ? i * (1 + D) : i] = 1.0;
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                Gr[i][d] = T(G ? in(i, 1 + d) : 0.0);
+                Gr[i][d] = T(GS ? in(i, 1 + d) : 0.0);
                 if (Phys::GRAD_U) Gr[i][d].d[i * (1 + D) + 1 + d] = 1.0;
             }
         }
@@ -141,7 +172,7 @@ __device__ __forceinline__ void volume_point(const PhysParams& ph, const double*
 #pragma unroll
         for (int e = 0; e < NC; ++e) {
             if (Phys::VOL_V) phi += fV[e] * in(NV + e, 0);
-            if (Phys::VOL_G)
+            if (Phys::VOL_G && G2)
 #pragma unroll
                 for (int d = 0; d < D; ++d) phi += fG[e][d] * in(NV + e, 1 + d);
         }
@@ -157,12 +188,11 @@ __device__ __forceinline__ void volume_point(const PhysParams& ph, const double*
 
 // Face node: inA/inB read the traces of the IN (lower) and OUT (upper) cell,
 // out(o, c, v) stores the own side's coefficients.
-template <class Phys, int MODE, int NCI, bool OV, bool OG, class InA, class InB, class Out>
+template <class Phys, int MODE, bool GS, bool G2, bool OV, bool OG, class InA, class InB, class Out>
 __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, bool selfA, double pnlty,
                                            const double* nrm, const double* x, double fac, const double* twoh,
                                            InA inA, InB inB, Out out) {
     constexpr int D = Phys::D, NV = Phys::NV, NC = Phys::NC;
-    constexpr bool G = NCI > 1;
     if constexpr (MODE == MODE_RES) {
         double UA[NV], GA[NV][D], UB[NV], GB[NV][D], gA[NC], GAv[NC][D], gB[NC], GBv[NC][D];
 #pragma unroll
@@ -171,8 +201,8 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
             UB[i] = inner ? inB(i, 0) : 0.0;
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                GA[i][d] = G ? inA(i, 1 + d) : 0.0;
-                GB[i][d] = (G && inner) ? inB(i, 1 + d) : 0.0;
+                GA[i][d] = GS ? inA(i, 1 + d) : 0.0;
+                GB[i][d] = (GS && inner) ? inB(i, 1 + d) : 0.0;
             }
         }
 #pragma unroll
@@ -201,10 +231,10 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
             UB[i].d[0] = inner ? inB(NV + i, 0) : 0.0;
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                GA[i][d].v = G ? inA(i, 1 + d) : 0.0;
-                GA[i][d].d[0] = G ? inA(NV + i, 1 + d) : 0.0;
-                GB[i][d].v = (G && inner) ? inB(i, 1 + d) : 0.0;
-                GB[i][d].d[0] = (G && inner) ? inB(NV + i, 1 + d) : 0.0;
+                GA[i][d].v = GS ? inA(i, 1 + d) : 0.0;
+                GA[i][d].d[0] = (GS && G2) ? inA(NV + i, 1 + d) : 0.0;
+                GB[i][d].v = (GS && inner) ? inB(i, 1 + d) : 0.0;
+                GB[i][d].d[0] = (GS && G2 && inner) ? inB(NV + i, 1 + d) : 0.0;
             }
         }
         if (inner) Phys::inner(ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
@@ -227,8 +257,8 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
             UB[i] = T(inner ? inB(i, 0) : 0.0);
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                GA[i][d] = T(G ? inA(i, 1 + d) : 0.0);
-                GB[i][d] = T((G && inner) ? inB(i, 1 + d) : 0.0);
+                GA[i][d] = T(GS ? inA(i, 1 + d) : 0.0);
+                GB[i][d] = T((GS && inner) ? inB(i, 1 + d) : 0.0);
             }
             (selfA ? UA[i] : UB[i]).d[Phys::GRAD_U ? i * (1 + D) : i] = 1.0;
             if (Phys::GRAD_U)
@@ -245,7 +275,7 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
                 phi += gA[e] * inA(fe, 0);
                 if (inner) phi += gB[e] * inB(fe, 0);
             }
-            if (Phys::FACE_G)
+            if (Phys::FACE_G && G2)
 #pragma unroll
                 for (int d = 0; d < D; ++d) {
                     phi += GAv[e][d] * inA(fe, 1 + d);
@@ -264,7 +294,7 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
 
 // ------------------------------------------------------------------ contraction helpers
 // interpolation of one field at the slab qz = q (Q*Q nodes), into node block `nb`
-template <int K, int Q, bool GRAD>
+template <int K, int Q, bool GRAD, int PART, int SPLIT>
 __device__ __forceinline__ void slab_interp(const Tables1D& T, const double* cf, const double* Az, const double* dAz,
                                             int q, double scaling, const double* twoh, double* nb) {
     constexpr int NPAIR = (K + 1) * (K + 2) / 2;
@@ -286,7 +316,7 @@ __device__ __forceinline__ void slab_interp(const Tables1D& T, const double* cf,
         }
     double* base = nb + q * SLV;
 #pragma unroll
-    for (int qy = 0; qy < Q; ++qy) {
+    for (int qy = PART; qy < Q; qy += SPLIT) {
         double T2[K + 1], T2y[K + 1], T2z[K + 1];
 #pragma unroll
         for (int a = 0; a <= K; ++a) {
@@ -327,7 +357,7 @@ __device__ __forceinline__ void slab_interp(const Tables1D& T, const double* cf,
 }
 
 // projection of the slab qz = q of one output field (block `ob`, comps) into R[NP]
-template <int K, int Q, bool OV, bool OG>
+template <int K, int Q, bool OV, bool OG, int PART, int SPLIT>
 __device__ __forceinline__ void slab_project(const Tables1D& T, const double* ob, const double* Az, const double* dAz,
                                              int q, double* R) {
     constexpr int NPAIR = (K + 1) * (K + 2) / 2;
@@ -338,7 +368,7 @@ __device__ __forceinline__ void slab_project(const Tables1D& T, const double* ob
     for (int i = 0; i < NPAIR; ++i) P2[i] = P2z[i] = 0.0;
     const double* base = ob + q * SLV;
 #pragma unroll
-    for (int qy = 0; qy < Q; ++qy) {
+    for (int qy = PART; qy < Q; qy += SPLIT) {
         double P[K + 1], Py[K + 1], Pz[K + 1];
 #pragma unroll
         for (int a = 0; a <= K; ++a) P[a] = Py[a] = Pz[a] = 0.0;
@@ -458,29 +488,76 @@ __device__ __forceinline__ void face_project(const Tables1D& T, const double* ob
 }
 
 // ------------------------------------------------------------------ the kernel
+template <class Phys, int K, int Q, int MODE, int PART>
+__device__ __forceinline__ void slab_volume_interp(const EvalArgs& args, const double* cin, double* wk, int o, int q,
+                                                   const double* Aq, const double* dAq) {
+    using C = SlabCfg<Phys, K, Q, MODE>;
+    constexpr int NP = C::NP;
+    for (int f = o; f < C::NFI; f += C::NO) {
+        double cf[NP];
+#pragma unroll
+        for (int n = 0; n < NP; ++n) cf[n] = cin[f * NP + n];
+        double* nb = wk + C::vnode(f);
+        if (f < C::NV) slab_interp<K, Q, C::G_STATE, PART, C::SPLIT>(args.tab, cf, Aq, dAq, q, args.g.scaling, args.g.twoh, nb);
+        else slab_interp<K, Q, C::G_SECOND_VOL, PART, C::SPLIT>(args.tab, cf, Aq, dAq, q, args.g.scaling, args.g.twoh, nb);
+    }
+}
+
+// traces of all interpolated fields at face (DIR, s): own (side 0) and neighbour (side 1)
+template <class Phys, int K, int Q, int MODE, int DIR, int S>
+__device__ __forceinline__ void slab_face_traces(const EvalArgs& args, const double* cin, double* wk, int o, int q,
+                                                 const int* ijk, const double* Aq, const double* dAq) {
+    using C = SlabCfg<Phys, K, Q, MODE>;
+    constexpr int NP = C::NP, NV = C::NV, SLF = C::SLF;
+    const long long nb = neighbour(args.g, ijk, DIR, S);
+    for (int f = o; f < C::NFI; f += C::NO) {
+        double cf[NP], cn[NP];
+#pragma unroll
+        for (int n = 0; n < NP; ++n) cf[n] = cin[f * NP + n];
+        if (nb >= 0) {
+            const double* src = (f < NV) ? args.U + nb * (NV * NP) + f * NP : args.V + nb * (C::NF1 * NP) + (f - NV) * NP;
+#pragma unroll
+            for (int n = 0; n < NP; ++n) cn[n] = __ldg(src + n);
+        } else {
+#pragma unroll
+            for (int n = 0; n < NP; ++n) cn[n] = 0.0;
+        }
+        double* t0 = wk + (S * 2 + 0) * C::TRB + C::fnode(f) + q * SLF;
+        double* t1 = wk + (S * 2 + 1) * C::TRB + C::fnode(f) + q * SLF;
+        if (f < NV ? C::G_STATE : C::G_SECOND_FACE) {
+            constexpr bool GG = C::G_STATE || C::G_SECOND_FACE;
+            face_interp<DIR, K, Q, GG>(args.tab, cf, S, Aq, dAq, args.g.scaling, args.g.twoh, t0);
+            face_interp<DIR, K, Q, GG>(args.tab, cn, 1 - S, Aq, dAq, args.g.scaling, args.g.twoh, t1);
+        } else {
+            face_interp<DIR, K, Q, false>(args.tab, cf, S, Aq, dAq, args.g.scaling, args.g.twoh, t0);
+            face_interp<DIR, K, Q, false>(args.tab, cn, 1 - S, Aq, dAq, args.g.scaling, args.g.twoh, t1);
+        }
+    }
+}
+
 template <class Phys, int K, int Q, int MODE>
-__global__ void __launch_bounds__(SlabCfg<Phys, K, Q, MODE>::NT)
+__global__ void __launch_bounds__(SlabCfg<Phys, K, Q, MODE>::NT, SlabCfg<Phys, K, Q, MODE>::MINB)
 dg_slab_kernel(const __grid_constant__ EvalArgs args) {
     using C = SlabCfg<Phys, K, Q, MODE>;
-    constexpr int NP = C::NP, NV = C::NV, NFI = C::NFI, NCI = C::NCI, NO = C::NO, CPB = C::CPB, NT = C::NT;
+    constexpr int NP = C::NP, NV = C::NV, NO = C::NO, CPB = C::CPB, NT = C::NT, SPLIT = C::SPLIT;
     constexpr int SLV = C::SLV, FV = C::FV, SLF = C::SLF, FF = C::FF, QF = Q * Q;
-    constexpr bool GI = C::GRAD_IN;
     extern __shared__ double smem[];
     const GridConst& g = args.g;
     const Tables1D& T = args.tab;
     const int tid = threadIdx.x;
     const long long c0 = (long long)blockIdx.x * CPB;
     const int ncell = (int)((g.J - c0) < CPB ? (g.J - c0) : CPB);
-    // own (cell, output field, slab)
-    const int q = tid % Q, o = (tid / Q) % NO, cl = tid / (Q * NO);
+    // own (part, cell, output field, slab); part is warp-uniform when HALF % 32 == 0
+    const int part = tid / C::HALF, r0 = tid % C::HALF;
+    const int q = r0 % Q, o = (r0 / Q) % NO, cl = r0 / (Q * NO);
     const bool active = cl < ncell;
     auto CIN = [&](int c) { return smem + (size_t)c * C::S_CELL; };
     auto WK = [&](int c) { return smem + (size_t)c * C::S_CELL + C::S_CIN; };
 
     constexpr int NVPC = NV * NP;
-    constexpr int N1PC = C::B::NF1 * NP;
+    constexpr int N1PC = C::NF1 * NP;
     for (int i = tid; i < ncell * NVPC; i += NT) CIN(i / NVPC)[i % NVPC] = args.U[c0 * NVPC + i];
-    if constexpr (C::B::NF1 > 0)
+    if constexpr (C::NF1 > 0)
         for (int i = tid; i < ncell * N1PC; i += NT) CIN(i / N1PC)[NVPC + i % N1PC] = args.V[c0 * N1PC + i];
 
     double Aq[K + 1], dAq[K + 1];
@@ -497,85 +574,55 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
     __syncthreads();
 
     // ---------------------------------------------------------- volume
-    {
-        double* nodes = nullptr;
-        (void)nodes;
-        if (active) {
-            for (int f = o; f < NFI; f += NO) {
-                double cf[NP];
-#pragma unroll
-                for (int n = 0; n < NP; ++n) cf[n] = CIN(cl)[f * NP + n];
-                if ((f < NV) ? C::G_STATE : C::G_SECOND_VOL)
-                    slab_interp<K, Q, GI>(T, cf, Aq, dAq, q, g.scaling, g.twoh, WK(cl) + f * NCI * FV);
-                else
-                    slab_interp<K, Q, false>(T, cf, Aq, dAq, q, g.scaling, g.twoh, WK(cl) + f * NCI * FV);
-            }
-        }
-        __syncthreads();
-        constexpr int OUT0 = NFI * NCI * FV;
-        for (int it = tid; it < CPB * Q * Q * Q; it += NT) {
-            const int n = it % (Q * Q * Q), c = it / (Q * Q * Q);
-            if (c >= ncell) continue;
-            const int qx = n % Q, qy = (n / Q) % Q, qz = n / (Q * Q);
-            const int off = qz * SLV + qy * Q + qx;
-            int cijk[3];
-            cell_ijk(g, c0 + c, cijk);
-            double x[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) x[d] = g.lo[d] + (cijk[d] + 0.5) * g.h[d];
-            x[0] += 0.5 * g.h[0] * T.xq[qx];
-            x[1] += 0.5 * g.h[1] * T.xq[qy];
-            x[2] += 0.5 * g.h[2] * T.xq[qz];
-            const double fac = T.w[qx] * T.w[qy] * T.w[qz] * g.detJ * g.scaling;
-            const double* nb = WK(c);
-            double* ob = WK(c) + OUT0;
-            volume_point<Phys, MODE, NCI, C::VOL_OV, C::VOL_OG>(
-                args.ph, x, fac, g.twoh, [&](int f, int comp) { return nb[(f * NCI + comp) * FV + off]; },
-                [&](int oo, int comp, double v) {
-                    const int cc = C::VOL_OV ? comp : comp - 1;
-                    ob[(oo * C::NCOV + cc) * FV + off] = v;
-                });
-        }
-        __syncthreads();
-        if (active) slab_project<K, Q, C::VOL_OV, C::VOL_OG>(T, WK(cl) + OUT0 + o * C::NCOV * FV, Aq, dAq, q, R);
-        __syncthreads();
+    constexpr int OUT0 = C::NODEV;
+    if (active) {
+        if (part == 0) slab_volume_interp<Phys, K, Q, MODE, 0>(args, CIN(cl), WK(cl), o, q, Aq, dAq);
+        else if constexpr (SPLIT > 1) slab_volume_interp<Phys, K, Q, MODE, 1>(args, CIN(cl), WK(cl), o, q, Aq, dAq);
     }
+    __syncthreads();
+    for (int it = tid; it < CPB * Q * Q * Q; it += NT) {
+        const int n = it % (Q * Q * Q), c = it / (Q * Q * Q);
+        if (c >= ncell) continue;
+        const int qx = n % Q, qy = (n / Q) % Q, qz = n / (Q * Q);
+        const int off = qz * SLV + qy * Q + qx;
+        int cijk[3];
+        cell_ijk(g, c0 + c, cijk);
+        double x[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) x[d] = g.lo[d] + (cijk[d] + 0.5) * g.h[d];
+        x[0] += 0.5 * g.h[0] * T.xq[qx];
+        x[1] += 0.5 * g.h[1] * T.xq[qy];
+        x[2] += 0.5 * g.h[2] * T.xq[qz];
+        const double fac = T.w[qx] * T.w[qy] * T.w[qz] * g.detJ * g.scaling;
+        const double* nb = WK(c);
+        double* ob = WK(c) + OUT0;
+        volume_point<Phys, MODE, C::G_STATE, C::G_SECOND_VOL, C::VOL_OV, C::VOL_OG>(
+            args.ph, x, fac, g.twoh, [&](int f, int comp) { return nb[C::vnode(f) + comp * FV + off]; },
+            [&](int oo, int comp, double v) {
+                const int cc = C::VOL_OV ? comp : comp - 1;
+                ob[(oo * C::NCOV + cc) * FV + off] = v;
+            });
+    }
+    __syncthreads();
+    if (active) {
+        const double* ob = WK(cl) + OUT0 + o * C::NCOV * FV;
+        if (part == 0) slab_project<K, Q, C::VOL_OV, C::VOL_OG, 0, SPLIT>(T, ob, Aq, dAq, q, R);
+        else if constexpr (SPLIT > 1) slab_project<K, Q, C::VOL_OV, C::VOL_OG, 1, SPLIT>(T, ob, Aq, dAq, q, R);
+    }
+    __syncthreads();
 
     // ---------------------------------------------------------- faces
     auto face_pass = [&](auto dirc) {
         constexpr int DIR = decltype(dirc)::value;
         constexpr int t1 = FaceDirs<DIR>::t1, t2 = FaceDirs<DIR>::t2;
-        constexpr int TRB = NFI * NCI * FF;     // one (s, side) trace block
-        constexpr int OUTF0 = 2 * 2 * TRB;
-        // traces: own side 0, neighbour side 1, faces s = 0 (lower), 1 (upper)
+        constexpr int OUTF0 = 2 * 2 * C::TRB;
         if (active) {
-            for (int f = o; f < NFI; f += NO) {
-                double cf[NP];
-#pragma unroll
-                for (int n = 0; n < NP; ++n) cf[n] = CIN(cl)[f * NP + n];
-                const bool fg = (f < NV) ? C::G_STATE : C::G_SECOND_FACE;
-#pragma unroll
-                for (int s = 0; s < 2; ++s) {
-                    double* tb = WK(cl) + (s * 2 + 0) * TRB + f * NCI * FF + q * SLF;
-                    if (fg) face_interp<DIR, K, Q, GI>(T, cf, s, Aq, dAq, g.scaling, g.twoh, tb);
-                    else face_interp<DIR, K, Q, false>(T, cf, s, Aq, dAq, g.scaling, g.twoh, tb);
-                }
-#pragma unroll
-                for (int s = 0; s < 2; ++s) {
-                    const long long nb = neighbour(g, ijk, DIR, s);
-                    double cn[NP];
-                    if (nb >= 0) {
-                        const double* src = (f < NV) ? args.U + nb * NVPC + f * NP : args.V + nb * N1PC + (f - NV) * NP;
-#pragma unroll
-                        for (int n = 0; n < NP; ++n) cn[n] = __ldg(src + n);
-                    } else {
-#pragma unroll
-                        for (int n = 0; n < NP; ++n) cn[n] = 0.0;
-                    }
-                    double* tb = WK(cl) + (s * 2 + 1) * TRB + f * NCI * FF + q * SLF;
-                    if (fg) face_interp<DIR, K, Q, GI>(T, cn, 1 - s, Aq, dAq, g.scaling, g.twoh, tb);
-                    else face_interp<DIR, K, Q, false>(T, cn, 1 - s, Aq, dAq, g.scaling, g.twoh, tb);
-                }
+            if constexpr (SPLIT > 1) {
+                if (part == 0) slab_face_traces<Phys, K, Q, MODE, DIR, 0>(args, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
+                else slab_face_traces<Phys, K, Q, MODE, DIR, 1>(args, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
+            } else {
+                slab_face_traces<Phys, K, Q, MODE, DIR, 0>(args, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
+                slab_face_traces<Phys, K, Q, MODE, DIR, 1>(args, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
             }
         }
         __syncthreads();
@@ -586,8 +633,8 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
             const int off = q2 * SLF + q1;
             int cijk[3];
             cell_ijk(g, c0 + c, cijk);
-            const long long nb = neighbour(g, cijk, DIR, s);
-            const bool inner = nb >= 0;
+            const long long nbc = neighbour(g, cijk, DIR, s);
+            const bool inner = nbc >= 0;
             double x[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) x[d] = g.lo[d] + (cijk[d] + 0.5) * g.h[d];
@@ -599,22 +646,22 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
             double pnlty;
             if (inner) {
                 int ijk2[3] = {cijk[0], cijk[1], cijk[2]};
-                ijk2[DIR] = (int)((nb / g.stride[DIR]) % g.n[DIR]);
+                ijk2[DIR] = (int)((nbc / g.stride[DIR]) % g.n[DIR]);
                 pnlty = args.ph.pen * fmax(cell_cj(g, cijk), cell_cj(g, ijk2));
             } else {
                 pnlty = 2.0 * args.ph.pen * cell_cj(g, cijk);
             }
             const bool selfA = !inner || s == 1;
-            const double* trOwn = WK(c) + (s * 2 + 0) * TRB;
-            const double* trNb = WK(c) + (s * 2 + 1) * TRB;
+            const double* trOwn = WK(c) + (s * 2 + 0) * C::TRB;
+            const double* trNb = WK(c) + (s * 2 + 1) * C::TRB;
             const double* trA = selfA ? trOwn : trNb;
             const double* trB = selfA ? trNb : trOwn;
             double* ob = WK(c) + OUTF0 + s * NO * C::NCOF * FF;
             const double fac = T.w[q1] * T.w[q2] * g.faceSG[DIR] * g.scaling;
-            face_point<Phys, MODE, NCI, C::FACE_OV, C::FACE_OG>(
+            face_point<Phys, MODE, C::G_STATE, C::G_SECOND_FACE, C::FACE_OV, C::FACE_OG>(
                 args.ph, inner, selfA, pnlty, nrm, x, fac, g.twoh,
-                [&](int f, int comp) { return trA[(f * NCI + comp) * FF + off]; },
-                [&](int f, int comp) { return trB[(f * NCI + comp) * FF + off]; },
+                [&](int f, int comp) { return trA[C::fnode(f) + comp * FF + off]; },
+                [&](int f, int comp) { return trB[C::fnode(f) + comp * FF + off]; },
                 [&](int oo, int comp, double v) {
                     const int cc = C::FACE_OV ? comp : comp - 1;
                     ob[(oo * C::NCOF + cc) * FF + off] = v;
@@ -622,10 +669,18 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
         }
         __syncthreads();
         if (active) {
-#pragma unroll
-            for (int s = 0; s < 2; ++s)
+            auto proj = [&](auto sc) {
+                constexpr int S = decltype(sc)::value;
                 face_project<DIR, K, Q, C::FACE_OV, C::FACE_OG>(
-                    T, WK(cl) + OUTF0 + (s * NO + o) * C::NCOF * FF + q * SLF, s, Aq, dAq, R);
+                    T, WK(cl) + OUTF0 + (S * NO + o) * C::NCOF * FF + q * SLF, S, Aq, dAq, R);
+            };
+            if constexpr (SPLIT > 1) {
+                if (part == 0) proj(std::integral_constant<int, 0>{});
+                else proj(std::integral_constant<int, 1>{});
+            } else {
+                proj(std::integral_constant<int, 0>{});
+                proj(std::integral_constant<int, 1>{});
+            }
         }
         __syncthreads();
     };
@@ -633,25 +688,23 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
     face_pass(std::integral_constant<int, 1>{});
     face_pass(std::integral_constant<int, 2>{});
 
-    // ---------------------------------------------------------- reduce slabs and store
+    // ---------------------------------------------------------- reduce partials and store
     if (active) {
-        double* red = WK(cl) + (o * Q + q) * NP;
+        double* red = WK(cl) + ((o * SPLIT + part) * Q + q) * NP;
 #pragma unroll
         for (int n = 0; n < NP; ++n) red[n] = R[n];
     }
     __syncthreads();
-    if (active) {
-        const long long obase = (c0 + cl) * (long long)(NO * NP) + o * NP;
-        for (int n = q; n < NP; n += Q) {
-            double v = 0.0;
+    for (int it = tid; it < ncell * NO * NP; it += NT) {
+        const int n = it % NP, oo = (it / NP) % NO, c = it / (NP * NO);
+        double v = 0.0;
 #pragma unroll
-            for (int qq = 0; qq < Q; ++qq) v += WK(cl)[(o * Q + qq) * NP + n];
-            if constexpr (MODE == MODE_RES) {
-                args.out[obase + n] =
-                    (args.beta == 0.0) ? args.alpha * v : args.beta * args.out[obase + n] + args.alpha * v;
-            } else {
-                args.out[obase + n] = v;
-            }
+        for (int pq = 0; pq < SPLIT * Q; ++pq) v += WK(c)[(oo * SPLIT * Q + pq) * NP + n];
+        const long long gi = c0 * (long long)(NO * NP) + it;
+        if constexpr (MODE == MODE_RES) {
+            args.out[gi] = (args.beta == 0.0) ? args.alpha * v : args.beta * args.out[gi] + args.alpha * v;
+        } else {
+            args.out[gi] = v;
         }
     }
 }
