@@ -78,15 +78,11 @@ struct SlabCfg {
     static constexpr int MINB = (MODE == MODE_VJP) ? BOSSS_SLAB_MINB_VJP : BOSSS_SLAB_MINB;
     static constexpr int CPB_MAX = (CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR) < 1 ? 1
                                    : (CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR);
-    // prefer a tile whose half-block is a whole number of warps (warp-uniform parts)
-    static constexpr int pick_cpb() {
-        for (int c = CPB_MAX; c >= 1; --c)
-            if ((c * NO * Q) % 32 == 0) return c;
-        return CPB_MAX;
-    }
-    static constexpr int CPB = pick_cpb();
-    static constexpr int HALF = CPB * NO * Q;
-    static constexpr int NT = CPB * TPC;
+    static constexpr int CPB = CPB_MAX;
+    static constexpr int HALF = CPB * NO * Q;                 // threads of one part
+    // with SPLIT > 1 each part is padded to whole warps, so `part` is warp-uniform
+    static constexpr int HALFP = (SPLIT > 1) ? (HALF + 31) / 32 * 32 : HALF;
+    static constexpr int NT = SPLIT * HALFP;
     static constexpr size_t SMEM_BYTES = (size_t)CPB * S_CELL * 8;
     // offset of field f's first comp block
     __host__ __device__ static constexpr int vnode(int f) { return f < NV ? f * NCI0 * FV : (NV * NCI0 + (f - NV) * NCI1V) * FV; }
@@ -547,9 +543,9 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
     const int tid = threadIdx.x;
     const long long c0 = (long long)blockIdx.x * CPB;
     const int ncell = (int)((g.J - c0) < CPB ? (g.J - c0) : CPB);
-    // own (part, cell, output field, slab); part is warp-uniform when HALF % 32 == 0
-    const int part = tid / C::HALF, r0 = tid % C::HALF;
-    const int q = r0 % Q, o = (r0 / Q) % NO, cl = r0 / (Q * NO);
+    // own (part, cell, output field, slab); part is warp-uniform (parts padded to warps)
+    const int part = tid / C::HALFP, r0 = tid % C::HALFP;
+    const int q = r0 % Q, o = (r0 / Q) % NO, cl = (r0 < C::HALF) ? r0 / (Q * NO) : CPB;
     const bool active = cl < ncell;
     auto CIN = [&](int c) { return smem + (size_t)c * C::S_CELL; };
     auto WK = [&](int c) { return smem + (size_t)c * C::S_CELL + C::S_CIN; };
