@@ -17,6 +17,8 @@ cudaError_t launch_cell_kernel(const EvalArgs& a, cudaStream_t s) {
         cudaError_t e = cudaFuncSetAttribute(dg_cell_kernel<Phys, K, Q, MODE>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM_BYTES);
         if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(dg_cell_kernel<Phys, K, Q, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
         attr_done |= (1ull << (dev & 63));
     }
     const long long blocks = ((long long)a.g.J + C::CPB - 1) / C::CPB;
@@ -44,6 +46,9 @@ cudaError_t launch_slab_kernel(const EvalArgs& a, cudaStream_t s) {
     if (!(attr_done & (1ull << (dev & 63)))) {
         cudaError_t e = cudaFuncSetAttribute(dg_slab_kernel<Phys, K, Q, MODE>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        // the tiles are sized for two resident CTAs: ask for the largest shared-memory carveout
+        e = cudaFuncSetAttribute(dg_slab_kernel<Phys, K, Q, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         attr_done |= (1ull << (dev & 63));
     }

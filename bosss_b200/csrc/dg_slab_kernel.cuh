@@ -69,7 +69,7 @@ struct SlabCfg {
 #define BOSSS_SLAB_THREADS_VJP 128
 #endif
 #ifndef BOSSS_SLAB_MINB
-#define BOSSS_SLAB_MINB 1
+#define BOSSS_SLAB_MINB 2
 #endif
 #ifndef BOSSS_SLAB_MINB_VJP
 #define BOSSS_SLAB_MINB_VJP 2
@@ -506,27 +506,30 @@ __device__ __forceinline__ void slab_face_traces(const EvalArgs& args, const dou
     using C = SlabCfg<Phys, K, Q, MODE>;
     constexpr int NP = C::NP, NV = C::NV, SLF = C::SLF;
     const long long nb = neighbour(args.g, ijk, DIR, S);
+    constexpr bool GG = C::G_STATE || C::G_SECOND_FACE;
     for (int f = o; f < C::NFI; f += C::NO) {
-        double cf[NP], cn[NP];
+        const bool fg = f < NV ? C::G_STATE : C::G_SECOND_FACE;
+        {   // own cell
+            double cf[NP];
 #pragma unroll
-        for (int n = 0; n < NP; ++n) cf[n] = cin[f * NP + n];
-        if (nb >= 0) {
-            const double* src = (f < NV) ? args.U + nb * (NV * NP) + f * NP : args.V + nb * (C::NF1 * NP) + (f - NV) * NP;
-#pragma unroll
-            for (int n = 0; n < NP; ++n) cn[n] = __ldg(src + n);
-        } else {
-#pragma unroll
-            for (int n = 0; n < NP; ++n) cn[n] = 0.0;
+            for (int n = 0; n < NP; ++n) cf[n] = cin[f * NP + n];
+            double* t0 = wk + (S * 2 + 0) * C::TRB + C::fnode(f) + q * SLF;
+            if (fg) face_interp<DIR, K, Q, GG>(args.tab, cf, S, Aq, dAq, args.g.scaling, args.g.twoh, t0);
+            else face_interp<DIR, K, Q, false>(args.tab, cf, S, Aq, dAq, args.g.scaling, args.g.twoh, t0);
         }
-        double* t0 = wk + (S * 2 + 0) * C::TRB + C::fnode(f) + q * SLF;
-        double* t1 = wk + (S * 2 + 1) * C::TRB + C::fnode(f) + q * SLF;
-        if (f < NV ? C::G_STATE : C::G_SECOND_FACE) {
-            constexpr bool GG = C::G_STATE || C::G_SECOND_FACE;
-            face_interp<DIR, K, Q, GG>(args.tab, cf, S, Aq, dAq, args.g.scaling, args.g.twoh, t0);
-            face_interp<DIR, K, Q, GG>(args.tab, cn, 1 - S, Aq, dAq, args.g.scaling, args.g.twoh, t1);
-        } else {
-            face_interp<DIR, K, Q, false>(args.tab, cf, S, Aq, dAq, args.g.scaling, args.g.twoh, t0);
-            face_interp<DIR, K, Q, false>(args.tab, cn, 1 - S, Aq, dAq, args.g.scaling, args.g.twoh, t1);
+        {   // neighbour across the face
+            double cn[NP];
+            if (nb >= 0) {
+                const double* src = (f < NV) ? args.U + nb * (NV * NP) + f * NP : args.V + nb * (C::NF1 * NP) + (f - NV) * NP;
+#pragma unroll
+                for (int n = 0; n < NP; ++n) cn[n] = __ldg(src + n);
+            } else {
+#pragma unroll
+                for (int n = 0; n < NP; ++n) cn[n] = 0.0;
+            }
+            double* t1 = wk + (S * 2 + 1) * C::TRB + C::fnode(f) + q * SLF;
+            if (fg) face_interp<DIR, K, Q, GG>(args.tab, cn, 1 - S, Aq, dAq, args.g.scaling, args.g.twoh, t1);
+            else face_interp<DIR, K, Q, false>(args.tab, cn, 1 - S, Aq, dAq, args.g.scaling, args.g.twoh, t1);
         }
     }
 }
