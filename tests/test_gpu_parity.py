@@ -201,9 +201,12 @@ def test_jvp_matches_central_fd_full_size():
         ev.Evaluate(1.0, 0.0, fp, pr.U + eps * V)
         ev.Evaluate(1.0, 0.0, fm, pr.U - eps * V)
     fd = (fp - fm) / (2 * eps)
+    # with the oracle's exact JVP on this state, FD(eps=1e-6) shows: median 1.0e-7 (the
+    # eps^2 truncation term), 90th percentile 1.4e-5, 99.9th 3.4e-3 (kink)
     err = np.abs(jv - fd) / np.max(np.abs(jv))
     assert np.median(err) < 1e-6
-    assert np.mean(err > 1e-5) < 1e-3   # only the few DOFs next to a kink
+    assert np.percentile(err, 90) < 1e-4
+    assert np.percentile(err, 99.9) < 1e-2
 
 
 def test_device_resident_path_matches_host_path():
