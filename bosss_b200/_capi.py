@@ -88,6 +88,31 @@ class GridDesc(ctypes.Structure):
     ]
 
 
+class SolverOpts(ctypes.Structure):
+    _fields_ = [
+        ("rtol", ctypes.c_double),
+        ("atol", ctypes.c_double),
+        ("max_outer", ctypes.c_int32),
+        ("restart", ctypes.c_int32),
+        ("max_krylov", ctypes.c_int32),
+        ("precond", ctypes.c_int32),
+        ("inner_rtol", ctypes.c_double),
+        ("reserved", ctypes.c_int32 * 8),
+    ]
+
+
+class SolverReport(ctypes.Structure):
+    _fields_ = [
+        ("outer_iters", ctypes.c_int32),
+        ("krylov_iters", ctypes.c_int32),
+        ("converged", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
+        ("residual0", ctypes.c_double),
+        ("residual", ctypes.c_double),
+        ("reserved", ctypes.c_double * 6),
+    ]
+
+
 class Options(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32),
@@ -127,6 +152,9 @@ SIGNATURES = {
     "bosss_b200_bsr_spmv_device": (ctypes.c_int, [_P, ctypes.c_double, _P, ctypes.c_double, _P, _P]),
     "bosss_b200_bsr_get": (ctypes.c_int, [_P, _I64, _I64, _I32, _I32, _I64, _P, _P, _P]),
     "bosss_b200_compute_jacobian": (ctypes.c_int, [_P, _P, ctypes.c_double, ctypes.POINTER(_P)]),
+    "bosss_b200_newton_solve": (ctypes.c_int, [_P, _P, ctypes.c_double, ctypes.POINTER(SolverOpts),
+                                               ctypes.POINTER(SolverReport)]),
+    "bosss_b200_bsr_solve": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(SolverOpts), ctypes.POINTER(SolverReport)]),
 }
 
 _lib = None

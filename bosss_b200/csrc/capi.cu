@@ -20,6 +20,7 @@
 #include "../../include/bosss_b200.h"
 #include "dg_kernel.cuh"
 #include "dg_registry.h"
+#include "handle.h"
 
 namespace bosss {
 
@@ -40,17 +41,11 @@ static void ensure_registered() {
 
 static thread_local std::string g_last_error;
 
-static int fail(int code, const std::string& msg) {
+int fail(int code, const std::string& msg) {
     g_last_error = msg;
     return code;
 }
 
-#define CUDA_TRY(call)                                                                            \
-    do {                                                                                          \
-        cudaError_t e_ = (call);                                                                  \
-        if (e_ != cudaSuccess)                                                                    \
-            return fail(BOSSS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
-    } while (0)
 
 // ------------------------------------------------------------------ host tables
 // Gauss-Legendre rule with n nodes (Newton iteration on P_n in long double), ascending.
@@ -156,33 +151,6 @@ static int quad_order(const bosss_op_desc& op) {
 
 using namespace bosss;
 
-struct bosss_handle {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int phys = 0, D = 0, K = 0, Q = 0, variant = 0;
-    EvalArgs base{};
-    int64_t ndom = 0, ncod = 0;
-    KernelEntry kern[3]{};
-    bool check_nan = false;
-    // device staging for the host-buffer entry points
-    double* dU = nullptr;
-    double* dV = nullptr;
-    double* dOut = nullptr;
-    int* dFlag = nullptr;
-};
-
-struct bosss_bsr {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int64_t nbr = 0, nbc = 0, nnzb = 0;
-    int br = 0, bc = 0;
-    int64_t* d_rowptr = nullptr;
-    int32_t* d_colidx = nullptr;
-    double* d_vals = nullptr;   // blocks stored column-major (coalesced row-lane loads)
-    double* dx = nullptr;
-    double* dy = nullptr;
-};
-
 namespace bosss {
 
 static int classify(const bosss_op_desc& op, int D, int& phys, PhysParams& ph) {
@@ -272,7 +240,7 @@ static int classify(const bosss_op_desc& op, int D, int& phys, PhysParams& ph) {
     return 0;
 }
 
-static int ensure_staging(bosss_handle* h) {
+int ensure_staging(bosss_handle* h) {
     if (h->dU) return 0;
     const int64_t n1 = std::max(h->ndom, h->ncod);
     CUDA_TRY(cudaMalloc(&h->dU, sizeof(double) * std::max<int64_t>(h->ndom, 1)));
@@ -289,7 +257,7 @@ __global__ void nan_scan_kernel(const double* x, long long n, int* flag) {
         }
 }
 
-static int run_mode(bosss_handle* h, int mode, double alpha, double beta, const double* U, const double* V,
+int run_mode(bosss_handle* h, int mode, double alpha, double beta, const double* U, const double* V,
                     double* out, double time, cudaStream_t s) {
     EvalArgs a = h->base;
     a.U = U;
@@ -635,6 +603,7 @@ int bosss_b200_bsr_destroy(bosss_bsr* A) {
     cudaFree(A->d_rowptr);
     cudaFree(A->d_colidx);
     cudaFree(A->d_vals);
+    cudaFree(A->d_vals32);
     cudaFree(A->dx);
     cudaFree(A->dy);
     if (A->stream) cudaStreamDestroy(A->stream);
@@ -697,10 +666,5 @@ int bosss_b200_bsr_get(const bosss_bsr* A, int64_t* n_block_rows, int64_t* n_blo
     return BOSSS_OK;
 }
 
-int bosss_b200_compute_jacobian(bosss_handle* h, const double* U, double time, bosss_bsr** out) {
-    (void)h; (void)U; (void)time;
-    if (out) *out = nullptr;
-    return fail(BOSSS_ERR_BAD_ARG, "compute_jacobian: not available in this build");
-}
 
 }  // extern "C"

@@ -1,0 +1,53 @@
+// handle.h -- private definitions shared by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/bosss_b200.h"
+#include "dg_kernel.cuh"
+#include "dg_registry.h"
+
+struct bosss_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int phys = 0, D = 0, K = 0, Q = 0, variant = 0;
+    bosss::EvalArgs base{};
+    int64_t ndom = 0, ncod = 0;
+    bosss::KernelEntry kern[3]{};
+    bool check_nan = false;
+    // device staging for the host-buffer entry points
+    double* dU = nullptr;
+    double* dV = nullptr;
+    double* dOut = nullptr;
+    int* dFlag = nullptr;
+};
+
+struct bosss_bsr {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t nbr = 0, nbc = 0, nnzb = 0;
+    int br = 0, bc = 0;
+    int64_t* d_rowptr = nullptr;
+    int32_t* d_colidx = nullptr;
+    double* d_vals = nullptr;   // blocks stored column-major (coalesced row-lane loads)
+    float* d_vals32 = nullptr;  // FP32 copy for the inner solves of the mixed-precision refinement
+    double* dx = nullptr;
+    double* dy = nullptr;
+};
+
+
+namespace bosss {
+int fail(int code, const std::string& msg);
+int run_mode(bosss_handle* h, int mode, double alpha, double beta, const double* U, const double* V, double* out,
+             double time, cudaStream_t s);
+int ensure_staging(bosss_handle* h);
+}  // namespace bosss
+
+#define CUDA_TRY(call)                                                                                  \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return ::bosss::fail(BOSSS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+    } while (0)

@@ -1,0 +1,585 @@
+// solve.cu -- Jacobian assembly, block-Jacobi preconditioner, matrix-free Newton-GMRES
+// and mixed-precision (FP32 GMRES / FP64 refinement) block-sparse solves.
+//
+// Reference counterparts:
+//  * bosss_b200_compute_jacobian: EvaluatorLinear.ComputeMatrix -> LEC quadrature ->
+//    BlockMsrMatrix.AccBlock (DifferentialOperator.cs:1766-1838) / FDJacobianBuilder
+//    (:2558-2858, cell colouring + repeated Evaluate). Here: exact JVP probes over a
+//    distance-2 colouring of the cells, one probe per (colour, local column), scattered
+//    into the cell-block pattern (self + face neighbours).
+//  * bosss_b200_newton_solve: Newton with MatrixFreeGMRES (Newton.cs:1231-1440), the FD
+//    directional derivative dirder (Newton.cs:1450-1495) replaced by the exact JVP.
+//  * bosss_b200_bsr_solve: GMRES (SoftGMRES.cs) on a BlockMsrMatrix, here in FP32 inside
+//    FP64 iterative refinement.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "handle.h"
+#include "solver.cuh"
+
+namespace bosss {
+
+// ------------------------------------------------------------------ colouring
+struct Colouring {
+    int m[3] = {1, 1, 1};
+    int ncol = 1;
+};
+
+static Colouring make_colouring(const GridConst& g) {
+    Colouring c;
+    for (int d = 0; d < g.D; ++d) {
+        const int n = g.n[d];
+        if (!g.periodic[d]) {
+            c.m[d] = std::min(3, n);
+        } else {
+            c.m[d] = n;
+            for (int k = 3; k <= n; ++k)
+                if (n % k == 0) {
+                    c.m[d] = k;
+                    break;
+                }
+        }
+        c.ncol *= c.m[d];
+    }
+    return c;
+}
+
+__device__ __forceinline__ int cell_colour(const GridConst& g, long long j, int m0, int m1, int m2) {
+    int ijk[3];
+    cell_ijk(g, j, ijk);
+    int c = ijk[0] % m0;
+    if (g.D >= 2) c = c * m1 + ijk[1] % m1;
+    if (g.D >= 3) c = c * m2 + ijk[2] % m2;
+    return c;
+}
+
+// probe: V[j*Nd + i] = 1 for cells of colour `col` and local column `i0`, else 0
+__global__ void k_probe(GridConst g, int m0, int m1, int m2, int col, int Nd, int i0, double* V) {
+    const long long n = (long long)g.J * Nd;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long j = t / Nd;
+        const int i = (int)(t - j * Nd);
+        V[t] = (i == i0 && cell_colour(g, j, m0, m1, m2) == col) ? 1.0 : 0.0;
+    }
+}
+
+// scatter JV into column i0 of every block whose column cell has colour `col`
+// (blocks column-major: vals[b*br*bc + i0*br + r])
+__global__ void k_scatter(GridConst g, int m0, int m1, int m2, int col, int i0, int br, int bc,
+                          const long long* __restrict__ rowptr, const int* __restrict__ colidx,
+                          const double* __restrict__ JV, double* __restrict__ vals) {
+    const long long nrows = (long long)g.J * br;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nrows; t += (long long)gridDim.x * blockDim.x) {
+        const long long j = t / br;
+        const int r = (int)(t - j * br);
+        for (long long b = rowptr[j]; b < rowptr[j + 1]; ++b)
+            if (cell_colour(g, colidx[b], m0, m1, m2) == col) vals[b * (long long)br * bc + (long long)i0 * br + r] = JV[t];
+    }
+}
+
+// cell-block pattern: self first, then the face neighbours (duplicates dropped)
+static void block_pattern(const GridConst& g, std::vector<int64_t>& rowptr, std::vector<int32_t>& colidx) {
+    rowptr.assign(1, 0);
+    colidx.clear();
+    for (long long j = 0; j < g.J; ++j) {
+        int ijk[3] = {0, 0, 0};
+        for (int d = 0; d < g.D; ++d) ijk[d] = (int)((j / g.stride[d]) % g.n[d]);
+        std::vector<int32_t> cols{(int32_t)j};
+        for (int d = 0; d < g.D; ++d)
+            for (int s = 0; s < 2; ++s) {
+                int i = ijk[d] + (s ? 1 : -1);
+                if (i < 0 || i >= g.n[d]) {
+                    if (!g.periodic[d]) continue;
+                    i = (i + g.n[d]) % g.n[d];
+                }
+                long long nb = 0;
+                for (int dd = 0; dd < g.D; ++dd) nb += (long long)((dd == d) ? i : ijk[dd]) * g.stride[dd];
+                if (std::find(cols.begin(), cols.end(), (int32_t)nb) == cols.end()) cols.push_back((int32_t)nb);
+            }
+        colidx.insert(colidx.end(), cols.begin(), cols.end());
+        rowptr.push_back((int64_t)colidx.size());
+    }
+}
+
+static int grid_of(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 16); }
+
+// assemble J(U_dev) into a new bosss_bsr (values on the device)
+static int assemble(bosss_handle* h, const double* U_dev, double time, bosss_bsr** out) {
+    const GridConst& g = h->base.g;
+    const int Nd = (int)(h->ndom / g.J), Nc = (int)(h->ncod / g.J);
+    std::vector<int64_t> rp;
+    std::vector<int32_t> ci;
+    block_pattern(g, rp, ci);
+    bosss_bsr* A = new bosss_bsr();
+    A->device = h->device;
+    A->nbr = A->nbc = g.J;
+    A->nnzb = (int64_t)ci.size();
+    A->br = Nc;
+    A->bc = Nd;
+    const size_t bs = (size_t)Nc * Nd;
+    cudaStream_t s = h->stream;
+    auto bail = [&](cudaError_t e) {
+        bosss_b200_bsr_destroy(A);
+        return fail(BOSSS_ERR_CUDA, std::string("Jacobian assembly: ") + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&A->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&A->d_rowptr, sizeof(int64_t) * rp.size());
+    if (e == cudaSuccess) e = cudaMalloc(&A->d_colidx, sizeof(int32_t) * ci.size());
+    if (e == cudaSuccess) e = cudaMalloc(&A->d_vals, sizeof(double) * bs * ci.size());
+    if (e == cudaSuccess) e = cudaMemcpy(A->d_rowptr, rp.data(), sizeof(int64_t) * rp.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(A->d_colidx, ci.data(), sizeof(int32_t) * ci.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemsetAsync(A->d_vals, 0, sizeof(double) * bs * ci.size(), s);
+    double *V = nullptr, *JV = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&V, sizeof(double) * h->ndom);
+    if (e == cudaSuccess) e = cudaMalloc(&JV, sizeof(double) * h->ncod);
+    if (e != cudaSuccess) {
+        cudaFree(V);
+        cudaFree(JV);
+        return bail(e);
+    }
+    const Colouring c = make_colouring(g);
+    for (int col = 0; col < c.ncol && e == cudaSuccess; ++col)
+        for (int i0 = 0; i0 < Nd && e == cudaSuccess; ++i0) {
+            k_probe<<<grid_of(h->ndom), 256, 0, s>>>(g, c.m[0], c.m[1], c.m[2], col, Nd, i0, V);
+            int rc = run_mode(h, MODE_JVP, 1.0, 0.0, U_dev, V, JV, time, s);
+            if (rc) {
+                cudaFree(V);
+                cudaFree(JV);
+                bosss_b200_bsr_destroy(A);
+                return rc;
+            }
+            k_scatter<<<grid_of(h->ncod), 256, 0, s>>>(g, c.m[0], c.m[1], c.m[2], col, i0, Nc, Nd,
+                                                       (const long long*)A->d_rowptr, A->d_colidx, JV, A->d_vals);
+            e = cudaGetLastError();
+        }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(V);
+    cudaFree(JV);
+    if (e != cudaSuccess) return bail(e);
+    *out = A;
+    return BOSSS_OK;
+}
+
+// ------------------------------------------------------------------ block-Jacobi
+// Gauss-Jordan with partial pivoting of the diagonal block of every block row; one CTA
+// per block, the augmented matrix [A | I] in shared memory. Output column-major.
+template <class T>
+__global__ void k_invert_diag(int nb, const long long* __restrict__ rowptr, const double* __restrict__ vals, T* __restrict__ inv,
+                              int* __restrict__ singular) {
+    extern __shared__ double sm[];
+    const int j = blockIdx.x;
+    double* Am = sm;              // nb x nb, row-major
+    double* Im = sm + nb * nb;    // nb x nb, row-major
+    __shared__ int piv;
+    const double* blk = vals + rowptr[j] * (long long)nb * nb;   // diagonal block is the first of the row
+    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+        const int r = t / nb, c = t % nb;
+        Am[t] = blk[(long long)c * nb + r];
+        Im[t] = (r == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < nb; ++k) {
+        if (threadIdx.x == 0) {
+            int p = k;
+            double best = fabs(Am[k * nb + k]);
+            for (int r = k + 1; r < nb; ++r)
+                if (fabs(Am[r * nb + k]) > best) {
+                    best = fabs(Am[r * nb + k]);
+                    p = r;
+                }
+            piv = p;
+            if (best == 0.0) atomicExch(singular, 1);
+        }
+        __syncthreads();
+        const int p = piv;
+        if (p != k)
+            for (int c = threadIdx.x; c < nb; c += blockDim.x) {
+                double t0 = Am[k * nb + c];
+                Am[k * nb + c] = Am[p * nb + c];
+                Am[p * nb + c] = t0;
+                t0 = Im[k * nb + c];
+                Im[k * nb + c] = Im[p * nb + c];
+                Im[p * nb + c] = t0;
+            }
+        __syncthreads();
+        const double d = Am[k * nb + k];
+        const double inv_d = (d != 0.0) ? 1.0 / d : 0.0;
+        __syncthreads();
+        for (int c = threadIdx.x; c < nb; c += blockDim.x) {
+            Am[k * nb + c] *= inv_d;
+            Im[k * nb + c] *= inv_d;
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+            const int r = t / nb, c = t % nb;
+            if (r == k) continue;
+            const double f = Am[r * nb + k];
+            if (c != k) Am[t] -= f * Am[k * nb + c];
+            Im[t] -= f * Im[k * nb + c];
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < nb; r += blockDim.x)
+            if (r != k) Am[r * nb + k] = 0.0;
+        __syncthreads();
+    }
+    T* out = inv + (long long)j * nb * nb;
+    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+        const int r = t / nb, c = t % nb;
+        out[(long long)c * nb + r] = (T)Im[t];
+    }
+}
+
+// y_j = Dinv_j x_j (blocks column-major), one thread per scalar row
+template <class T>
+__global__ void k_apply_blockdiag(long long ncell, int nb, const T* __restrict__ inv, const T* __restrict__ x,
+                                  T* __restrict__ y) {
+    const long long n = ncell * nb;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long j = t / nb;
+        const int r = (int)(t - j * nb);
+        const T* B = inv + j * (long long)nb * nb;
+        const T* xj = x + j * nb;
+        double acc = 0.0;
+        for (int c = 0; c < nb; ++c) acc += (double)B[(long long)c * nb + r] * (double)xj[c];
+        y[t] = (T)acc;
+    }
+}
+
+template <class T>
+static int block_jacobi(const bosss_bsr* A, T** inv, cudaStream_t s) {
+    if (A->br != A->bc || A->nbr != A->nbc) return fail(BOSSS_ERR_BAD_ARG, "block-Jacobi needs square diagonal blocks");
+    const int nb = A->br;
+    if ((size_t)2 * nb * nb * 8 > 200 * 1024) return fail(BOSSS_ERR_BAD_ARG, "cell block too large for block-Jacobi");
+    CUDA_TRY(cudaMalloc(inv, sizeof(T) * (size_t)nb * nb * A->nbr));
+    int* sing = nullptr;
+    CUDA_TRY(cudaMalloc(&sing, sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(sing, 0, sizeof(int), s));
+    const size_t smem = (size_t)2 * nb * nb * 8;
+    CUDA_TRY(cudaFuncSetAttribute(k_invert_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (A->nbr > 0) k_invert_diag<T><<<(unsigned)A->nbr, 128, smem, s>>>(nb, (const long long*)A->d_rowptr, A->d_vals, *inv, sing);
+    CUDA_TRY(cudaGetLastError());
+    int flag = 0;
+    CUDA_TRY(cudaMemcpyAsync(&flag, sing, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    cudaFree(sing);
+    if (flag) return fail(BOSSS_ERR_BAD_ARG, "singular diagonal block in block-Jacobi");
+    return BOSSS_OK;
+}
+
+template <class T>
+__global__ void bsr_spmv_t(long long nbr, int br, int bc, const long long* __restrict__ rowptr, const int* __restrict__ colidx,
+                           const T* __restrict__ vals, const T* __restrict__ x, T* __restrict__ y) {
+    const long long nrows = nbr * br;
+    for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < nrows; row += (long long)gridDim.x * blockDim.x) {
+        const long long i = row / br;
+        const int r = (int)(row - i * br);
+        T acc = T(0);
+        for (long long b = rowptr[i]; b < rowptr[i + 1]; ++b) {
+            const T* blk = vals + b * (long long)br * bc;
+            const T* xb = x + (long long)colidx[b] * bc;
+            for (int c = 0; c < bc; ++c) acc += blk[(long long)c * br + r] * xb[c];
+        }
+        y[row] = acc;
+    }
+}
+
+static void fill_defaults(const bosss_solver_opts* o, bosss_solver_opts& r, double rtol, int outer) {
+    std::memset(&r, 0, sizeof(r));
+    r.rtol = rtol;
+    r.atol = 0.0;
+    r.max_outer = outer;
+    r.restart = 50;
+    r.max_krylov = 2000;
+    r.precond = 1;
+    r.inner_rtol = 1e-3;
+    if (o) {
+        if (o->rtol > 0) r.rtol = o->rtol;
+        if (o->atol > 0) r.atol = o->atol;
+        if (o->max_outer > 0) r.max_outer = o->max_outer;
+        if (o->restart > 0) r.restart = std::min(o->restart, 200);
+        if (o->max_krylov > 0) r.max_krylov = o->max_krylov;
+        r.precond = o->precond;
+        if (o->inner_rtol > 0) r.inner_rtol = o->inner_rtol;
+    }
+}
+
+template <class T>
+struct KrylovWork {
+    T* V = nullptr;
+    T* w = nullptr;
+    T* z = nullptr;
+    double* partials = nullptr;
+    double* hbuf = nullptr;
+    ~KrylovWork() {
+        cudaFree(V);
+        cudaFree(w);
+        cudaFree(z);
+        cudaFree(partials);
+        cudaFree(hbuf);
+    }
+    cudaError_t alloc(long long n, int m) {
+        cudaError_t e = cudaMalloc(&V, sizeof(T) * (size_t)(m + 1) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&w, sizeof(T) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&z, sizeof(T) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&partials, sizeof(double) * RED_BLOCKS * (m + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&hbuf, sizeof(double) * (m + 1));
+        return e;
+    }
+};
+
+static double norm2(const double* x, long long n, double* partials, cudaStream_t s) {
+    k_dot_partials<double><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, x, x, partials);
+    std::vector<double> hp(RED_BLOCKS);
+    cudaMemcpyAsync(hp.data(), partials, sizeof(double) * RED_BLOCKS, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    double acc = 0.0;
+    for (double v : hp) acc += v;
+    return std::sqrt(std::max(acc, 0.0));
+}
+
+}  // namespace bosss
+
+using namespace bosss;
+
+extern "C" {
+
+int bosss_b200_compute_jacobian(bosss_handle* h, const double* U, double time, bosss_bsr** out) {
+    if (!h || !U || !out) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    *out = nullptr;
+    int rc = ensure_staging(h);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaMemcpyAsync(h->dU, U, sizeof(double) * h->ndom, cudaMemcpyHostToDevice, h->stream));
+    return assemble(h, h->dU, time, out);
+}
+
+int bosss_b200_newton_solve(bosss_handle* h, double* U, double time, const bosss_solver_opts* opt,
+                            bosss_solver_report* rep) {
+    if (!h || !U) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    if (h->ndom != h->ncod) return fail(BOSSS_ERR_BAD_ARG, "Newton needs a square operator");
+    bosss_solver_opts o;
+    fill_defaults(opt, o, 1e-10, 20);
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = h->stream;
+    const long long n = h->ndom;
+    double *dU = nullptr, *dR = nullptr, *dX = nullptr, *dT = nullptr, *dW = nullptr, *dinv = nullptr;
+    KrylovWork<double> kw;
+    auto cleanup = [&]() {
+        cudaFree(dU);
+        cudaFree(dR);
+        cudaFree(dX);
+        cudaFree(dT);
+        cudaFree(dW);
+        cudaFree(dinv);
+    };
+    cudaError_t e = cudaMalloc(&dU, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dR, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dX, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dT, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dW, sizeof(double) * n);
+    if (e == cudaSuccess) e = kw.alloc(n, o.restart);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dU, U, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        cleanup();
+        return fail(BOSSS_ERR_CUDA, std::string("Newton work arrays: ") + cudaGetErrorString(e));
+    }
+    bosss_solver_report r{};
+    int rc = 0;
+    const int nb = (int)(n / h->base.g.J);
+    double res = 0.0, res0 = 0.0;
+    for (int it = 0; it <= o.max_outer; ++it) {
+        rc = run_mode(h, MODE_RES, 1.0, 0.0, dU, nullptr, dR, time, s);
+        if (rc) break;
+        res = norm2(dR, n, kw.partials, s);
+        if (it == 0) res0 = res;
+        r.residual = res;
+        if (!std::isfinite(res)) {
+            rc = fail(BOSSS_ERR_NAN, "non-finite residual in Newton");
+            break;
+        }
+        if (res <= std::max(o.rtol * res0, o.atol)) {
+            r.converged = 1;
+            break;
+        }
+        if (it == o.max_outer) break;
+        r.outer_iters = it + 1;
+        // right-preconditioned J M^-1 z = -R, dU_step = M^-1 z
+        if (o.precond == 1) {
+            cudaFree(dinv);
+            dinv = nullptr;
+            bosss_bsr* A = nullptr;
+            rc = assemble(h, dU, time, &A);
+            if (rc) break;
+            rc = block_jacobi<double>(A, &dinv, s);
+            bosss_b200_bsr_destroy(A);
+            if (rc) break;
+        }
+        k_axpby<double><<<grid_of(n), 256, 0, s>>>(n, -1.0, dR, 0.0, dW);   // rhs = -R
+        CUDA_TRY(cudaMemsetAsync(dX, 0, sizeof(double) * n, s));
+        int inner_rc = 0;
+        auto apply = [&](const double* x, double* y) -> cudaError_t {
+            const double* xin = x;
+            if (dinv) {
+                k_apply_blockdiag<double><<<grid_of(n), 256, 0, s>>>(h->base.g.J, nb, dinv, x, dT);
+                xin = dT;
+            }
+            int rr = run_mode(h, MODE_JVP, 1.0, 0.0, dU, xin, y, time, s);
+            if (rr) inner_rc = rr;
+            return rr ? cudaErrorUnknown : cudaGetLastError();
+        };
+        GmresResult g = gmres<double>(n, apply, dW, dX, o.restart, o.max_krylov, o.inner_rtol, 0.0, kw.V, kw.w,
+                                      kw.partials, kw.hbuf, s);
+        r.krylov_iters += g.iters;
+        if (inner_rc) {
+            rc = inner_rc;
+            break;
+        }
+        if (g.error) {
+            rc = fail(BOSSS_ERR_CUDA, "GMRES: " + std::string(cudaGetErrorString((cudaError_t)g.error)));
+            break;
+        }
+        const double* step = dX;
+        if (dinv) {
+            k_apply_blockdiag<double><<<grid_of(n), 256, 0, s>>>(h->base.g.J, nb, dinv, dX, dT);
+            step = dT;
+        }
+        // backtracking on the residual norm
+        CUDA_TRY(cudaMemcpyAsync(dW, dU, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        double lam = 1.0;
+        for (int ls = 0; ls < 8; ++ls) {
+            CUDA_TRY(cudaMemcpyAsync(dU, dW, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+            k_axpby<double><<<grid_of(n), 256, 0, s>>>(n, lam, step, 1.0, dU);
+            rc = run_mode(h, MODE_RES, 1.0, 0.0, dU, nullptr, dR, time, s);
+            if (rc) break;
+            const double rn = norm2(dR, n, kw.partials, s);
+            if (std::isfinite(rn) && rn < res) break;
+            lam *= 0.5;
+        }
+        if (rc) break;
+    }
+    if (!rc) {
+        cudaError_t e2 = cudaMemcpyAsync(U, dU, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+        if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(s);
+        if (e2 != cudaSuccess) rc = fail(BOSSS_ERR_CUDA, cudaGetErrorString(e2));
+    }
+    r.residual0 = res0;
+    if (rep) *rep = r;
+    cleanup();
+    return rc;
+}
+
+int bosss_b200_bsr_solve(bosss_bsr* A, const double* b, double* x, const bosss_solver_opts* opt,
+                         bosss_solver_report* rep) {
+    if (!A || !b || !x) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    if (A->nbr != A->nbc || A->br != A->bc) return fail(BOSSS_ERR_BAD_ARG, "bsr_solve needs a square matrix");
+    bosss_solver_opts o;
+    fill_defaults(opt, o, 1e-10, 30);
+    CUDA_TRY(cudaSetDevice(A->device));
+    cudaStream_t s = A->stream;
+    const long long n = A->nbr * A->br;
+    const size_t nv = (size_t)A->nnzb * A->br * A->bc;
+    if (!A->d_vals32) {
+        CUDA_TRY(cudaMalloc(&A->d_vals32, sizeof(float) * std::max<size_t>(nv, 1)));
+        k_convert<double, float><<<grid_of((long long)nv), 256, 0, s>>>((long long)nv, A->d_vals, A->d_vals32);
+        CUDA_TRY(cudaGetLastError());
+    }
+    double *db = nullptr, *dx = nullptr, *dr = nullptr;
+    float *rf = nullptr, *cf = nullptr, *tf = nullptr, *inv = nullptr;
+    KrylovWork<float> kw;
+    auto cleanup = [&]() {
+        cudaFree(db);
+        cudaFree(dx);
+        cudaFree(dr);
+        cudaFree(rf);
+        cudaFree(cf);
+        cudaFree(tf);
+        cudaFree(inv);
+    };
+    cudaError_t e = cudaMalloc(&db, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dx, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dr, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&rf, sizeof(float) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&cf, sizeof(float) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&tf, sizeof(float) * n);
+    if (e == cudaSuccess) e = kw.alloc(n, o.restart);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db, b, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        cleanup();
+        return fail(BOSSS_ERR_CUDA, std::string("solver work arrays: ") + cudaGetErrorString(e));
+    }
+    int rc = 0;
+    if (o.precond == 1) {
+        rc = block_jacobi<float>(A, &inv, s);
+        if (rc) {
+            cleanup();
+            return rc;
+        }
+    }
+    const double bnorm = norm2(db, n, kw.partials, s);
+    bosss_solver_report r{};
+    const int nb = A->br;
+    for (int it = 0; it <= o.max_outer; ++it) {
+        // r = b - A x in FP64
+        rc = bosss_b200_bsr_spmv_device(A, -1.0, dx, 0.0, dr, s);
+        if (rc) break;
+        k_axpby<double><<<grid_of(n), 256, 0, s>>>(n, 1.0, db, 1.0, dr);
+        const double res = norm2(dr, n, kw.partials, s);
+        if (it == 0) r.residual0 = res;
+        r.residual = res;
+        if (!std::isfinite(res)) {
+            rc = fail(BOSSS_ERR_NAN, "non-finite residual in refinement");
+            break;
+        }
+        if (res <= std::max(o.rtol * bnorm, o.atol)) {
+            r.converged = 1;
+            break;
+        }
+        if (it == o.max_outer) break;
+        r.outer_iters = it + 1;
+        // FP32 correction: A c = r
+        k_convert<double, float><<<grid_of(n), 256, 0, s>>>(n, dr, rf);
+        CUDA_TRY(cudaMemsetAsync(cf, 0, sizeof(float) * n, s));
+        auto apply = [&](const float* xx, float* yy) -> cudaError_t {
+            const float* xin = xx;
+            if (inv) {
+                k_apply_blockdiag<float><<<grid_of(n), 256, 0, s>>>(A->nbr, nb, inv, xx, tf);
+                xin = tf;
+            }
+            bsr_spmv_t<float><<<grid_of(n), 256, 0, s>>>(A->nbr, A->br, A->bc, (const long long*)A->d_rowptr,
+                                                          A->d_colidx, A->d_vals32, xin, yy);
+            return cudaGetLastError();
+        };
+        GmresResult g = gmres<float>(n, apply, rf, cf, o.restart, o.max_krylov, o.inner_rtol, 0.0, kw.V, kw.w,
+                                     kw.partials, kw.hbuf, s);
+        r.krylov_iters += g.iters;
+        if (g.error) {
+            rc = fail(BOSSS_ERR_CUDA, "GMRES: " + std::string(cudaGetErrorString((cudaError_t)g.error)));
+            break;
+        }
+        const float* corr = cf;
+        if (inv) {
+            k_apply_blockdiag<float><<<grid_of(n), 256, 0, s>>>(A->nbr, nb, inv, cf, tf);
+            corr = tf;
+        }
+        // x += c (FP64 accumulation of the FP32 correction)
+        k_convert<float, double><<<grid_of(n), 256, 0, s>>>(n, corr, dr);
+        k_axpby<double><<<grid_of(n), 256, 0, s>>>(n, 1.0, dr, 1.0, dx);
+        CUDA_TRY(cudaGetLastError());
+    }
+    if (!rc) {
+        cudaError_t e2 = cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+        if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(s);
+        if (e2 != cudaSuccess) rc = fail(BOSSS_ERR_CUDA, cudaGetErrorString(e2));
+    }
+    if (rep) *rep = r;
+    cleanup();
+    return rc;
+}
+
+}  // extern "C"

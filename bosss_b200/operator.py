@@ -318,6 +318,81 @@ class DifferentialOperator:
                          device, precision, check_nan, kernel)
 
 
+def _solver_opts(rtol=None, atol=None, max_outer=None, restart=None, max_krylov=None, precond=1, inner_rtol=None):
+    o = C.SolverOpts()
+    o.rtol = rtol or 0.0
+    o.atol = atol or 0.0
+    o.max_outer = max_outer or 0
+    o.restart = restart or 0
+    o.max_krylov = max_krylov or 0
+    o.precond = int(precond)
+    o.inner_rtol = inner_rtol or 0.0
+    return o
+
+
+def _report(r):
+    return {"outer_iters": r.outer_iters, "krylov_iters": r.krylov_iters, "converged": bool(r.converged),
+            "residual0": r.residual0, "residual": r.residual}
+
+
+class BlockMsrMatrix:
+    """Device block-sparse matrix with dense cell blocks (``BlockMsrMatrix.cs:186``):
+    ``SpMV(alpha, x, beta, y)`` is ``BlockMsrMatrix.SpMV`` (``:2554``)."""
+
+    def __init__(self, handle):
+        self.handle = handle
+        nbr, nbc, br, bc, nnzb = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        C.check(C.lib().bosss_b200_bsr_get(handle, ctypes.byref(nbr), ctypes.byref(nbc), ctypes.byref(br),
+                                           ctypes.byref(bc), ctypes.byref(nnzb), None, None, None))
+        self.n_block_rows, self.n_block_cols = nbr.value, nbc.value
+        self.row_block, self.col_block, self.nnz_blocks = br.value, bc.value, nnzb.value
+
+    @classmethod
+    def from_blocks(cls, n_block_rows, n_block_cols, row_ptr, col_idx, values, device=0):
+        rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
+        ci = np.ascontiguousarray(col_idx, dtype=np.int32)
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        nnzb = len(ci)
+        bs = v.size // max(nnzb, 1)
+        br = v.shape[1] if v.ndim == 3 else None
+        if br is None:
+            raise ValueError("values must have shape (nnz_blocks, row_block, col_block)")
+        h = ctypes.c_void_p()
+        C.check(C.lib().bosss_b200_bsr_create(n_block_rows, n_block_cols, v.shape[1], v.shape[2], C.ptr(rp),
+                                              C.ptr(ci), C.ptr(v), int(device), ctypes.byref(h)))
+        del bs
+        return cls(h)
+
+    def Dispose(self):
+        if self.handle:
+            C.lib().bosss_b200_bsr_destroy(self.handle)
+            self.handle = None
+
+    __del__ = Dispose
+
+    def blocks(self):
+        """(row_ptr, col_idx, values[nnz, row_block, col_block])."""
+        rp = np.zeros(self.n_block_rows + 1, dtype=np.int64)
+        ci = np.zeros(self.nnz_blocks, dtype=np.int32)
+        v = np.zeros(self.nnz_blocks * self.row_block * self.col_block)
+        C.check(C.lib().bosss_b200_bsr_get(self.handle, None, None, None, None, None, C.ptr(rp), C.ptr(ci), C.ptr(v)))
+        return rp, ci, v.reshape(self.nnz_blocks, self.row_block, self.col_block)
+
+    def SpMV(self, alpha, x, beta, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        C.check(C.lib().bosss_b200_bsr_spmv(self.handle, alpha, C.ptr(x), beta, C.ptr(y)))
+        return y
+
+    def Solve(self, b, x=None, **kw):
+        """FP32 GMRES in FP64 iterative refinement; returns (x, report)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b) if x is None else np.array(x, dtype=np.float64, copy=True)
+        o = _solver_opts(**kw)
+        r = C.SolverReport()
+        C.check(C.lib().bosss_b200_bsr_solve(self.handle, C.ptr(b), C.ptr(x), ctypes.byref(o), ctypes.byref(r)))
+        return x, _report(r)
+
+
 class Evaluator:
     """``IEvaluatorNonLin`` backed by one ``bosss_handle``."""
 
@@ -397,6 +472,21 @@ class Evaluator:
         out = np.empty(self.n_codomain) if out is None else out
         C.check(C.lib().bosss_b200_jvp(self.handle, C.ptr(U), C.ptr(V), C.ptr(out), self.time))
         return out
+
+    def ComputeJacobian(self, U):
+        """Exact Jacobian at U as a device BlockMsrMatrix (cell blocks: self + face neighbours)."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        h = ctypes.c_void_p()
+        C.check(C.lib().bosss_b200_compute_jacobian(self.handle, C.ptr(U), self.time, ctypes.byref(h)))
+        return BlockMsrMatrix(h)
+
+    def NewtonSolve(self, U0, **kw):
+        """Matrix-free Newton-GMRES for Op(U) = 0; returns (U, report)."""
+        U = np.array(U0, dtype=np.float64, copy=True)
+        o = _solver_opts(**kw)
+        r = C.SolverReport()
+        C.check(C.lib().bosss_b200_newton_solve(self.handle, C.ptr(U), self.time, ctypes.byref(o), ctypes.byref(r)))
+        return U, _report(r)
 
     def vjp(self, U, W, out=None):
         """J(U)^T W (adjoint product)."""

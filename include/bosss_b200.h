@@ -201,6 +201,41 @@ int bosss_b200_bsr_get(const bosss_bsr* A, int64_t* n_block_rows, int64_t* n_blo
                        int32_t* row_block, int32_t* col_block, int64_t* nnz_blocks,
                        int64_t* row_ptr, int32_t* col_idx, double* values);
 
+/* ---- solvers ----
+ * Options and report of the Krylov solvers. The matrix-free Newton-GMRES replaces the
+ * reference's Newton with MatrixFreeGMRES and the FD `dirder` (Newton.cs:1231-1495) by the
+ * exact JVP; bosss_b200_bsr_solve is restarted GMRES in FP32 inside FP64 iterative
+ * refinement on an assembled block-sparse matrix. */
+typedef struct bosss_solver_opts {
+    double rtol;            /* outer relative tolerance on the residual 2-norm */
+    double atol;            /* outer absolute tolerance */
+    int32_t max_outer;      /* Newton steps (newton_solve) / refinement steps (bsr_solve) */
+    int32_t restart;        /* GMRES restart length m (<= 200) */
+    int32_t max_krylov;     /* GMRES iterations per outer step */
+    int32_t precond;        /* 0 = none, 1 = block-Jacobi on the cell blocks of the Jacobian */
+    double inner_rtol;      /* relative tolerance of each inner (Krylov) solve */
+    int32_t reserved[8];
+} bosss_solver_opts;
+
+typedef struct bosss_solver_report {
+    int32_t outer_iters;    /* Newton / refinement steps taken */
+    int32_t krylov_iters;   /* total GMRES iterations */
+    int32_t converged;      /* 1 if the outer tolerance was met */
+    int32_t reserved0;
+    double residual0;       /* initial residual 2-norm */
+    double residual;        /* final residual 2-norm */
+    double reserved[6];
+} bosss_solver_report;
+
+/* Solve Op(U) = 0 by Newton's method; each step solves J(U) dU = -Op(U) with matrix-free
+ * right-preconditioned GMRES on the exact JVP. U: host buffer, initial guess in, solution out. */
+int bosss_b200_newton_solve(bosss_handle* h, double* U, double time, const bosss_solver_opts* opt,
+                            bosss_solver_report* rep);
+/* Solve A x = b (square block-sparse A) with FP32 GMRES inside FP64 iterative refinement;
+ * x: host buffer, initial guess in, solution out. */
+int bosss_b200_bsr_solve(bosss_bsr* A, const double* b, double* x, const bosss_solver_opts* opt,
+                         bosss_solver_report* rep);
+
 /* Jacobian assembly of the operator at state U into a new block-sparse matrix
  * (EvaluatorLinear.ComputeMatrix, LECVolumeQuadrature2.cs:132 / LECEdgeQuadrature2.cs:127 ->
  * BlockMsrMatrix.AccBlock): exact linearisation, cell-block pattern = self + face neighbours. */
