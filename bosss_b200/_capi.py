@@ -46,6 +46,10 @@ CELLS_GLOBALID = 1
 # handle's own stream)
 CUDA_STREAM_LEGACY = 1
 
+MODE_RESIDUAL = 0
+MODE_JVP = 1
+MODE_VJP = 2
+
 KERNEL_AUTO = 0
 KERNEL_GENERIC = 1
 KERNEL_SLAB = 2
@@ -155,6 +159,17 @@ SIGNATURES = {
     "bosss_b200_newton_solve": (ctypes.c_int, [_P, _P, ctypes.c_double, ctypes.POINTER(SolverOpts),
                                                ctypes.POINTER(SolverReport)]),
     "bosss_b200_bsr_solve": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(SolverOpts), ctypes.POINTER(SolverReport)]),
+    "bosss_b200_batch_create": (ctypes.c_int, [ctypes.c_int32, _P, _P, ctypes.POINTER(Options), ctypes.POINTER(_P)]),
+    "bosss_b200_batch_destroy": (ctypes.c_int, [_P]),
+    "bosss_b200_batch_get_sizes": (ctypes.c_int, [_P, _P, _P]),
+    "bosss_b200_batch_evaluate": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_double, _P, _P, _P,
+                                                 ctypes.c_double]),
+    "bosss_b200_batch_evaluate_device": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_double, _P, _P,
+                                                        _P, ctypes.c_double, _P]),
+    "bosss_b200_batch_capture": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_double]),
+    "bosss_b200_batch_replay": (ctypes.c_int, [_P, _P]),
+    "bosss_b200_batch_autotune": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_char_p]),
+    "bosss_b200_batch_tiles": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _I32, _I32]),
 }
 
 _lib = None

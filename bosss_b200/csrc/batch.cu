@@ -1,0 +1,558 @@
+// batch.cu -- many independent operator instances in one persistent launch.
+//
+// Each instance is a full EvaluatorNonLin (its own grid, DG degree and quadrature rule);
+// the instances' coefficient vectors are concatenated. A persistent kernel (grid = resident
+// CTAs of the device) pulls work items (instance, first cell, number of tiles) from a
+// queue counter in device memory and evaluates them with the tile routine of the generic
+// kernel specialised for the instance's degree. Work items are ordered longest first
+// (or round-robin, as the autotuner decides), so uneven instances balance over the SMs.
+// The residual and VJP launches of a batch can be captured once into a CUDA graph and
+// replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "handle.h"
+
+namespace bosss {
+
+struct BatchInst {
+    EvalArgs a;
+    long long dom_off, cod_off;
+    int K, Q;
+};
+
+struct WorkItem {
+    int inst;
+    int ntiles;
+    long long c0;
+};
+
+// degrees with batched kernels: Q = K+1 (Linear(), order 2K / 2K+1) and 2K+1 (NonLinear(3))
+#define BOSSS_BATCH_CASES(X) X(1, 2) X(2, 3) X(3, 4) X(4, 5) X(1, 3) X(2, 5) X(3, 7)
+
+template <class Phys, int MODE>
+constexpr size_t batch_smem() {
+    size_t m = 0;
+#define BOSSS_SMEM_MAX(K, Q) m = m > Cfg<Phys, K, Q, MODE>::SMEM_BYTES ? m : Cfg<Phys, K, Q, MODE>::SMEM_BYTES;
+    BOSSS_BATCH_CASES(BOSSS_SMEM_MAX)
+#undef BOSSS_SMEM_MAX
+    return m;
+}
+
+template <class Phys, int K, int Q, int MODE>
+__device__ __forceinline__ void run_item(const EvalArgs& a, const WorkItem& w, double* smem) {
+    constexpr int CPB = Cfg<Phys, K, Q, MODE>::CPB;
+    for (int t = 0; t < w.ntiles; ++t) {
+        const long long c0 = w.c0 + (long long)t * CPB;
+        if (c0 >= a.g.J) break;
+        cell_tile<Phys, K, Q, MODE>(a, c0, smem);
+        __syncthreads();
+    }
+}
+
+template <class Phys, int MODE>
+__global__ void __launch_bounds__(256) batch_kernel(const BatchInst* __restrict__ inst, const WorkItem* __restrict__ items,
+                                                    int nitems, int* __restrict__ counter, const double* U, const double* V,
+                                                    double* out, double alpha, double beta, double time) {
+    extern __shared__ double smem[];
+    __shared__ EvalArgs sa;
+    __shared__ WorkItem w;
+    __shared__ int K, Q;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int it = atomicAdd(counter, 1);
+            w.inst = -1;
+            if (it < nitems) w = items[it];
+        }
+        __syncthreads();
+        if (w.inst < 0) break;
+        const BatchInst* b = inst + w.inst;
+        for (int i = threadIdx.x; i < (int)(sizeof(EvalArgs) / 8); i += blockDim.x)
+            reinterpret_cast<double*>(&sa)[i] = reinterpret_cast<const double*>(&b->a)[i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            sa.U = U + b->dom_off;
+            sa.V = V ? V + ((MODE == MODE_VJP) ? b->cod_off : b->dom_off) : nullptr;
+            sa.out = out + ((MODE == MODE_VJP) ? b->dom_off : b->cod_off);
+            sa.alpha = alpha;
+            sa.beta = beta;
+            sa.time = time;
+            K = b->K;
+            Q = b->Q;
+        }
+        __syncthreads();
+#define BOSSS_CASE(KK, QQ) \
+    if (K == KK && Q == QQ) run_item<Phys, KK, QQ, MODE>(sa, w, smem);
+        BOSSS_BATCH_CASES(BOSSS_CASE)
+#undef BOSSS_CASE
+        __syncthreads();
+    }
+}
+
+template <class Phys, int MODE>
+static bool batch_supported(int K, int Q) {
+#define BOSSS_SUP(KK, QQ) \
+    if (K == KK && Q == QQ) return Cfg<Phys, KK, QQ, MODE>::SMEM_BYTES <= 227 * 1024;
+    BOSSS_BATCH_CASES(BOSSS_SUP)
+#undef BOSSS_SUP
+    return false;
+}
+
+template <class Phys, int MODE>
+static int cpb_of(int K, int Q) {
+#define BOSSS_CPB(KK, QQ) \
+    if (K == KK && Q == QQ) return Cfg<Phys, KK, QQ, MODE>::CPB;
+    BOSSS_BATCH_CASES(BOSSS_CPB)
+#undef BOSSS_CPB
+    return 1;
+}
+
+using BatchLaunch = cudaError_t (*)(const BatchInst*, const WorkItem*, int, int*, const double*, const double*, double*,
+                                    double, double, double, int, cudaStream_t);
+
+template <class Phys, int MODE>
+static cudaError_t launch_batch(const BatchInst* inst, const WorkItem* items, int nitems, int* counter, const double* U,
+                                const double* V, double* out, double alpha, double beta, double time, int grid,
+                                cudaStream_t s) {
+    constexpr size_t smem = batch_smem<Phys, MODE>();
+    static unsigned long long done = 0ull;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(done & (1ull << (dev & 63)))) {
+        cudaError_t e = cudaFuncSetAttribute(batch_kernel<Phys, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(batch_kernel<Phys, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
+        done |= 1ull << (dev & 63);
+    }
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    batch_kernel<Phys, MODE><<<grid, 256, smem, s>>>(inst, items, nitems, counter, U, V, out, alpha, beta, time);
+    return cudaGetLastError();
+}
+
+template <class Phys, int MODE>
+static int resident_grid() {
+    int dev = 0, nsm = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    constexpr size_t smem = batch_smem<Phys, MODE>();
+    cudaFuncSetAttribute(batch_kernel<Phys, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<Phys, MODE>, 256, smem);
+    return std::max(1, per) * std::max(1, nsm);
+}
+
+}  // namespace bosss
+
+using namespace bosss;
+
+struct bosss_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int phys = 0, D = 0, n = 0;
+    std::vector<bosss_handle*> h;                 // per-instance descriptors (tables, grid, physics)
+    std::vector<long long> dom_off, cod_off;      // n+1 prefix offsets
+    BatchInst* d_inst = nullptr;
+    WorkItem* d_items[3] = {nullptr, nullptr, nullptr};
+    int nitems[3] = {0, 0, 0};
+    int* d_counter = nullptr;                     // two queue counters (two kernels per graph)
+    int grid[3] = {0, 0, 0};
+    std::map<std::pair<int, int>, int> tiles;     // (K, Q) -> tiles per work item (autotuned)
+    bool lpt = true;                              // longest-processing-time-first order
+    cudaGraphExec_t graph = nullptr;
+};
+
+namespace bosss {
+
+static BatchLaunch batch_launcher(int phys, int D, int mode) {
+    if (D != 3) return nullptr;
+    if (phys == PHYS_SIP) {
+        if (mode == MODE_RES) return &launch_batch<PhysScalar<3, true>, MODE_RES>;
+        if (mode == MODE_JVP) return &launch_batch<PhysScalar<3, true>, MODE_JVP>;
+        return &launch_batch<PhysScalar<3, true>, MODE_VJP>;
+    }
+    if (phys == PHYS_TRANSPORT) {
+        if (mode == MODE_RES) return &launch_batch<PhysScalar<3, false>, MODE_RES>;
+        if (mode == MODE_JVP) return &launch_batch<PhysScalar<3, false>, MODE_JVP>;
+        return &launch_batch<PhysScalar<3, false>, MODE_VJP>;
+    }
+    return nullptr;
+}
+
+static bool batch_ok(int phys, int mode, int K, int Q) {
+    if (phys == PHYS_SIP) {
+        if (mode == MODE_RES) return batch_supported<PhysScalar<3, true>, MODE_RES>(K, Q);
+        if (mode == MODE_JVP) return batch_supported<PhysScalar<3, true>, MODE_JVP>(K, Q);
+        return batch_supported<PhysScalar<3, true>, MODE_VJP>(K, Q);
+    }
+    if (mode == MODE_RES) return batch_supported<PhysScalar<3, false>, MODE_RES>(K, Q);
+    if (mode == MODE_JVP) return batch_supported<PhysScalar<3, false>, MODE_JVP>(K, Q);
+    return batch_supported<PhysScalar<3, false>, MODE_VJP>(K, Q);
+}
+
+static int batch_cpb(int phys, int mode, int K, int Q) {
+    if (phys == PHYS_SIP) {
+        if (mode == MODE_RES) return cpb_of<PhysScalar<3, true>, MODE_RES>(K, Q);
+        if (mode == MODE_JVP) return cpb_of<PhysScalar<3, true>, MODE_JVP>(K, Q);
+        return cpb_of<PhysScalar<3, true>, MODE_VJP>(K, Q);
+    }
+    if (mode == MODE_RES) return cpb_of<PhysScalar<3, false>, MODE_RES>(K, Q);
+    if (mode == MODE_JVP) return cpb_of<PhysScalar<3, false>, MODE_JVP>(K, Q);
+    return cpb_of<PhysScalar<3, false>, MODE_VJP>(K, Q);
+}
+
+static int batch_grid(int phys, int mode) {
+    if (phys == PHYS_SIP) {
+        if (mode == MODE_RES) return resident_grid<PhysScalar<3, true>, MODE_RES>();
+        if (mode == MODE_JVP) return resident_grid<PhysScalar<3, true>, MODE_JVP>();
+        return resident_grid<PhysScalar<3, true>, MODE_VJP>();
+    }
+    if (mode == MODE_RES) return resident_grid<PhysScalar<3, false>, MODE_RES>();
+    if (mode == MODE_JVP) return resident_grid<PhysScalar<3, false>, MODE_JVP>();
+    return resident_grid<PhysScalar<3, false>, MODE_VJP>();
+}
+
+// work items of one mode, ordered by the batch's schedule
+static int build_items(bosss_batch* b, int mode) {
+    struct Tmp {
+        WorkItem w;
+        double cost;
+    };
+    std::vector<Tmp> v;
+    for (int i = 0; i < b->n; ++i) {
+        const bosss_handle* h = b->h[i];
+        const int cpb = batch_cpb(b->phys, mode, h->K, h->Q);
+        int r = 1;
+        auto it = b->tiles.find({h->K, h->Q});
+        if (it != b->tiles.end()) r = it->second;
+        const long long J = h->base.g.J, step = (long long)cpb * r;
+        // cost of a cell ~ (quadrature nodes) x (modes)
+        const double cell_cost = (double)h->Q * h->Q * h->Q * (h->K + 1) * (h->K + 2) * (h->K + 3) / 6.0;
+        for (long long c0 = 0; c0 < J; c0 += step) {
+            Tmp t;
+            t.w.inst = i;
+            t.w.ntiles = r;
+            t.w.c0 = c0;
+            t.cost = cell_cost * (double)std::min(step, J - c0);
+            v.push_back(t);
+        }
+    }
+    if (b->lpt)
+        std::stable_sort(v.begin(), v.end(), [](const Tmp& x, const Tmp& y) { return x.cost > y.cost; });
+    std::vector<WorkItem> w(v.size());
+    for (size_t k = 0; k < v.size(); ++k) w[k] = v[k].w;
+    cudaFree(b->d_items[mode]);
+    b->d_items[mode] = nullptr;
+    CUDA_TRY(cudaMalloc(&b->d_items[mode], sizeof(WorkItem) * std::max<size_t>(w.size(), 1)));
+    CUDA_TRY(cudaMemcpy(b->d_items[mode], w.data(), sizeof(WorkItem) * w.size(), cudaMemcpyHostToDevice));
+    b->nitems[mode] = (int)w.size();
+    return BOSSS_OK;
+}
+
+static int batch_run(bosss_batch* b, int mode, double alpha, double beta, const double* U, const double* V, double* out,
+                     double time, cudaStream_t s, int counter_slot) {
+    BatchLaunch L = batch_launcher(b->phys, b->D, mode);
+    if (!L) return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no batched kernel for this physics");
+    CUDA_TRY(L(b->d_inst, b->d_items[mode], b->nitems[mode], b->d_counter + counter_slot, U, V, out, alpha, beta, time,
+               b->grid[mode], s));
+    return BOSSS_OK;
+}
+
+static std::string table_key(int phys, int D, int K, int Q) {
+    std::ostringstream o;
+    o << "phys" << phys << "_D" << D << "_K" << K << "_Q" << Q;
+    return o.str();
+}
+
+}  // namespace bosss
+
+extern "C" {
+
+int bosss_b200_batch_create(int32_t n, const bosss_op_desc* ops, const bosss_grid_desc* grids,
+                            const bosss_options* opt, bosss_batch** out) {
+    if (!ops || !grids || !out || n < 1) return fail(BOSSS_ERR_BAD_ARG, "bad batch arguments");
+    *out = nullptr;
+    bosss_batch* b = new bosss_batch();
+    b->n = n;
+    b->dom_off.assign(1, 0);
+    b->cod_off.assign(1, 0);
+    for (int i = 0; i < n; ++i) {
+        bosss_handle* h = nullptr;
+        int rc = bosss_b200_create(&ops[i], &grids[i], opt, &h);
+        if (rc) {
+            bosss_b200_batch_destroy(b);
+            return rc;
+        }
+        b->h.push_back(h);
+        if (i == 0) {
+            b->phys = h->phys;
+            b->D = h->D;
+            b->device = h->device;
+        } else if (h->phys != b->phys || h->D != b->D || h->device != b->device) {
+            bosss_b200_batch_destroy(b);
+            return fail(BOSSS_ERR_BAD_ARG, "batch instances must share physics family, dimension and device");
+        }
+        for (int m = 0; m < 3; ++m)
+            if (!batch_ok(h->phys, m, h->K, h->Q)) {
+                bosss_b200_batch_destroy(b);
+                return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT,
+                            "no batched kernel for degree " + std::to_string(h->K) + " with " + std::to_string(h->Q) +
+                                " Gauss nodes (batched path: 3D scalar transport / advection-diffusion)");
+            }
+        b->dom_off.push_back(b->dom_off.back() + h->ndom);
+        b->cod_off.push_back(b->cod_off.back() + h->ncod);
+    }
+    if (!batch_launcher(b->phys, b->D, MODE_RES)) {
+        bosss_b200_batch_destroy(b);
+        return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "batched path: 3D scalar transport / advection-diffusion only");
+    }
+    auto bail = [&](cudaError_t e) {
+        bosss_b200_batch_destroy(b);
+        return fail(BOSSS_ERR_CUDA, std::string("batch setup: ") + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    std::vector<BatchInst> hi(n);
+    for (int i = 0; i < n; ++i) {
+        hi[i].a = b->h[i]->base;
+        hi[i].dom_off = b->dom_off[i];
+        hi[i].cod_off = b->cod_off[i];
+        hi[i].K = b->h[i]->K;
+        hi[i].Q = b->h[i]->Q;
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_inst, sizeof(BatchInst) * n);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_inst, hi.data(), sizeof(BatchInst) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(int) * 2);
+    if (e != cudaSuccess) return bail(e);
+    for (int m = 0; m < 3; ++m) {
+        b->grid[m] = batch_grid(b->phys, m);
+        int rc = build_items(b, m);
+        if (rc) {
+            bosss_b200_batch_destroy(b);
+            return rc;
+        }
+    }
+    *out = b;
+    return BOSSS_OK;
+}
+
+int bosss_b200_batch_destroy(bosss_batch* b) {
+    if (!b) return BOSSS_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (int m = 0; m < 3; ++m) cudaFree(b->d_items[m]);
+    cudaFree(b->d_inst);
+    cudaFree(b->d_counter);
+    for (auto* h : b->h) bosss_b200_destroy(h);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return BOSSS_OK;
+}
+
+int bosss_b200_batch_get_sizes(const bosss_batch* b, int64_t* domain_offsets, int64_t* codomain_offsets) {
+    if (!b) return fail(BOSSS_ERR_BAD_ARG, "null batch");
+    for (int i = 0; i <= b->n; ++i) {
+        if (domain_offsets) domain_offsets[i] = b->dom_off[i];
+        if (codomain_offsets) codomain_offsets[i] = b->cod_off[i];
+    }
+    return BOSSS_OK;
+}
+
+int bosss_b200_batch_evaluate_device(bosss_batch* b, int32_t mode, double alpha, double beta, const double* U_dev,
+                                     const double* V_dev, double* out_dev, double time, void* stream) {
+    if (!b || !U_dev || !out_dev || mode < 0 || mode > 2) return fail(BOSSS_ERR_BAD_ARG, "bad argument");
+    if (mode != MODE_RES && !V_dev) return fail(BOSSS_ERR_BAD_ARG, "JVP/VJP need a second vector");
+    CUDA_TRY(cudaSetDevice(b->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
+    return batch_run(b, mode, alpha, beta, U_dev, V_dev, out_dev, time, s, 0);
+}
+
+int bosss_b200_batch_evaluate(bosss_batch* b, int32_t mode, double alpha, double beta, const double* U,
+                              const double* V, double* out, double time) {
+    if (!b || !U || !out || mode < 0 || mode > 2) return fail(BOSSS_ERR_BAD_ARG, "bad argument");
+    if (mode != MODE_RES && !V) return fail(BOSSS_ERR_BAD_ARG, "JVP/VJP need a second vector");
+    CUDA_TRY(cudaSetDevice(b->device));
+    const long long nd = b->dom_off.back(), nc = b->cod_off.back();
+    const long long nin2 = (mode == MODE_VJP) ? nc : nd, nout = (mode == MODE_VJP) ? nd : nc;
+    double *dU = nullptr, *dV = nullptr, *dO = nullptr;
+    cudaStream_t s = b->stream;
+    auto cleanup = [&]() {
+        cudaFree(dU);
+        cudaFree(dV);
+        cudaFree(dO);
+    };
+    cudaError_t e = cudaMalloc(&dU, sizeof(double) * nd);
+    if (e == cudaSuccess && mode != MODE_RES) e = cudaMalloc(&dV, sizeof(double) * nin2);
+    if (e == cudaSuccess) e = cudaMalloc(&dO, sizeof(double) * nout);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dU, U, sizeof(double) * nd, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && dV) e = cudaMemcpyAsync(dV, V, sizeof(double) * nin2, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && mode == MODE_RES && beta != 0.0)
+        e = cudaMemcpyAsync(dO, out, sizeof(double) * nout, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        cleanup();
+        return fail(BOSSS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    int rc = batch_run(b, mode, alpha, beta, dU, dV, dO, time, s, 0);
+    if (!rc) {
+        e = cudaMemcpyAsync(out, dO, sizeof(double) * nout, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(BOSSS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cleanup();
+    return rc;
+}
+
+int bosss_b200_batch_capture(bosss_batch* b, const double* U_dev, const double* W_dev, double* R_dev, double* G_dev,
+                             double time) {
+    if (!b || !U_dev || !W_dev || !R_dev || !G_dev) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(b->device));
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = batch_run(b, MODE_RES, 1.0, 0.0, U_dev, nullptr, R_dev, time, b->stream, 0);
+    if (!rc) rc = batch_run(b, MODE_VJP, 1.0, 0.0, U_dev, W_dev, G_dev, time, b->stream, 1);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(BOSSS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(BOSSS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return BOSSS_OK;
+}
+
+int bosss_b200_batch_replay(bosss_batch* b, void* stream) {
+    if (!b || !b->graph) return fail(BOSSS_ERR_BAD_ARG, "no captured graph");
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaGraphLaunch(b->graph, stream ? (cudaStream_t)stream : b->stream));
+    return BOSSS_OK;
+}
+
+int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double* W_dev, double* R_dev, double* G_dev,
+                              const char* table_path) {
+    if (!b || !U_dev || !W_dev || !R_dev || !G_dev) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(b->device));
+    // persisted table: "<key> <tiles>" per line, plus "schedule lpt|fifo"
+    std::map<std::string, int> table;
+    bool have_sched = false, lpt = true;
+    if (table_path && *table_path) {
+        std::ifstream f(table_path);
+        std::string k;
+        int v = 0;
+        while (f >> k) {
+            if (k == "schedule") {
+                std::string sv;
+                f >> sv;
+                have_sched = true;
+                lpt = (sv == "lpt");
+            } else if (f >> v) {
+                table[k] = v;
+            }
+        }
+    }
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    auto time_once = [&](float& ms) -> int {
+        for (int m : {MODE_RES, MODE_VJP}) {
+            int rc = build_items(b, m);
+            if (rc) return rc;
+        }
+        for (int rep = 0; rep < 2; ++rep) {   // warm-up
+            int rc = batch_run(b, MODE_RES, 1.0, 0.0, U_dev, nullptr, R_dev, 0.0, b->stream, 0);
+            if (!rc) rc = batch_run(b, MODE_VJP, 1.0, 0.0, U_dev, W_dev, G_dev, 0.0, b->stream, 1);
+            if (rc) return rc;
+        }
+        CUDA_TRY(cudaEventRecord(e0, b->stream));
+        for (int rep = 0; rep < 3; ++rep) {
+            int rc = batch_run(b, MODE_RES, 1.0, 0.0, U_dev, nullptr, R_dev, 0.0, b->stream, 0);
+            if (!rc) rc = batch_run(b, MODE_VJP, 1.0, 0.0, U_dev, W_dev, G_dev, 0.0, b->stream, 1);
+            if (rc) return rc;
+        }
+        CUDA_TRY(cudaEventRecord(e1, b->stream));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        return BOSSS_OK;
+    };
+    // classes present in the batch
+    std::vector<std::pair<int, int>> classes;
+    for (auto* h : b->h)
+        if (std::find(classes.begin(), classes.end(), std::make_pair(h->K, h->Q)) == classes.end())
+            classes.push_back({h->K, h->Q});
+    int rc = 0;
+    for (auto kq : classes) {
+        const std::string key = table_key(b->phys, b->D, kq.first, kq.second);
+        if (table.count(key)) {
+            b->tiles[kq] = table[key];
+            continue;
+        }
+        int best = 1;
+        float best_ms = 1e30f;
+        for (int r : {1, 2, 4, 8}) {
+            b->tiles[kq] = r;
+            float ms = 0.f;
+            rc = time_once(ms);
+            if (rc) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = r;
+            }
+        }
+        if (rc) break;
+        b->tiles[kq] = best;
+        table[key] = best;
+    }
+    if (!rc) {
+        if (have_sched) {
+            b->lpt = lpt;
+        } else {
+            float ms_l = 0.f, ms_f = 0.f;
+            b->lpt = true;
+            rc = time_once(ms_l);
+            if (!rc) {
+                b->lpt = false;
+                rc = time_once(ms_f);
+            }
+            b->lpt = rc ? true : (ms_l <= ms_f);
+        }
+        for (int m = 0; m < 3 && !rc; ++m) rc = build_items(b, m);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (table_path && *table_path) {
+        std::ofstream f(table_path);
+        for (auto& kv : table) f << kv.first << " " << kv.second << "\n";
+        f << "schedule " << (b->lpt ? "lpt" : "fifo") << "\n";
+    }
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;   // items changed: the caller re-captures
+    }
+    return BOSSS_OK;
+}
+
+int bosss_b200_batch_tiles(const bosss_batch* b, int32_t K, int32_t Q, int32_t* tiles, int32_t* lpt) {
+    if (!b) return fail(BOSSS_ERR_BAD_ARG, "null batch");
+    auto it = b->tiles.find({K, Q});
+    if (tiles) *tiles = (it == b->tiles.end()) ? 1 : it->second;
+    if (lpt) *lpt = b->lpt ? 1 : 0;
+    return BOSSS_OK;
+}
+
+}  // extern "C"

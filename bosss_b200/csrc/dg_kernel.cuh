@@ -123,18 +123,19 @@ __device__ __forceinline__ double cell_cj(const GridConst& g, const int* ijk) {
     return 0.5 * cj;
 }
 
-// ------------------------------------------------------------------ the kernel
+// ------------------------------------------------------------------ one tile
+// Evaluates the tile of cells [c0, c0 + CPB) of one operator instance; all NT threads of
+// the CTA take part. Used by dg_cell_kernel (one tile per CTA) and by the persistent
+// batched kernel (tiles of many instances pulled from a work queue).
 template <class Phys, int K, int Q, int MODE>
-__global__ void __launch_bounds__(256) dg_cell_kernel(const __grid_constant__ EvalArgs args) {
+__device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, double* smem) {
     using C = Cfg<Phys, K, Q, MODE>;
     constexpr int D = C::D, NP = C::NP, QF = C::QF, QV = C::QV, NV = C::NV, NC = C::NC;
     constexpr int NFI = C::NFI, NCI = C::NCI, NO = C::NO, NCO = C::NCO, CPB = C::CPB, NT = C::NT;
     constexpr int NPAIR = C::NPAIR;
-    extern __shared__ double smem[];
 
     const GridConst& g = args.g;
     const int tid = threadIdx.x;
-    const long long c0 = (long long)blockIdx.x * CPB;
     const int ncell = (int)((g.J - c0) < CPB ? (g.J - c0) : CPB);
 
     // ---- carve shared memory
@@ -867,6 +868,13 @@ __global__ void __launch_bounds__(256) dg_cell_kernel(const __grid_constant__ Ev
             args.out[gi] = v;
         }
     }
+}
+
+// ------------------------------------------------------------------ the kernel
+template <class Phys, int K, int Q, int MODE>
+__global__ void __launch_bounds__(256) dg_cell_kernel(const __grid_constant__ EvalArgs args) {
+    extern __shared__ double smem[];
+    cell_tile<Phys, K, Q, MODE>(args, (long long)blockIdx.x * Cfg<Phys, K, Q, MODE>::CPB, smem);
 }
 
 }  // namespace bosss

@@ -501,3 +501,75 @@ class Evaluator:
         out = np.empty(self.n_domain) if out is None else out
         C.check(C.lib().bosss_b200_vjp(self.handle, C.ptr(U), C.ptr(W), C.ptr(out), self.time))
         return out
+
+
+class BatchEvaluator:
+    """Independent operator instances evaluated by one persistent launch per mode.
+
+    ``problems``: list of objects with ``descs()`` (operator and grid descriptors), e.g.
+    :class:`bosss_b200.problems.Problem`. Vectors are the concatenation of the
+    instances' vectors; ``offsets`` gives the instance boundaries."""
+
+    def __init__(self, problems, device=0):
+        self.handle = None
+        descs = [p.descs() for p in problems]
+        self.n = len(descs)
+        self._ops = (C.OpDesc * self.n)(*[d[0] for d in descs])
+        self._grids = (C.GridDesc * self.n)(*[d[1] for d in descs])
+        opt = C.Options()
+        opt.device = int(device)
+        h = ctypes.c_void_p()
+        C.check(C.lib().bosss_b200_batch_create(self.n, ctypes.byref(self._ops), ctypes.byref(self._grids),
+                                                ctypes.byref(opt), ctypes.byref(h)))
+        self.handle = h
+        self.dom_offsets = np.zeros(self.n + 1, dtype=np.int64)
+        self.cod_offsets = np.zeros(self.n + 1, dtype=np.int64)
+        C.check(C.lib().bosss_b200_batch_get_sizes(h, C.ptr(self.dom_offsets), C.ptr(self.cod_offsets)))
+
+    def Dispose(self):
+        if self.handle:
+            C.lib().bosss_b200_batch_destroy(self.handle)
+            self.handle = None
+
+    __del__ = Dispose
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.Dispose()
+
+    def evaluate(self, mode, U, V=None, out=None, alpha=1.0, beta=0.0):
+        """Host or CUDA-tensor buffers (device path enqueued on the current torch stream)."""
+        nout = int(self.dom_offsets[-1] if mode == C.MODE_VJP else self.cod_offsets[-1])
+        if hasattr(U, "is_cuda") and U.is_cuda:
+            import torch
+            out = torch.zeros(nout, dtype=torch.float64, device=U.device) if out is None else out
+            s = torch.cuda.current_stream().cuda_stream
+            C.check(C.lib().bosss_b200_batch_evaluate_device(self.handle, mode, alpha, beta, C.ptr(U), C.ptr(V),
+                                                             C.ptr(out), 0.0,
+                                                             ctypes.c_void_p(s if s else C.CUDA_STREAM_LEGACY)))
+            return out
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        V = None if V is None else np.ascontiguousarray(V, dtype=np.float64)
+        out = np.zeros(nout) if out is None else out
+        C.check(C.lib().bosss_b200_batch_evaluate(self.handle, mode, alpha, beta, C.ptr(U), C.ptr(V), C.ptr(out), 0.0))
+        return out
+
+    def capture(self, U, W, R, G):
+        """Capture residual R = Op(U) and adjoint G = J^T W (CUDA tensors) into a CUDA graph."""
+        C.check(C.lib().bosss_b200_batch_capture(self.handle, C.ptr(U), C.ptr(W), C.ptr(R), C.ptr(G), 0.0))
+
+    def replay(self, stream=None):
+        import torch
+        s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        C.check(C.lib().bosss_b200_batch_replay(self.handle, ctypes.c_void_p(s if s else C.CUDA_STREAM_LEGACY)))
+
+    def autotune(self, U, W, R, G, table_path=None):
+        C.check(C.lib().bosss_b200_batch_autotune(self.handle, C.ptr(U), C.ptr(W), C.ptr(R), C.ptr(G),
+                                                  table_path.encode() if table_path else None))
+
+    def tiles(self, K, Q):
+        t, lpt = ctypes.c_int32(), ctypes.c_int32()
+        C.check(C.lib().bosss_b200_batch_tiles(self.handle, K, Q, ctypes.byref(t), ctypes.byref(lpt)))
+        return t.value, bool(lpt.value)

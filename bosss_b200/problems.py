@@ -179,3 +179,14 @@ def advection_diffusion3d(n=16, k=2, seed=5000, nu=0.01, penalty_base=4.0, veloc
     return Problem("advection_diffusion3d", op, g, [u], [r_], U,
                    {"workload": "advdiff_%d^3_k%d" % (n, k), "cells": g.NoOfCells, "k": k, "seed": seed,
                     "velocity": list(map(float, a)), "nu": nu})
+
+
+def batched_advection_diffusion(n_instances=256, seed=5000, sizes=(16, 24, 32, 48), degrees=(1, 2, 3, 4), nu=0.01):
+    """The batched mixed workload: independent advection-diffusion instances with grid
+    sizes drawn from ``sizes``^3 and DG degrees from ``degrees`` (seeded), each with its
+    own velocity a ~ U[-1,1]^3 and FP64 coefficients U[-1,1]; periodic, Linear() order."""
+    r = rng(seed)
+    ns = r.choice(sizes, n_instances)
+    ks = r.choice(degrees, n_instances)
+    return [advection_diffusion3d(n=int(n), k=int(k), seed=seed * 1000 + i, nu=nu)
+            for i, (n, k) in enumerate(zip(ns, ks))]

@@ -241,6 +241,38 @@ int bosss_b200_bsr_solve(bosss_bsr* A, const double* b, double* x, const bosss_s
  * BlockMsrMatrix.AccBlock): exact linearisation, cell-block pattern = self + face neighbours. */
 int bosss_b200_compute_jacobian(bosss_handle* h, const double* U, double time, bosss_bsr** out);
 
+/* ---- batched evaluation ----
+ * Many independent operator instances (own grid, DG degree and quadrature rule each,
+ * same physics family; device path: 3D scalar transport / advection-diffusion) evaluated
+ * by ONE persistent launch per mode: CTAs pull (instance, cell tile) work items from a
+ * queue in device memory. Vectors are the concatenation of the instances' vectors
+ * (offsets from bosss_b200_batch_get_sizes). The residual + VJP pair can be captured once
+ * into a CUDA graph and replayed; an autotuner picks the cell tiles per work item for each
+ * (degree, quadrature nodes) class and the queue order, persisted in a small text table. */
+typedef struct bosss_batch bosss_batch;
+
+enum bosss_eval_mode { BOSSS_MODE_RESIDUAL = 0, BOSSS_MODE_JVP = 1, BOSSS_MODE_VJP = 2 };
+
+int bosss_b200_batch_create(int32_t n, const bosss_op_desc* ops, const bosss_grid_desc* grids,
+                            const bosss_options* opt, bosss_batch** out);
+int bosss_b200_batch_destroy(bosss_batch* b);
+/* prefix offsets (n+1 entries each) of the instances in the concatenated vectors */
+int bosss_b200_batch_get_sizes(const bosss_batch* b, int64_t* domain_offsets, int64_t* codomain_offsets);
+/* mode RESIDUAL: out = beta*out + alpha*Op(U); JVP: out = J(U) V; VJP: out = J(U)^T V. Host buffers. */
+int bosss_b200_batch_evaluate(bosss_batch* b, int32_t mode, double alpha, double beta, const double* U,
+                              const double* V, double* out, double time);
+int bosss_b200_batch_evaluate_device(bosss_batch* b, int32_t mode, double alpha, double beta, const double* U_dev,
+                                     const double* V_dev, double* out_dev, double time, void* stream);
+/* capture R = Op(U) and G = J(U)^T W for all instances into a CUDA graph (device buffers) */
+int bosss_b200_batch_capture(bosss_batch* b, const double* U_dev, const double* W_dev, double* R_dev, double* G_dev,
+                             double time);
+int bosss_b200_batch_replay(bosss_batch* b, void* stream);
+/* time candidate tile counts per (degree, nodes) class and the queue order on the given
+ * buffers; reads/writes the text table at table_path (NULL: no persistence) */
+int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double* W_dev, double* R_dev, double* G_dev,
+                              const char* table_path);
+int bosss_b200_batch_tiles(const bosss_batch* b, int32_t K, int32_t Q, int32_t* tiles, int32_t* lpt);
+
 #ifdef __cplusplus
 }
 #endif
