@@ -170,6 +170,8 @@ SIGNATURES = {
     "bosss_b200_batch_replay": (ctypes.c_int, [_P, _P]),
     "bosss_b200_batch_autotune": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_char_p]),
     "bosss_b200_batch_tiles": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _I32, _I32]),
+    "bosss_b200_batch_evaluate_noalloc": (ctypes.c_int, [ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_double,
+                                                         ctypes.c_double, _P, _P, _P, ctypes.c_double, _P]),
 }
 
 _lib = None

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -556,3 +557,193 @@ int bosss_b200_batch_tiles(const bosss_batch* b, int32_t K, int32_t Q, int32_t* 
 }
 
 }  // extern "C"
+
+// ======================================================================================
+// Batched evaluation that allocates nothing.
+//
+// Some callers cannot call cudaMalloc: code that must not allocate device memory while it
+// runs (a host application whose device memory is owned by another allocator or pool, or
+// a time-critical loop where an allocation would synchronise the device). For them,
+// bosss_b200_batch_evaluate_noalloc evaluates a batch of single-instance handles with the
+// same persistent kernel design, but its scratch -- the work-queue counter, the instance
+// table and the per-instance tile prefix sums -- lives in the file-scope device array
+// below, of fixed size. The handles come from bosss_b200_create, which allocates no
+// device memory; inputs and outputs are the caller's device buffers.
+// ======================================================================================
+namespace bosss {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = 1u << 20;   // 1 MiB
+constexpr int NOALLOC_MAX_INSTANCES = 512;
+
+// Shared by every call on a device: each call overwrites it, so calls whose kernels
+// overlap on the GPU race on it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+struct NoallocLayout {
+    static constexpr size_t counter = 0;                       // int, cleared by every call
+    static constexpr size_t inst = 256;                        // BatchInst[n]
+    static size_t prefix(int n) { return inst + ((sizeof(BatchInst) * n + 255) / 256) * 256; }   // long long[n+1]
+    static size_t bytes(int n) { return prefix(n) + sizeof(long long) * (n + 1); }
+};
+
+template <class Phys, int MODE>
+__global__ void __launch_bounds__(256) batch_kernel_noalloc(unsigned char* scratch, int n, const double* U,
+                                                            const double* V, double* out, double alpha, double beta,
+                                                            double time, size_t prefix_off) {
+    extern __shared__ double smem[];
+    __shared__ EvalArgs sa;
+    __shared__ WorkItem w;
+    __shared__ int K, Q;
+    int* counter = reinterpret_cast<int*>(scratch + NoallocLayout::counter);
+    const BatchInst* inst = reinterpret_cast<const BatchInst*>(scratch + NoallocLayout::inst);
+    const long long* prefix = reinterpret_cast<const long long*>(scratch + prefix_off);
+    const long long total = prefix[n];
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long it = atomicAdd(counter, 1);
+            w.inst = -1;
+            if (it < total) {
+                int lo = 0, hi = n;   // prefix[lo] <= it < prefix[hi]
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) / 2;
+                    if (prefix[mid] <= it) lo = mid;
+                    else hi = mid;
+                }
+                w.inst = lo;
+                w.ntiles = 1;
+                w.c0 = it - prefix[lo];   // tile index; scaled by the instance's tile size below
+            }
+        }
+        __syncthreads();
+        if (w.inst < 0) break;
+        const BatchInst* b = inst + w.inst;
+        for (int i = threadIdx.x; i < (int)(sizeof(EvalArgs) / 8); i += blockDim.x)
+            reinterpret_cast<double*>(&sa)[i] = reinterpret_cast<const double*>(&b->a)[i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            sa.U = U + b->dom_off;
+            sa.V = V ? V + ((MODE == MODE_VJP) ? b->cod_off : b->dom_off) : nullptr;
+            sa.out = out + ((MODE == MODE_VJP) ? b->dom_off : b->cod_off);
+            sa.alpha = alpha;
+            sa.beta = beta;
+            sa.time = time;
+            K = b->K;
+            Q = b->Q;
+        }
+        __syncthreads();
+#define BOSSS_CASE(KK, QQ)                                                     \
+    if (K == KK && Q == QQ) {                                                 \
+        WorkItem wt = w;                                                      \
+        wt.c0 *= Cfg<Phys, KK, QQ, MODE>::CPB;                                 \
+        run_item<Phys, KK, QQ, MODE>(sa, wt, smem);                           \
+    }
+        BOSSS_BATCH_CASES(BOSSS_CASE)
+#undef BOSSS_CASE
+        __syncthreads();
+    }
+}
+
+template <class Phys, int MODE>
+static cudaError_t launch_noalloc(unsigned char* scratch, int n, const double* U, const double* V, double* out,
+                                  double alpha, double beta, double time, size_t prefix_off, cudaStream_t s) {
+    constexpr size_t smem = batch_smem<Phys, MODE>();
+    cudaError_t e = cudaFuncSetAttribute(batch_kernel_noalloc<Phys, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel_noalloc<Phys, MODE>, 256, smem);
+    batch_kernel_noalloc<Phys, MODE><<<std::max(1, per) * std::max(1, nsm), 256, smem, s>>>(scratch, n, U, V, out, alpha,
+                                                                                          beta, time, prefix_off);
+    return cudaGetLastError();
+}
+
+// device address of the scratch array, looked up once per device (first call on it)
+static unsigned char* noalloc_scratch_ptr(int dev, int& rc) {
+    static std::mutex mu;
+    static unsigned char* ptrs[64] = {nullptr};
+    rc = 0;
+    if (dev < 0 || dev >= 64) {
+        rc = fail(BOSSS_ERR_BAD_ARG, "device ordinal out of range");
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptrs[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            rc = fail(BOSSS_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch array: ") + cudaGetErrorString(e));
+            return nullptr;
+        }
+        ptrs[dev] = static_cast<unsigned char*>(p);
+    }
+    return ptrs[dev];
+}
+
+}  // namespace bosss
+
+extern "C" int bosss_b200_batch_evaluate_noalloc(int32_t n, bosss_handle* const* instances, int32_t mode, double alpha,
+                                                 double beta, const double* U_dev, const double* V_dev, double* out_dev,
+                                                 double time, void* stream) {
+    if (!instances || !U_dev || !out_dev || mode < 0 || mode > 2) return fail(BOSSS_ERR_BAD_ARG, "bad argument");
+    if (mode != MODE_RES && !V_dev) return fail(BOSSS_ERR_BAD_ARG, "JVP/VJP need a second vector");
+    if (n < 1 || n > NOALLOC_MAX_INSTANCES || NoallocLayout::bytes(n) > NOALLOC_SCRATCH_BYTES)
+        return fail(BOSSS_ERR_BAD_ARG, "allocation-free batch: between 1 and " + std::to_string(NOALLOC_MAX_INSTANCES) +
+                                           " instances (scratch array of " +
+                                           std::to_string(NOALLOC_SCRATCH_BYTES >> 10) + " KiB)");
+    const bosss_handle* h0 = instances[0];
+    if (!h0) return fail(BOSSS_ERR_BAD_ARG, "null instance handle");
+    const int phys = h0->phys, D = h0->D, dev = h0->device;
+    if (D != 3 || (phys != PHYS_SIP && phys != PHYS_TRANSPORT))
+        return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "allocation-free batch: 3D scalar transport / advection-diffusion");
+    // pack the instance table and tile prefix sums in a fixed host staging area
+    static std::mutex stage_mu;
+    static BatchInst stage_inst[NOALLOC_MAX_INSTANCES];
+    static long long stage_prefix[NOALLOC_MAX_INSTANCES + 1];
+    std::lock_guard<std::mutex> lock(stage_mu);
+    long long doff = 0, coff = 0;
+    stage_prefix[0] = 0;
+    for (int i = 0; i < n; ++i) {
+        const bosss_handle* h = instances[i];
+        if (!h || h->phys != phys || h->D != D || h->device != dev)
+            return fail(BOSSS_ERR_BAD_ARG, "instances must share physics family, dimension and device");
+        for (int m = 0; m < 3; ++m)
+            if (!batch_ok(phys, m, h->K, h->Q))
+                return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no batched kernel for degree " + std::to_string(h->K) +
+                                                                 " with " + std::to_string(h->Q) + " Gauss nodes");
+        stage_inst[i].a = h->base;
+        stage_inst[i].dom_off = doff;
+        stage_inst[i].cod_off = coff;
+        stage_inst[i].K = h->K;
+        stage_inst[i].Q = h->Q;
+        doff += h->ndom;
+        coff += h->ncod;
+        const long long cpb = batch_cpb(phys, mode, h->K, h->Q);
+        stage_prefix[i + 1] = stage_prefix[i] + (h->base.g.J + cpb - 1) / cpb;
+    }
+    if (stage_prefix[n] > 2000000000LL) return fail(BOSSS_ERR_BAD_ARG, "allocation-free batch: too many cell tiles");
+    CUDA_TRY(cudaSetDevice(dev));
+    int rc = 0;
+    unsigned char* scratch = noalloc_scratch_ptr(dev, rc);
+    if (rc) return rc;
+    cudaStream_t s = stream ? (cudaStream_t)stream : h0->stream;
+    const size_t poff = NoallocLayout::prefix(n);
+    CUDA_TRY(cudaMemsetAsync(scratch + NoallocLayout::counter, 0, sizeof(int), s));
+    CUDA_TRY(cudaMemcpyAsync(scratch + NoallocLayout::inst, stage_inst, sizeof(BatchInst) * n, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(scratch + poff, stage_prefix, sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, s));
+    cudaError_t e;
+    if (phys == PHYS_SIP) {
+        e = (mode == MODE_RES) ? launch_noalloc<PhysScalar<3, true>, MODE_RES>(scratch, n, U_dev, V_dev, out_dev, alpha, beta, time, poff, s)
+          : (mode == MODE_JVP) ? launch_noalloc<PhysScalar<3, true>, MODE_JVP>(scratch, n, U_dev, V_dev, out_dev, alpha, beta, time, poff, s)
+                               : launch_noalloc<PhysScalar<3, true>, MODE_VJP>(scratch, n, U_dev, V_dev, out_dev, alpha, beta, time, poff, s);
+    } else {
+        e = (mode == MODE_RES) ? launch_noalloc<PhysScalar<3, false>, MODE_RES>(scratch, n, U_dev, V_dev, out_dev, alpha, beta, time, poff, s)
+          : (mode == MODE_JVP) ? launch_noalloc<PhysScalar<3, false>, MODE_JVP>(scratch, n, U_dev, V_dev, out_dev, alpha, beta, time, poff, s)
+                               : launch_noalloc<PhysScalar<3, false>, MODE_VJP>(scratch, n, U_dev, V_dev, out_dev, alpha, beta, time, poff, s);
+    }
+    if (e != cudaSuccess) return fail(BOSSS_ERR_CUDA, std::string("allocation-free batch launch: ") + cudaGetErrorString(e));
+    // the host staging area is reused by the next call: wait until the copies have read it
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return BOSSS_OK;
+}

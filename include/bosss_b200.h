@@ -273,6 +273,24 @@ int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double*
                               const char* table_path);
 int bosss_b200_batch_tiles(const bosss_batch* b, int32_t K, int32_t Q, int32_t* tiles, int32_t* lpt);
 
+/* Batched evaluation that allocates no device memory (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc: hosts whose device memory belongs to another
+ * allocator, or loops that must not synchronise the device with an allocation. Same
+ * persistent kernel as the batch above, but its scratch (work-queue counter, instance
+ * table, tile prefix sums) lives in a fixed 1 MiB device array inside the library, held
+ * by every GPU that loads the library until exit: at most 512 instances per call; larger
+ * batches are rejected with BOSSS_ERR_BAD_ARG. `instances`: n handles from
+ * bosss_b200_create (which allocates no device memory), same physics family (3D scalar
+ * transport / advection-diffusion); vectors are the caller's device buffers, the
+ * concatenation of the instances' vectors in the given order; modes as above. The first
+ * call on a device looks up the array's device address; make that first call before any
+ * stream capture. Every call overwrites the shared array (the queue counter is cleared
+ * by each call), so calls whose kernels overlap on the GPU race; the call returns after
+ * its launch has been enqueued and its staging copies have completed. */
+int bosss_b200_batch_evaluate_noalloc(int32_t n, bosss_handle* const* instances, int32_t mode, double alpha,
+                                      double beta, const double* U_dev, const double* V_dev, double* out_dev,
+                                      double time, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
