@@ -117,6 +117,18 @@ class SolverReport(ctypes.Structure):
     ]
 
 
+class LevelSetDesc(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("params", ctypes.c_double * 8)]
+
+
+class XdgOpts(ctypes.Structure):
+    _fields_ = [("cut_nodes_1d", ctypes.c_int32), ("fallback_nodes_1d", ctypes.c_int32),
+                ("moment_degree", ctypes.c_int32), ("subdivision", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8)]
+
+
+LEVELSET_SPHERE = 1
+
+
 class Options(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32),
@@ -170,6 +182,16 @@ SIGNATURES = {
     "bosss_b200_batch_replay": (ctypes.c_int, [_P, _P]),
     "bosss_b200_batch_autotune": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_char_p]),
     "bosss_b200_batch_tiles": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _I32, _I32]),
+    "bosss_b200_xdg_create": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(LevelSetDesc), ctypes.POINTER(XdgOpts),
+                                             ctypes.POINTER(Options), ctypes.POINTER(_P)]),
+    "bosss_b200_xdg_destroy": (ctypes.c_int, [_P]),
+    "bosss_b200_xdg_info": (ctypes.c_int, [_P, ctypes.c_int32, _I64, _I64, _I64, _I32, _I32, _I32, _D]),
+    "bosss_b200_xdg_get_rules": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P]),
+    "bosss_b200_xdg_get_moments": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
+    "bosss_b200_xdg_evaluate": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_double, _P, _P,
+                                               ctypes.c_double]),
+    "bosss_b200_xdg_evaluate_device": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_double, _P, _P,
+                                                      ctypes.c_double, _P]),
     "bosss_b200_batch_evaluate_noalloc": (ctypes.c_int, [ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_double,
                                                          ctypes.c_double, _P, _P, _P, ctypes.c_double, _P]),
 }

@@ -41,6 +41,13 @@ struct EvalArgs {
     double* out;       // RES/JVP: codomain layout; VJP: domain layout
     double alpha, beta;
     double time;
+    // optional species masks of the XDG bulk evaluation (null: every cell and face):
+    // vol_flag[j] == 1 -> the cell's volume integral uses the standard rule;
+    // face_flag[j*2D + 2d + s] == 1 -> face (d, s) of cell j uses the standard rule.
+    // Any other value: the term is skipped here (not in the species, or integrated with a
+    // cut-cell rule by the explicit-rule kernel).
+    const unsigned char* vol_flag;
+    const unsigned char* face_flag;
 };
 
 template <class Phys, int K, int Q, int MODE>
@@ -300,6 +307,11 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
         for (int it = tid; it < CPB * QV; it += NT) {
             const int q = it % QV, cl = it / QV;
             if (cl >= ncell) continue;
+            if (args.vol_flag && args.vol_flag[c0 + cl] != 1) {
+                double* no0 = NOUT(cl);
+                for (int e = 0; e < NO * NCO; ++e) no0[e * QV + q] = 0.0;
+                continue;
+            }
             int qi[3] = {q % Q, (q / Q) % Q, q / (Q * Q)};
             double W = 1.0;
             double x[3] = {0, 0, 0};
@@ -636,6 +648,11 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
         for (int it = tid; it < 2 * CPB * QF; it += NT) {
             const int qf = it % QF, cl = (it / QF) % CPB, s = it / (QF * CPB);
             if (cl >= ncell) continue;
+            if (args.face_flag && args.face_flag[(c0 + cl) * (2 * D) + 2 * d + s] != 1) {
+                double* fo0 = FOUT(cl) + s * NO * NCO * QF;
+                for (int e = 0; e < NO * NCO; ++e) fo0[e * QF + qf] = 0.0;
+                continue;
+            }
             int ijk[3];
             cell_ijk(g, c0 + cl, ijk);
             const long long nb = neighbour(g, ijk, d, s);

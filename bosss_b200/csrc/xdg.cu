@@ -1,0 +1,871 @@
+// xdg.cu -- XDG bulk evaluation with moment-fitted cut-cell rules.
+//
+// Reference counterparts:
+//  * XEvaluatorNonlin.Evaluate, per-species bulk part (XSpatialOperatorMk2_XEvaluators.cs:372-511,
+//    SpeciesBulkEval per species :409-430): each species s evaluates its bulk operator (here
+//    XLaplace_Bulk = SIPLaplace with nu = mu_s, XLaplace.cs:50-120) on the cells and faces that
+//    contain s, with species-restricted quadrature on cut cells;
+//  * cut-cell volume and face rules by moment fitting (LevelSetComboRuleFactory2.cs:300-528):
+//    candidate nodes, moments b_m = int_{K cap s} phi_m, min-norm least squares
+//    w = argmin |w| s.t. Phi w = b (IMatrixExtensions.cs:2318-2340, LAPACK DGELSY).
+//
+// Split of the work: the uncut cells and faces of a species go through the tensor kernel with
+// species masks (EvalArgs::vol_flag / face_flag); the cut cells and cut faces go through
+// the explicit-rule kernel below, which adds its contributions with atomics. Moments are
+// integrated on the device by two-level uniform subdivision of the cell (or face) with
+// tensor Gauss rules per sub-box (exact on uncut sub-boxes); the weights are solved on the
+// device in FP64 per rule (Gram matrix, Cholesky, degree reduced on loss of rank).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "handle.h"
+
+namespace bosss {
+
+constexpr int XDG_MAXM = 35;     // moments of degree <= 4 in 3D
+constexpr int XDG_MAXN = 128;    // nodes per rule
+
+struct LevelSetDev {
+    int type;
+    double c[3];
+    double r;
+};
+
+__host__ __device__ inline double ls_phi(const LevelSetDev& L, const double* x) {
+    const double a = x[0] - L.c[0], b = x[1] - L.c[1], c = x[2] - L.c[2];
+    return sqrt(a * a + b * b + c * c) - L.r;
+}
+
+// sign classification of an axis-aligned box [lo, hi] for the sphere:
+// -1 fully inside (phi < 0), +1 fully outside, 0 cut
+__host__ __device__ inline int ls_box(const LevelSetDev& L, const double* lo, const double* hi, int dim_mask) {
+    double dmin2 = 0.0, dmax2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        if (!(dim_mask & (1 << d))) {   // degenerate direction (face): lo == hi
+            const double v = lo[d] - L.c[d];
+            dmin2 += v * v;
+            dmax2 += v * v;
+            continue;
+        }
+        const double cl = fmin(fmax(L.c[d], lo[d]), hi[d]) - L.c[d];
+        dmin2 += cl * cl;
+        const double f = fmax(fabs(lo[d] - L.c[d]), fabs(hi[d] - L.c[d]));
+        dmax2 += f * f;
+    }
+    if (sqrt(dmax2) <= L.r) return -1;
+    if (sqrt(dmin2) >= L.r) return +1;
+    return 0;
+}
+
+__host__ __device__ inline int nmodes3(int p) { return (p + 1) * (p + 2) * (p + 3) / 6; }
+__host__ __device__ inline int nmodes2(int p) { return (p + 1) * (p + 2) / 2; }
+
+__host__ __device__ inline void legendre_vals(int K, double x, double* L, double* dL) {
+    double P0 = 1.0, P1 = x, dP0 = 0.0, dP1 = 1.0;
+    double P[5], dP[5];
+    P[0] = 1.0;
+    dP[0] = 0.0;
+    if (K >= 1) {
+        P[1] = x;
+        dP[1] = 1.0;
+    }
+    for (int m = 1; m < K; ++m) {
+        const double P2 = ((2 * m + 1) * x * P1 - m * P0) / (m + 1);
+        const double dP2 = dP0 + (2 * m + 1) * P1;
+        P[m + 1] = P2;
+        dP[m + 1] = dP2;
+        P0 = P1;
+        P1 = P2;
+        dP0 = dP1;
+        dP1 = dP2;
+    }
+    for (int a = 0; a <= K; ++a) {
+        const double s = sqrt((2.0 * a + 1.0) / 2.0);
+        L[a] = s * P[a];
+        if (dL) dL[a] = s * dP[a];
+    }
+}
+
+// reference basis (3D, reference order) values at xi: out[n], n < nmodes3(p)
+__host__ __device__ inline void basis3(int p, const double* xi, double* out) {
+    double Lx[5], Ly[5], Lz[5];
+    legendre_vals(p, xi[0], Lx, nullptr);
+    legendre_vals(p, xi[1], Ly, nullptr);
+    legendre_vals(p, xi[2], Lz, nullptr);
+    int n = 0;
+    for (int deg = 0; deg <= p; ++deg)
+        for (int a = 0; a <= deg; ++a)
+            for (int b = 0; b <= deg - a; ++b) out[n++] = Lx[a] * Ly[b] * Lz[deg - a - b];
+}
+
+__host__ __device__ inline void basis2(int p, const double* t, double* out) {
+    double L1[5], L2[5];
+    legendre_vals(p, t[0], L1, nullptr);
+    legendre_vals(p, t[1], L2, nullptr);
+    int n = 0;
+    for (int deg = 0; deg <= p; ++deg)
+        for (int a = 0; a <= deg; ++a) out[n++] = L1[a] * L2[deg - a];
+}
+
+// Gauss-Legendre nodes/weights (host), ascending
+static void gauss(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    const long double PI = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i < n; ++i) {
+        long double z = std::cos(PI * (i + 0.75L) / (n + 0.5L)), dp = 1.0L;
+        for (int it = 0; it < 80; ++it) {
+            long double p0 = 1.0L, p1 = z;
+            for (int m = 1; m < n; ++m) {
+                long double p2 = ((2 * m + 1) * z * p1 - m * p0) / (m + 1);
+                p0 = p1;
+                p1 = p2;
+            }
+            long double pn = (n == 1) ? z : p1, pm = (n == 1) ? 1.0L : p0;
+            dp = n * (z * pn - pm) / (z * z - 1.0L);
+            long double dz = pn / dp;
+            z -= dz;
+            if (std::fabs((double)dz) < 1e-19) break;
+        }
+        long double p0 = 1.0L, p1 = z;
+        for (int m = 1; m < n; ++m) {
+            long double p2 = ((2 * m + 1) * z * p1 - m * p0) / (m + 1);
+            p0 = p1;
+            p1 = p2;
+        }
+        long double pn = (n == 1) ? z : p1, pm = (n == 1) ? 1.0L : p0;
+        dp = n * (z * pn - pm) / (z * z - 1.0L);
+        x[n - 1 - i] = (double)z;
+        w[n - 1 - i] = (double)(2.0L / ((1.0L - z * z) * dp * dp));
+    }
+    if (n % 2 == 1) x[n / 2] = 0.0;
+}
+
+// ------------------------------------------------------------------ device: moments
+// One rule item: a cut cell (dim 3) or a cut face (dim 2: in-plane dims t1 < t2, fixed
+// coordinate along `dir` at `xfix`) restricted to species `sp` (-1 inside, +1 outside).
+struct CutItem {
+    long long cell;     // cell (volume) / lower or own cell (face)
+    int dim;            // 3 volume, 2 face
+    int dir;            // face normal direction
+    int side;           // face: 0 lower, 1 upper face of `cell`
+    int sp;             // -1 species A (phi < 0), +1 species B
+    int p;              // moment degree requested
+    int nnodes;
+    long long node_off; // offset into the node / weight arrays
+    double center[3];   // cell centre (volume) or face centre (face)
+    double h[3];
+};
+
+struct Sub {
+    int S1, S2;   // coarse and fine subdivision per direction
+    double gx[3], gw[3];   // 3-point Gauss rule on [-1,1]
+};
+
+// moments of one item accumulated by one CTA; out[m], m < nmodes(dim, p)
+__global__ void k_moments(const CutItem* __restrict__ items, int nitems, LevelSetDev L, Sub sub, double* __restrict__ mom) {
+    const int r = blockIdx.x;
+    if (r >= nitems) return;
+    const CutItem it = items[r];
+    const int M = (it.dim == 3) ? nmodes3(it.p) : nmodes2(it.p);
+    double acc[XDG_MAXM];
+    for (int m = 0; m < XDG_MAXM; ++m) acc[m] = 0.0;
+    const int dims = it.dim;
+    int t[3];   // reference directions integrated
+    if (dims == 3) {
+        t[0] = 0;
+        t[1] = 1;
+        t[2] = 2;
+    } else {
+        t[0] = (it.dir == 0) ? 1 : 0;
+        t[1] = (it.dir == 2) ? 1 : 2;
+    }
+    const int S1 = sub.S1, S2 = sub.S2;
+    const long long ncoarse = (dims == 3) ? (long long)S1 * S1 * S1 : (long long)S1 * S1;
+    // every thread takes coarse boxes; cut coarse boxes are refined S2-fold
+    for (long long cb = threadIdx.x; cb < ncoarse; cb += blockDim.x) {
+        int ci[3] = {(int)(cb % S1), (int)((cb / S1) % S1), (int)(cb / ((long long)S1 * S1))};
+        // reference coordinates of the coarse box
+        double rlo[3], rhi[3];
+        for (int k = 0; k < dims; ++k) {
+            rlo[k] = -1.0 + 2.0 * ci[k] / S1;
+            rhi[k] = rlo[k] + 2.0 / S1;
+        }
+        auto to_phys = [&](const double* rr, double* x) {
+            for (int d = 0; d < 3; ++d) x[d] = it.center[d];
+            for (int k = 0; k < dims; ++k) x[t[k]] = it.center[t[k]] + 0.5 * it.h[t[k]] * rr[k];
+        };
+        auto classify = [&](const double* a, const double* b) {
+            double plo[3], phi_[3];
+            to_phys(a, plo);
+            to_phys(b, phi_);
+            int mask = 0;
+            for (int k = 0; k < dims; ++k) mask |= 1 << t[k];
+            return ls_box(L, plo, phi_, mask);
+        };
+        const int cls = classify(rlo, rhi);
+        if (cls == -it.sp) continue;   // fully in the other species
+        const int nsub = (cls == 0) ? S2 : 1;
+        const int nfine = (dims == 3) ? nsub * nsub * nsub : nsub * nsub;
+        for (int fb = 0; fb < nfine; ++fb) {
+            int fi[3] = {fb % nsub, (fb / nsub) % nsub, fb / (nsub * nsub)};
+            double flo[3], fhi[3];
+            for (int k = 0; k < dims; ++k) {
+                const double hh = (rhi[k] - rlo[k]) / nsub;
+                flo[k] = rlo[k] + fi[k] * hh;
+                fhi[k] = flo[k] + hh;
+            }
+            const int fcls = (nsub > 1) ? classify(flo, fhi) : cls;
+            if (fcls == -it.sp) continue;
+            const int nq = (dims == 3) ? 27 : 9;
+            for (int q = 0; q < nq; ++q) {
+                int qi[3] = {q % 3, (q / 3) % 3, q / 9};
+                double rr[3], wq = 1.0;
+                for (int k = 0; k < dims; ++k) {
+                    const double hh = fhi[k] - flo[k];
+                    rr[k] = flo[k] + 0.5 * hh * (sub.gx[qi[k]] + 1.0);
+                    wq *= 0.5 * hh * sub.gw[qi[k]];
+                }
+                if (fcls == 0) {   // cut leaf: indicator of the species at the node
+                    double x[3];
+                    to_phys(rr, x);
+                    const double ph = ls_phi(L, x);
+                    if ((it.sp < 0) ? !(ph < 0.0) : (ph < 0.0)) continue;
+                }
+                double v[XDG_MAXM];
+                if (dims == 3) basis3(it.p, rr, v);
+                else basis2(it.p, rr, v);
+                for (int m = 0; m < M; ++m) acc[m] += wq * v[m];
+            }
+        }
+    }
+    // block reduction
+    __shared__ double red[XDG_MAXM][33];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int m = 0; m < M; ++m) {
+        double v = acc[m];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[m][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < M) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+        mom[(long long)r * XDG_MAXM + threadIdx.x] = s;
+    }
+}
+
+// ------------------------------------------------------------------ device: weight solve
+// Per rule: A[m][j] = phi_m(node_j), G = A A^T, Cholesky of the leading block for the
+// largest degree whose Cholesky succeeds (relative pivot > 1e-13), y = G^-1 b, w = A^T y
+// (the minimum-norm solution of A w = b, which DGELSY returns for full row rank).
+__global__ void k_weight_solve(const CutItem* __restrict__ items, int nitems, const double* __restrict__ nodes,
+                               const double* __restrict__ mom, double* __restrict__ weights, int* __restrict__ deg_out,
+                               double* __restrict__ resid) {
+    const int r = blockIdx.x;
+    if (r >= nitems) return;
+    const CutItem it = items[r];
+    const int n = it.nnodes;
+    const int dims = it.dim;
+    __shared__ double A[XDG_MAXM][XDG_MAXN];
+    __shared__ double G[XDG_MAXM][XDG_MAXM + 1];
+    __shared__ double y[XDG_MAXM];
+    __shared__ int meff, peff;
+    const int Mmax = (dims == 3) ? nmodes3(it.p) : nmodes2(it.p);
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double v[XDG_MAXM];
+        const double* xi = nodes + (it.node_off + j) * 3;
+        if (dims == 3) basis3(it.p, xi, v);
+        else basis2(it.p, xi, v);
+        for (int m = 0; m < Mmax; ++m) A[m][j] = v[m];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < Mmax * Mmax; t += blockDim.x) {
+        const int a = t / Mmax, b = t % Mmax;
+        double s = 0.0;
+        for (int j = 0; j < n; ++j) s += A[a][j] * A[b][j];
+        G[a][b] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // in-place Cholesky, degree by degree
+        int m_ok = 0, p_ok = -1;
+        bool fail = false;
+        double gmax = 0.0;
+        for (int a = 0; a < Mmax; ++a) gmax = fmax(gmax, G[a][a]);
+        for (int p = 0; p <= it.p && !fail; ++p) {
+            const int m1 = (dims == 3) ? nmodes3(p) : nmodes2(p);
+            if (m1 > n) break;
+            for (int i = m_ok; i < m1 && !fail; ++i) {
+                for (int k = 0; k < i; ++k) {
+                    double s = G[i][k];
+                    for (int l = 0; l < k; ++l) s -= G[i][l] * G[k][l];
+                    G[i][k] = s / G[k][k];
+                }
+                double s = G[i][i];
+                for (int l = 0; l < i; ++l) s -= G[i][l] * G[i][l];
+                if (!(s > 1e-13 * gmax)) fail = true;
+                else G[i][i] = sqrt(s);
+            }
+            if (!fail) {
+                m_ok = m1;
+                p_ok = p;
+            }
+        }
+        meff = m_ok;
+        peff = p_ok;
+        // solve L L^T y = b on the leading m_ok block
+        const double* b = mom + (long long)r * XDG_MAXM;
+        for (int i = 0; i < m_ok; ++i) {
+            double s = b[i];
+            for (int k = 0; k < i; ++k) s -= G[i][k] * y[k];
+            y[i] = s / G[i][i];
+        }
+        for (int i = m_ok - 1; i >= 0; --i) {
+            double s = y[i];
+            for (int k = i + 1; k < m_ok; ++k) s -= G[k][i] * y[k];
+            y[i] = s / G[i][i];
+        }
+    }
+    __syncthreads();
+    const int M = meff;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double s = 0.0;
+        for (int m = 0; m < M; ++m) s += A[m][j] * y[m];
+        weights[it.node_off + j] = s;
+    }
+    __syncthreads();
+    // residual of the fitted moments, |A w - b|_inf / max(|b_0|, tiny)
+    if (threadIdx.x == 0) {
+        const double* b = mom + (long long)r * XDG_MAXM;
+        double e = 0.0;
+        for (int m = 0; m < M; ++m) {
+            double s = 0.0;
+            for (int j = 0; j < n; ++j) s += A[m][j] * weights[it.node_off + j];
+            e = fmax(e, fabs(s - b[m]));
+        }
+        deg_out[r] = peff;
+        resid[r] = e / fmax(fabs(b[0]), 1e-300);
+    }
+}
+
+// ------------------------------------------------------------------ device: cut-rule evaluation
+// Residual contributions of the cut items of one species, added with atomics:
+// volume items: int_{K cap s} (fV v + fG . grad v) with the item's rule;
+// face items: the SIP edge form on the cut face part (both cells, or boundary).
+template <int K>
+__global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const double* __restrict__ nodes,
+                           const double* __restrict__ weights, EvalArgs a) {
+    using Phys = PhysScalar<3, true>;
+    constexpr int NP = np_of(3, K);
+    const int r = blockIdx.x;
+    if (r >= nitems) return;
+    const CutItem it = items[r];
+    const GridConst& g = a.g;
+    __shared__ double cA[NP], cB[NP];
+    __shared__ double RA[NP], RB[NP];
+    int ijk[3];
+    cell_ijk(g, it.cell, ijk);
+    long long other = -1;
+    if (it.dim == 2) other = neighbour(g, ijk, it.dir, it.side);
+    for (int n = threadIdx.x; n < NP; n += blockDim.x) {
+        cA[n] = a.U[it.cell * NP + n];
+        cB[n] = (other >= 0) ? a.U[other * NP + n] : 0.0;
+        RA[n] = 0.0;
+        RB[n] = 0.0;
+    }
+    __syncthreads();
+    double rA[NP], rB[NP];
+    for (int n = 0; n < NP; ++n) rA[n] = rB[n] = 0.0;
+    const double sc = g.scaling;
+    for (int j = threadIdx.x; j < it.nnodes; j += blockDim.x) {
+        const double* t = nodes + (it.node_off + j) * 3;
+        const double wq = weights[it.node_off + j];
+        // reference coordinates of the node in the own cell (and the neighbour)
+        double xiA[3], xiB[3];
+        if (it.dim == 3) {
+            xiA[0] = t[0];
+            xiA[1] = t[1];
+            xiA[2] = t[2];
+        } else {
+            const int t1 = (it.dir == 0) ? 1 : 0, t2 = (it.dir == 2) ? 1 : 2;
+            xiA[it.dir] = it.side ? 1.0 : -1.0;
+            xiA[t1] = t[0];
+            xiA[t2] = t[1];
+            xiB[it.dir] = -xiA[it.dir];
+            xiB[t1] = t[0];
+            xiB[t2] = t[1];
+        }
+        double LA[3][K + 1], dLA[3][K + 1], LB[3][K + 1], dLB[3][K + 1];
+        for (int d = 0; d < 3; ++d) {
+            legendre_vals(K, xiA[d], LA[d], dLA[d]);
+            if (it.dim == 2) legendre_vals(K, xiB[d], LB[d], dLB[d]);
+        }
+        double phA[NP], gA_[NP][3], phB[NP], gB_[NP][3];
+        {
+            int nn = 0;
+            for (int deg = 0; deg <= K; ++deg)
+                for (int aa = 0; aa <= deg; ++aa)
+                    for (int bb = 0; bb <= deg - aa; ++bb) {
+                        const int cc = deg - aa - bb;
+                        phA[nn] = LA[0][aa] * LA[1][bb] * LA[2][cc];
+                        gA_[nn][0] = dLA[0][aa] * LA[1][bb] * LA[2][cc];
+                        gA_[nn][1] = LA[0][aa] * dLA[1][bb] * LA[2][cc];
+                        gA_[nn][2] = LA[0][aa] * LA[1][bb] * dLA[2][cc];
+                        if (it.dim == 2) {
+                            phB[nn] = LB[0][aa] * LB[1][bb] * LB[2][cc];
+                            gB_[nn][0] = dLB[0][aa] * LB[1][bb] * LB[2][cc];
+                            gB_[nn][1] = LB[0][aa] * dLB[1][bb] * LB[2][cc];
+                            gB_[nn][2] = LB[0][aa] * LB[1][bb] * dLB[2][cc];
+                        }
+                        ++nn;
+                    }
+        }
+        double uA = 0.0, GA[1][3] = {{0.0, 0.0, 0.0}};
+        for (int n = 0; n < NP; ++n) {
+            uA += cA[n] * phA[n];
+            for (int d = 0; d < 3; ++d) GA[0][d] += cA[n] * gA_[n][d];
+        }
+        uA *= sc;
+        for (int d = 0; d < 3; ++d) GA[0][d] *= sc * g.twoh[d];
+        double x[3];
+        for (int d = 0; d < 3; ++d) x[d] = g.lo[d] + (ijk[d] + 0.5 + 0.5 * xiA[d]) * g.h[d];
+        if (it.dim == 3) {
+            double U1[1] = {uA}, fV[1] = {0.0}, fG[1][3] = {{0.0, 0.0, 0.0}};
+            Phys::volume(a.ph, U1, GA, x, fV, fG);
+            const double fac = wq * g.detJ * sc;
+            for (int n = 0; n < NP; ++n) {
+                double acc = fV[0] * phA[n];
+                for (int d = 0; d < 3; ++d) acc += fG[0][d] * gA_[n][d] * g.twoh[d];
+                rA[n] += fac * acc;
+            }
+        } else {
+            const double fac = wq * g.faceSG[it.dir] * sc;
+            double nrm[3] = {0.0, 0.0, 0.0};
+            if (other >= 0) {
+                double uB = 0.0, GB[1][3] = {{0.0, 0.0, 0.0}};
+                for (int n = 0; n < NP; ++n) {
+                    uB += cB[n] * phB[n];
+                    for (int d = 0; d < 3; ++d) GB[0][d] += cB[n] * gB_[n][d];
+                }
+                uB *= sc;
+                for (int d = 0; d < 3; ++d) GB[0][d] *= sc * g.twoh[d];
+                // reference roles: IN = lower cell, normal +e_dir
+                const bool selfLower = it.side == 1;
+                nrm[it.dir] = 1.0;
+                int ijk2[3] = {ijk[0], ijk[1], ijk[2]};
+                ijk2[it.dir] = (int)((other / g.stride[it.dir]) % g.n[it.dir]);
+                const double pnlty = a.ph.pen * fmax(cell_cj(g, ijk), cell_cj(g, ijk2));
+                double U_in[1], U_out[1], G_in[1][3], G_out[1][3];
+                U_in[0] = selfLower ? uA : uB;
+                U_out[0] = selfLower ? uB : uA;
+                for (int d = 0; d < 3; ++d) {
+                    G_in[0][d] = selfLower ? GA[0][d] : GB[0][d];
+                    G_out[0][d] = selfLower ? GB[0][d] : GA[0][d];
+                }
+                double gi[1] = {0.0}, go[1] = {0.0}, Gi[1][3] = {{0, 0, 0}}, Go[1][3] = {{0, 0, 0}};
+                Phys::inner(a.ph, pnlty, U_in, G_in, U_out, G_out, nrm, x, gi, Gi, go, Go);
+                // own cell A gets IN terms if it is the lower cell
+                const double gsA = selfLower ? gi[0] : go[0], gsB = selfLower ? go[0] : gi[0];
+                const double* GsA = selfLower ? Gi[0] : Go[0];
+                const double* GsB = selfLower ? Go[0] : Gi[0];
+                for (int n = 0; n < NP; ++n) {
+                    double accA = gsA * phA[n], accB = gsB * phB[n];
+                    for (int d = 0; d < 3; ++d) {
+                        accA += GsA[d] * gA_[n][d] * g.twoh[d];
+                        accB += GsB[d] * gB_[n][d] * g.twoh[d];
+                    }
+                    rA[n] += fac * accA;
+                    rB[n] += fac * accB;
+                }
+            } else {
+                nrm[it.dir] = it.side ? 1.0 : -1.0;
+                const double pnlty = 2.0 * a.ph.pen * cell_cj(g, ijk);
+                double U1[1] = {uA}, gi[1] = {0.0}, Gi[1][3] = {{0, 0, 0}};
+                Phys::boundary(a.ph, pnlty, U1, GA, nrm, x, gi, Gi);
+                for (int n = 0; n < NP; ++n) {
+                    double acc = gi[0] * phA[n];
+                    for (int d = 0; d < 3; ++d) acc += Gi[0][d] * gA_[n][d] * g.twoh[d];
+                    rA[n] += fac * acc;
+                }
+            }
+        }
+    }
+    for (int n = 0; n < NP; ++n) {
+        atomicAdd(&RA[n], rA[n]);
+        if (it.dim == 2 && other >= 0) atomicAdd(&RB[n], rB[n]);
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < NP; n += blockDim.x) {
+        atomicAdd(&a.out[it.cell * NP + n], a.alpha * RA[n]);
+        if (it.dim == 2 && other >= 0) atomicAdd(&a.out[other * NP + n], a.alpha * RB[n]);
+    }
+}
+
+}  // namespace bosss
+
+using namespace bosss;
+
+struct bosss_xdg {
+    int device = 0;
+    bosss_handle* h[2] = {nullptr, nullptr};   // species A (phi < 0), B (phi > 0)
+    LevelSetDev ls{};
+    int K = 0;
+    // per species: masks and cut items
+    unsigned char* d_vol[2] = {nullptr, nullptr};
+    unsigned char* d_face[2] = {nullptr, nullptr};
+    std::vector<unsigned char> vol[2], face[2];
+    std::vector<CutItem> items[2];
+    CutItem* d_items[2] = {nullptr, nullptr};
+    double* d_nodes[2] = {nullptr, nullptr};
+    double* d_weights[2] = {nullptr, nullptr};
+    std::vector<double> nodes[2], weights[2];
+    std::vector<int> fitted_deg[2];
+    std::vector<double> fit_resid[2];
+    std::vector<double> moments[2];   // XDG_MAXM per item
+    long long n_cells[2] = {0, 0};
+};
+
+namespace bosss {
+
+static int build_species(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
+    const GridConst& g = X->h[s]->base.g;
+    const int sp = s == 0 ? -1 : +1;
+    const long long J = g.J;
+    X->vol[s].assign(J, 0);
+    X->face[s].assign(J * 6, 0);
+    std::vector<double> gx5, gw5, gx9, gw9;
+    gauss(xo.cut_nodes_1d, gx5, gw5);
+    gauss(xo.fallback_nodes_1d, gx9, gw9);
+    auto& items = X->items[s];
+    auto& nodes = X->nodes[s];
+    items.clear();
+    nodes.clear();
+    const int pmax = xo.moment_degree;
+    auto add_item = [&](long long cell, int dim, int dir, int side, const double* center, const double* hh) {
+        CutItem it{};
+        it.cell = cell;
+        it.dim = dim;
+        it.dir = dir;
+        it.side = side;
+        it.sp = sp;
+        it.p = pmax;
+        for (int d = 0; d < 3; ++d) {
+            it.center[d] = center[d];
+            it.h[d] = hh[d];
+        }
+        // candidate nodes: tensor Gauss nodes of the species part, finer set for small parts
+        auto collect = [&](const std::vector<double>& gx) {
+            std::vector<std::array<double, 3>> v;
+            const int nq = (int)gx.size();
+            const int tot = (dim == 3) ? nq * nq * nq : nq * nq;
+            const int t1 = (dir == 0) ? 1 : 0, t2 = (dir == 2) ? 1 : 2;
+            for (int q = 0; q < tot; ++q) {
+                double rr[3] = {gx[q % nq], gx[(q / nq) % nq], (dim == 3) ? gx[q / (nq * nq)] : 0.0};
+                double x[3];
+                if (dim == 3) {
+                    for (int d = 0; d < 3; ++d) x[d] = center[d] + 0.5 * hh[d] * rr[d];
+                } else {
+                    for (int d = 0; d < 3; ++d) x[d] = center[d];
+                    x[t1] += 0.5 * hh[t1] * rr[0];
+                    x[t2] += 0.5 * hh[t2] * rr[1];
+                }
+                const double ph = ls_phi(X->ls, x);
+                if ((sp < 0) ? (ph < 0.0) : !(ph < 0.0)) v.push_back({rr[0], rr[1], rr[2]});
+            }
+            return v;
+        };
+        auto cand = collect(gx5);
+        if ((int)cand.size() < 8) cand = collect(gx9);
+        if ((int)cand.size() > XDG_MAXN) cand.resize(XDG_MAXN);
+        if (cand.empty()) return;   // no node of the species part: negligible fragment
+        it.nnodes = (int)cand.size();
+        it.node_off = (long long)nodes.size() / 3;
+        for (auto& c : cand)
+            for (int d = 0; d < 3; ++d) nodes.push_back(c[d]);
+        items.push_back(it);
+    };
+    for (long long j = 0; j < J; ++j) {
+        int ijk[3];
+        for (int d = 0; d < 3; ++d) ijk[d] = (int)((j / g.stride[d]) % g.n[d]);
+        double lo[3], hi[3], c[3];
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = g.lo[d] + ijk[d] * g.h[d];
+            hi[d] = lo[d] + g.h[d];
+            c[d] = 0.5 * (lo[d] + hi[d]);
+        }
+        const int cls = ls_box(X->ls, lo, hi, 7);
+        if (cls == sp) X->vol[s][j] = 1;
+        else if (cls == 0) {
+            X->vol[s][j] = 2;
+            add_item(j, 3, 0, 0, c, g.h);
+        }
+        if (X->vol[s][j] == 0) continue;
+        // faces of the cell
+        for (int d = 0; d < 3; ++d)
+            for (int side = 0; side < 2; ++side) {
+                double flo[3], fhi[3], fc[3];
+                for (int dd = 0; dd < 3; ++dd) {
+                    flo[dd] = lo[dd];
+                    fhi[dd] = hi[dd];
+                    fc[dd] = c[dd];
+                }
+                flo[d] = fhi[d] = fc[d] = side ? hi[d] : lo[d];
+                const int fcls = ls_box(X->ls, flo, fhi, 7 & ~(1 << d));
+                unsigned char fl = 0;
+                if (fcls == sp) fl = 1;
+                else if (fcls == 0) fl = 2;
+                X->face[s][j * 6 + 2 * d + side] = fl;
+                if (fl == 2) {
+                    // one item per cut face: interior faces from the lower cell, boundary faces from their cell
+                    const bool boundary = !g.periodic[d] && ((side == 0 && ijk[d] == 0) || (side == 1 && ijk[d] == g.n[d] - 1));
+                    if (boundary || side == 1) add_item(j, 2, d, side, fc, g.h);
+                }
+            }
+    }
+    long long cnt = 0;
+    for (long long j = 0; j < J; ++j) cnt += X->vol[s][j] != 0;
+    X->n_cells[s] = cnt;
+    return BOSSS_OK;
+}
+
+static int upload_and_fit(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
+    auto& items = X->items[s];
+    const int n = (int)items.size();
+    const size_t nn = X->nodes[s].size() / 3;
+    CUDA_TRY(cudaMalloc(&X->d_vol[s], X->vol[s].size()));
+    CUDA_TRY(cudaMalloc(&X->d_face[s], X->face[s].size()));
+    CUDA_TRY(cudaMemcpy(X->d_vol[s], X->vol[s].data(), X->vol[s].size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(X->d_face[s], X->face[s].data(), X->face[s].size(), cudaMemcpyHostToDevice));
+    X->weights[s].assign(nn, 0.0);
+    X->fitted_deg[s].assign(n, -1);
+    X->fit_resid[s].assign(n, 0.0);
+    if (n == 0) return BOSSS_OK;
+    CUDA_TRY(cudaMalloc(&X->d_items[s], sizeof(CutItem) * n));
+    CUDA_TRY(cudaMalloc(&X->d_nodes[s], sizeof(double) * 3 * nn));
+    CUDA_TRY(cudaMalloc(&X->d_weights[s], sizeof(double) * nn));
+    CUDA_TRY(cudaMemcpy(X->d_items[s], items.data(), sizeof(CutItem) * n, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(X->d_nodes[s], X->nodes[s].data(), sizeof(double) * 3 * nn, cudaMemcpyHostToDevice));
+    double* d_mom = nullptr;
+    int* d_deg = nullptr;
+    double* d_res = nullptr;
+    CUDA_TRY(cudaMalloc(&d_mom, sizeof(double) * XDG_MAXM * n));
+    CUDA_TRY(cudaMalloc(&d_deg, sizeof(int) * n));
+    CUDA_TRY(cudaMalloc(&d_res, sizeof(double) * n));
+    Sub sub{};
+    sub.S1 = xo.subdivision;
+    sub.S2 = xo.subdivision;
+    std::vector<double> gx, gw;
+    gauss(3, gx, gw);
+    for (int q = 0; q < 3; ++q) {
+        sub.gx[q] = gx[q];
+        sub.gw[q] = gw[q];
+    }
+    k_moments<<<n, 256>>>(X->d_items[s], n, X->ls, sub, d_mom);
+    CUDA_TRY(cudaGetLastError());
+    k_weight_solve<<<n, 128>>>(X->d_items[s], n, X->d_nodes[s], d_mom, X->d_weights[s], d_deg, d_res);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaDeviceSynchronize());
+    CUDA_TRY(cudaMemcpy(X->weights[s].data(), X->d_weights[s], sizeof(double) * nn, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(X->fitted_deg[s].data(), d_deg, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(X->fit_resid[s].data(), d_res, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    X->moments[s].assign((size_t)XDG_MAXM * n, 0.0);
+    CUDA_TRY(cudaMemcpy(X->moments[s].data(), d_mom, sizeof(double) * XDG_MAXM * n, cudaMemcpyDeviceToHost));
+    cudaFree(d_mom);
+    cudaFree(d_deg);
+    cudaFree(d_res);
+    return BOSSS_OK;
+}
+
+}  // namespace bosss
+
+extern "C" {
+
+int bosss_b200_xdg_create(const bosss_op_desc* opA, const bosss_op_desc* opB, const bosss_grid_desc* grid,
+                          const bosss_levelset_desc* ls, const bosss_xdg_opts* xopt, const bosss_options* opt,
+                          bosss_xdg** out) {
+    if (!opA || !opB || !grid || !ls || !out) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    *out = nullptr;
+    if (grid->dim != 3) return fail(BOSSS_ERR_BAD_ARG, "XDG path: 3D grids");
+    if (ls->type != BOSSS_LEVELSET_SPHERE || !(ls->params[3] > 0.0))
+        return fail(BOSSS_ERR_BAD_ARG, "XDG path: sphere level set phi = |x - c| - r, r > 0");
+    bosss_xdg_opts xo{};
+    xo.cut_nodes_1d = 5;
+    xo.fallback_nodes_1d = 9;
+    xo.moment_degree = -1;
+    xo.subdivision = 8;
+    if (xopt) {
+        if (xopt->cut_nodes_1d > 0) xo.cut_nodes_1d = xopt->cut_nodes_1d;
+        if (xopt->fallback_nodes_1d > 0) xo.fallback_nodes_1d = xopt->fallback_nodes_1d;
+        if (xopt->moment_degree >= 0) xo.moment_degree = xopt->moment_degree;
+        if (xopt->subdivision > 0) xo.subdivision = xopt->subdivision;
+    }
+    bosss_xdg* X = new bosss_xdg();
+    for (int s = 0; s < 2; ++s) {
+        int rc = bosss_b200_create(s == 0 ? opA : opB, grid, opt, &X->h[s]);
+        if (rc) {
+            bosss_b200_xdg_destroy(X);
+            return rc;
+        }
+        if (X->h[s]->phys != PHYS_SIP || X->h[s]->D != 3 || X->h[s]->K < 1 || X->h[s]->K > 4) {
+            bosss_b200_xdg_destroy(X);
+            return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "XDG bulk: SIP (XLaplace_Bulk) operators, degree 1..4");
+        }
+    }
+    X->device = X->h[0]->device;
+    X->K = X->h[0]->K;
+    if (X->h[1]->K != X->K) {
+        bosss_b200_xdg_destroy(X);
+        return fail(BOSSS_ERR_BAD_ARG, "both species need the same DG degree");
+    }
+    if (xo.moment_degree < 0) xo.moment_degree = std::min(4, 2 * X->K);
+    if (xo.moment_degree > 4) xo.moment_degree = 4;
+    X->ls.type = ls->type;
+    for (int d = 0; d < 3; ++d) X->ls.c[d] = ls->params[d];
+    X->ls.r = ls->params[3];
+    cudaError_t e = cudaSetDevice(X->device);
+    if (e != cudaSuccess) {
+        bosss_b200_xdg_destroy(X);
+        return fail(BOSSS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    for (int s = 0; s < 2; ++s) {
+        int rc = build_species(X, s, xo);
+        if (!rc) rc = upload_and_fit(X, s, xo);
+        if (rc) {
+            bosss_b200_xdg_destroy(X);
+            return rc;
+        }
+    }
+    *out = X;
+    return BOSSS_OK;
+}
+
+int bosss_b200_xdg_destroy(bosss_xdg* X) {
+    if (!X) return BOSSS_OK;
+    cudaSetDevice(X->device);
+    for (int s = 0; s < 2; ++s) {
+        cudaFree(X->d_vol[s]);
+        cudaFree(X->d_face[s]);
+        cudaFree(X->d_items[s]);
+        cudaFree(X->d_nodes[s]);
+        cudaFree(X->d_weights[s]);
+        bosss_b200_destroy(X->h[s]);
+    }
+    delete X;
+    return BOSSS_OK;
+}
+
+int bosss_b200_xdg_info(const bosss_xdg* X, int32_t species, int64_t* n_cells, int64_t* n_cut_cells,
+                        int64_t* n_cut_faces, int32_t* min_nodes, int32_t* max_nodes, int32_t* min_degree,
+                        double* max_fit_residual) {
+    if (!X || species < 0 || species > 1) return fail(BOSSS_ERR_BAD_ARG, "bad argument");
+    const int s = species;
+    long long nc = 0, nf = 0;
+    int mn = 1 << 30, mx = 0, mdeg = 99;
+    double r = 0.0;
+    for (size_t i = 0; i < X->items[s].size(); ++i) {
+        const CutItem& it = X->items[s][i];
+        (it.dim == 3 ? nc : nf)++;
+        mn = std::min(mn, it.nnodes);
+        mx = std::max(mx, it.nnodes);
+        mdeg = std::min(mdeg, X->fitted_deg[s][i]);
+        r = std::max(r, X->fit_resid[s][i]);
+    }
+    if (n_cells) *n_cells = X->n_cells[s];
+    if (n_cut_cells) *n_cut_cells = nc;
+    if (n_cut_faces) *n_cut_faces = nf;
+    if (min_nodes) *min_nodes = X->items[s].empty() ? 0 : mn;
+    if (max_nodes) *max_nodes = mx;
+    if (min_degree) *min_degree = X->items[s].empty() ? -1 : mdeg;
+    if (max_fit_residual) *max_fit_residual = r;
+    return BOSSS_OK;
+}
+
+int bosss_b200_xdg_get_rules(const bosss_xdg* X, int32_t species, int64_t* n_items, int64_t* item_info,
+                             int64_t* node_offsets, double* nodes, double* weights, unsigned char* vol_flags,
+                             unsigned char* face_flags) {
+    if (!X || species < 0 || species > 1) return fail(BOSSS_ERR_BAD_ARG, "bad argument");
+    const int s = species;
+    const auto& items = X->items[s];
+    if (n_items) n_items[0] = (int64_t)items.size(), n_items[1] = (int64_t)(X->nodes[s].size() / 3);
+    for (size_t i = 0; i < items.size(); ++i) {
+        if (item_info) {
+            item_info[i * 5 + 0] = items[i].cell;
+            item_info[i * 5 + 1] = items[i].dim;
+            item_info[i * 5 + 2] = items[i].dir;
+            item_info[i * 5 + 3] = items[i].side;
+            item_info[i * 5 + 4] = X->fitted_deg[s][i];
+        }
+        if (node_offsets) node_offsets[i] = items[i].node_off;
+    }
+    if (node_offsets) node_offsets[items.size()] = (int64_t)(X->nodes[s].size() / 3);
+    if (nodes) std::memcpy(nodes, X->nodes[s].data(), sizeof(double) * X->nodes[s].size());
+    if (weights) std::memcpy(weights, X->weights[s].data(), sizeof(double) * X->weights[s].size());
+    if (vol_flags) std::memcpy(vol_flags, X->vol[s].data(), X->vol[s].size());
+    if (face_flags) std::memcpy(face_flags, X->face[s].data(), X->face[s].size());
+    return BOSSS_OK;
+}
+
+int bosss_b200_xdg_get_moments(const bosss_xdg* X, int32_t species, double* moments) {
+    if (!X || species < 0 || species > 1 || !moments) return fail(BOSSS_ERR_BAD_ARG, "bad argument");
+    std::memcpy(moments, X->moments[species].data(), sizeof(double) * X->moments[species].size());
+    return BOSSS_OK;
+}
+
+int bosss_b200_xdg_evaluate_device(bosss_xdg* X, int32_t species, double alpha, double beta, const double* U_dev,
+                                   double* out_dev, double time, void* stream) {
+    if (!X || species < 0 || species > 1 || !U_dev || !out_dev) return fail(BOSSS_ERR_BAD_ARG, "bad argument");
+    const int s = species;
+    bosss_handle* h = X->h[s];
+    CUDA_TRY(cudaSetDevice(X->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    // uncut cells and faces of the species: tensor kernel with masks
+    EvalArgs keep = h->base;
+    h->base.vol_flag = X->d_vol[s];
+    h->base.face_flag = X->d_face[s];
+    int rc = run_mode(h, MODE_RES, alpha, beta, U_dev, nullptr, out_dev, time, st);
+    h->base = keep;
+    if (rc) return rc;
+    // cut cells and faces: explicit rules, added atomically
+    const int n = (int)X->items[s].size();
+    if (n > 0) {
+        EvalArgs a = h->base;
+        a.U = U_dev;
+        a.out = out_dev;
+        a.alpha = alpha;
+        a.time = time;
+        switch (X->K) {
+            case 1: k_cut_eval<1><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a); break;
+            case 2: k_cut_eval<2><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a); break;
+            case 3: k_cut_eval<3><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a); break;
+            default: k_cut_eval<4><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a); break;
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+    return BOSSS_OK;
+}
+
+int bosss_b200_xdg_evaluate(bosss_xdg* X, int32_t species, double alpha, double beta, const double* U, double* out,
+                            double time) {
+    if (!X || species < 0 || species > 1 || !U || !out) return fail(BOSSS_ERR_BAD_ARG, "bad argument");
+    bosss_handle* h = X->h[species];
+    int rc = ensure_staging(h);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(X->device));
+    cudaStream_t s = h->stream;
+    CUDA_TRY(cudaMemcpyAsync(h->dU, U, sizeof(double) * h->ndom, cudaMemcpyHostToDevice, s));
+    if (beta != 0.0) CUDA_TRY(cudaMemcpyAsync(h->dOut, out, sizeof(double) * h->ncod, cudaMemcpyHostToDevice, s));
+    rc = bosss_b200_xdg_evaluate_device(X, species, alpha, beta, h->dU, h->dOut, time, s);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(out, h->dOut, sizeof(double) * h->ncod, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return BOSSS_OK;
+}
+
+}  // extern "C"

@@ -573,3 +573,81 @@ class BatchEvaluator:
         t, lpt = ctypes.c_int32(), ctypes.c_int32()
         C.check(C.lib().bosss_b200_batch_tiles(self.handle, K, Q, ctypes.byref(t), ctypes.byref(lpt)))
         return t.value, bool(lpt.value)
+
+
+class XdgEvaluator:
+    """Per-species bulk evaluation of an XDG operator (``XEvaluatorNonlin.Evaluate``, bulk
+    part): ``opA`` / ``opB`` are the committed bulk operators of species A (phi < 0) and B
+    (phi >= 0), e.g. ``XLaplace_Bulk`` = :class:`SIPLaplace` with nu = mu_s; the level set is a
+    sphere ``phi = |x - c| - r``. Vectors are full-grid species frames."""
+
+    def __init__(self, opA, opB, grid, degree, center, radius, device=0, cut_nodes_1d=5, fallback_nodes_1d=9,
+                 moment_degree=-1, subdivision=8):
+        self.handle = None
+        self.grid, self.degree = grid, degree
+        self.descA = opA.descriptor([degree], [degree], grid.dim)
+        self.descB = opB.descriptor([degree], [degree], grid.dim)
+        self.gdesc = grid.desc()
+        ls = C.LevelSetDesc()
+        ls.type = C.LEVELSET_SPHERE
+        for i, v in enumerate(list(center) + [radius]):
+            ls.params[i] = float(v)
+        xo = C.XdgOpts()
+        xo.cut_nodes_1d, xo.fallback_nodes_1d = cut_nodes_1d, fallback_nodes_1d
+        xo.moment_degree, xo.subdivision = moment_degree, subdivision
+        opt = C.Options()
+        opt.device = int(device)
+        h = ctypes.c_void_p()
+        C.check(C.lib().bosss_b200_xdg_create(ctypes.byref(self.descA), ctypes.byref(self.descB),
+                                              ctypes.byref(self.gdesc), ctypes.byref(ls), ctypes.byref(xo),
+                                              ctypes.byref(opt), ctypes.byref(h)))
+        self.handle = h
+        self.n = grid.NoOfCells * np_of(grid.dim, degree)
+
+    def Dispose(self):
+        if self.handle:
+            C.lib().bosss_b200_xdg_destroy(self.handle)
+            self.handle = None
+
+    __del__ = Dispose
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.Dispose()
+
+    def info(self, species):
+        v = [ctypes.c_int64() for _ in range(3)] + [ctypes.c_int32() for _ in range(3)] + [ctypes.c_double()]
+        C.check(C.lib().bosss_b200_xdg_info(self.handle, species, *[ctypes.byref(x) for x in v]))
+        keys = ["cells", "cut_cells", "cut_faces", "min_nodes", "max_nodes", "min_degree", "max_fit_residual"]
+        return dict(zip(keys, [x.value for x in v]))
+
+    def rules(self, species):
+        cnt = (ctypes.c_int64 * 2)()
+        C.check(C.lib().bosss_b200_xdg_get_rules(self.handle, species, cnt, None, None, None, None, None, None))
+        ni, nn = cnt[0], cnt[1]
+        J = self.grid.NoOfCells
+        info = np.zeros(ni * 5, dtype=np.int64)
+        offs = np.zeros(ni + 1, dtype=np.int64)
+        nodes = np.zeros(nn * 3)
+        w = np.zeros(nn)
+        vf = np.zeros(J, dtype=np.uint8)
+        ff = np.zeros(J * 6, dtype=np.uint8)
+        C.check(C.lib().bosss_b200_xdg_get_rules(self.handle, species, cnt, C.ptr(info), C.ptr(offs), C.ptr(nodes),
+                                                 C.ptr(w), C.ptr(vf), C.ptr(ff)))
+        mom = np.zeros(ni * 35)
+        C.check(C.lib().bosss_b200_xdg_get_moments(self.handle, species, C.ptr(mom)))
+        return {"info": info.reshape(ni, 5), "offsets": offs, "nodes": nodes.reshape(nn, 3), "weights": w,
+                "vol_flags": vf, "face_flags": ff, "moments": mom.reshape(ni, 35)}
+
+    def Evaluate(self, species, alpha, beta, output, U):
+        if hasattr(U, "is_cuda") and U.is_cuda:
+            import torch
+            s = torch.cuda.current_stream().cuda_stream
+            C.check(C.lib().bosss_b200_xdg_evaluate_device(self.handle, species, alpha, beta, C.ptr(U), C.ptr(output),
+                                                           0.0, ctypes.c_void_p(s if s else C.CUDA_STREAM_LEGACY)))
+            return output
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        C.check(C.lib().bosss_b200_xdg_evaluate(self.handle, species, alpha, beta, C.ptr(U), C.ptr(output), 0.0))
+        return output

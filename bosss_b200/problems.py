@@ -190,3 +190,25 @@ def batched_advection_diffusion(n_instances=256, seed=5000, sizes=(16, 24, 32, 4
     ks = r.choice(degrees, n_instances)
     return [advection_diffusion3d(n=int(n), k=int(k), seed=seed * 1000 + i, nu=nu)
             for i, (n, k) in enumerate(zip(ns, ks))]
+
+
+def xdg_poisson3d(n=128, k=2, seed=4000, muA=1.0, muB=10.0, radius=0.4, penalty_base=4.0):
+    """XDG two-phase Poisson with jump, bulk part: -div(mu grad u) = 1 on [-1,1]^3, n^3 hexes,
+    phi = |x - c| - radius with c ~ 0.05 U[-1,1]^3 (seeded), mu = muA inside, muB outside,
+    Dirichlet 0, uncut cells with the Gauss rule of order 5. Returns (opA, opB, grid, center,
+    UA, UB) with species frames UA, UB (coefficients iid U[-1,1])."""
+    r = rng(seed)
+    c = 0.05 * r.uniform(-1, 1, 3)
+    nodes = np.linspace(-1.0, 1.0, n + 1)
+    g = O.Cartesian3DGrid(nodes, nodes, nodes, False, False, False)
+    ops = []
+    for mu in (muA, muB):
+        op = O.DifferentialOperator(["u"], [], ["R"], O.QuadOrderFunc.FixedOrder(5))
+        op.EquationComponents["R"].Add(O.SIPLaplace(penalty_base, "u", nu0=mu, nu2=0.0, dirichlet=True))
+        op.EquationComponents["R"].Add(O.ConstantSource(1.0, "u"))
+        op.Commit()
+        ops.append(op)
+    Np = O.np_of(3, k)
+    UA = r.uniform(-1, 1, g.NoOfCells * Np)
+    UB = r.uniform(-1, 1, g.NoOfCells * Np)
+    return ops[0], ops[1], g, c, UA, UB

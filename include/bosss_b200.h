@@ -273,6 +273,59 @@ int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double*
                               const char* table_path);
 int bosss_b200_batch_tiles(const bosss_batch* b, int32_t K, int32_t Q, int32_t* tiles, int32_t* lpt);
 
+/* ---- XDG: per-species bulk evaluation with moment-fitted cut-cell rules ----
+ * XEvaluatorNonlin.Evaluate, bulk part (XSpatialOperatorMk2_XEvaluators.cs:372-511): for
+ * species A (phi < 0) and B (phi >= 0) the species' bulk operator (XLaplace_Bulk =
+ * SIPLaplace with nu = mu_s, XLaplace.cs:50-120, plus sources) is integrated over the
+ * cells and faces that contain the species; cut cells and cut faces use per-item rules
+ * fitted to the moments of the species part (LevelSetComboRuleFactory2.cs:300-528:
+ * candidate nodes = tensor Gauss nodes inside the species part, moments integrated on the
+ * device, minimum-norm least-squares weights as DGELSY returns them, IMatrixExtensions.cs:
+ * 2318-2340). Level-set (interface) terms are not part of this evaluator.
+ * Vectors are species frames: a full-grid DG vector per species (J * Np, the reference's
+ * cell-major layout); entries of cells without the species are ignored and returned 0. */
+enum bosss_levelset_type { BOSSS_LEVELSET_SPHERE = 1 };   /* phi = |x - c| - r, params = c[3], r */
+
+typedef struct bosss_levelset_desc {
+    int32_t type;
+    double params[8];
+} bosss_levelset_desc;
+
+typedef struct bosss_xdg_opts {
+    int32_t cut_nodes_1d;       /* candidate Gauss nodes per direction (default 5) */
+    int32_t fallback_nodes_1d;  /* candidates for species parts with < 8 nodes (default 9) */
+    int32_t moment_degree;      /* fitted polynomial degree (default min(2k, 4)); <0: default */
+    int32_t subdivision;        /* moment integration: S x S coarse boxes, cut ones S x S again (default 8) */
+    int32_t reserved[8];
+} bosss_xdg_opts;
+
+typedef struct bosss_xdg bosss_xdg;
+
+int bosss_b200_xdg_create(const bosss_op_desc* opA, const bosss_op_desc* opB, const bosss_grid_desc* grid,
+                          const bosss_levelset_desc* ls, const bosss_xdg_opts* xopt, const bosss_options* opt,
+                          bosss_xdg** out);
+int bosss_b200_xdg_destroy(bosss_xdg* X);
+/* cells with the species, cut cells / cut faces with rules, node-count range, lowest fitted
+ * degree and the largest relative moment residual of the fitted rules */
+int bosss_b200_xdg_info(const bosss_xdg* X, int32_t species, int64_t* n_cells, int64_t* n_cut_cells,
+                        int64_t* n_cut_faces, int32_t* min_nodes, int32_t* max_nodes, int32_t* min_degree,
+                        double* max_fit_residual);
+/* rules of a species: n_items[2] = {items, nodes}; item_info[5 per item] = (cell, dim (3 volume,
+ * 2 face), face direction, face side, fitted degree); node_offsets[items+1]; nodes[3 per node]
+ * (reference coordinates of the cell, or of the face in its two in-plane directions);
+ * weights[nodes]; vol_flags[J] and face_flags[J*6] (0 absent, 1 standard rule, 2 cut rule).
+ * Any output pointer may be NULL. */
+int bosss_b200_xdg_get_rules(const bosss_xdg* X, int32_t species, int64_t* n_items, int64_t* item_info,
+                             int64_t* node_offsets, double* nodes, double* weights, unsigned char* vol_flags,
+                             unsigned char* face_flags);
+/* the fitted moments, 35 per item (unused trailing entries 0): int over the species part of the
+ * reference basis functions of degree <= moment_degree (3D items) or of the face basis (faces) */
+int bosss_b200_xdg_get_moments(const bosss_xdg* X, int32_t species, double* moments);
+int bosss_b200_xdg_evaluate(bosss_xdg* X, int32_t species, double alpha, double beta, const double* U, double* out,
+                            double time);
+int bosss_b200_xdg_evaluate_device(bosss_xdg* X, int32_t species, double alpha, double beta, const double* U_dev,
+                                   double* out_dev, double time, void* stream);
+
 /* Batched evaluation that allocates no device memory (no counterpart in the reference).
  * For callers that cannot call cudaMalloc: hosts whose device memory belongs to another
  * allocator, or loops that must not synchronise the device with an allocation. Same

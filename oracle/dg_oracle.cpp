@@ -849,7 +849,167 @@ static void evaluate(const Problem& P, double alpha, double beta, const T* U, T*
 
 static thread_local std::string g_err;
 
+// ------------------------------------------------------------------ XDG bulk (given rules)
+// Volume integral of cell j with reference nodes xi[npts*D] and weights w[npts]
+// (NECQuadratureVolume semantics with a cut-cell rule), added to R[Nc].
+static void vol_integral(const Problem& P, int j, int npts, const double* xi, const double* w, const double* U,
+                         double* R) {
+    const int D = P.D, nd = P.op.n_domain, nc = P.op.n_codomain, Nd = P.dom_per_cell;
+    double c[3];
+    cell_center(P, j, c);
+    for (int q = 0; q < npts; ++q) {
+        const double* x0 = xi + (size_t)q * D;
+        double Uq[BOSSS_MAX_VARS], Gq[BOSSS_MAX_VARS][3];
+        for (int f = 0; f < nd; ++f) {
+            int k = P.op.domain_degree[f], Np = P.dom_np[f];
+            double v = 0, gr[3] = {0, 0, 0};
+            for (int n = 0; n < Np; ++n) {
+                double pv, pg[3];
+                poly_eval(P.basis[k][n], D, x0, pv, pg);
+                double cf = U[(long)j * Nd + P.dom_off[f] + n];
+                v += cf * pv;
+                for (int d = 0; d < D; ++d) gr[d] += cf * pg[d];
+            }
+            Uq[f] = v * P.scaling;
+            for (int d = 0; d < D; ++d) Gq[f][d] = gr[d] * P.scaling * 2.0 / P.h[d];
+        }
+        double x[3];
+        for (int d = 0; d < D; ++d) x[d] = c[d] + 0.5 * P.h[d] * x0[d];
+        for (int e = 0; e < nc; ++e) {
+            double fV = 0, fG[3] = {0, 0, 0};
+            for (int ci = 0; ci < P.op.n_components; ++ci)
+                if (P.op.components[ci].codomain == e) volume_terms<double>(P, P.op.components[ci], Uq, Gq, x, fV, fG);
+            int k = P.op.codomain_degree[e], Np = P.cod_np[e];
+            for (int m = 0; m < Np; ++m) {
+                double pv, pg[3];
+                poly_eval(P.basis[k][m], D, x0, pv, pg);
+                double acc = fV * pv;
+                for (int d = 0; d < D; ++d) acc += fG[d] * pg[d] * 2.0 / P.h[d];
+                R[P.cod_off[e] + m] += w[q] * P.detJ * P.scaling * acc;
+            }
+        }
+    }
+}
+
+// Face integral between jin (IN, lower cell, its face xi_d = +1) and jout (OUT, xi_d = -1),
+// or a boundary face of jin (jout < 0, outward normal sgn*e_d, face xi_d = sgn); face
+// nodes t[npts*(D-1)] in the in-plane directions (ascending), weights w.
+static void face_integral(const Problem& P, int jin, int jout, int d, double sgn, int npts, const double* t,
+                          const double* w, const double* U, double* Rin, double* Rout) {
+    const int D = P.D, nd = P.op.n_domain, nc = P.op.n_codomain, Nd = P.dom_per_cell;
+    int oth[2], no = 0;
+    for (int d2 = 0; d2 < D; ++d2)
+        if (d2 != d) oth[no++] = d2;
+    double cIn[3];
+    cell_center(P, jin, cIn);
+    double nrm[3] = {0, 0, 0};
+    nrm[d] = (jout >= 0) ? 1.0 : sgn;
+    for (int q = 0; q < npts; ++q) {
+        double xiIn[3], xiOut[3], x[3];
+        xiIn[d] = (jout >= 0) ? 1.0 : sgn;
+        xiOut[d] = -1.0;
+        for (int k = 0; k < D - 1; ++k) xiIn[oth[k]] = xiOut[oth[k]] = t[(size_t)q * (D - 1) + k];
+        for (int d2 = 0; d2 < D; ++d2) x[d2] = cIn[d2] + 0.5 * P.h[d2] * xiIn[d2];
+        double UA[BOSSS_MAX_VARS], GA[BOSSS_MAX_VARS][3], UB[BOSSS_MAX_VARS], GB[BOSSS_MAX_VARS][3];
+        for (int side = 0; side < 2; ++side) {
+            if (side == 1 && jout < 0) break;
+            const int jc = side ? jout : jin;
+            const double* xi = side ? xiOut : xiIn;
+            for (int f = 0; f < nd; ++f) {
+                int k = P.op.domain_degree[f], Np = P.dom_np[f];
+                double v = 0, gr[3] = {0, 0, 0};
+                for (int n = 0; n < Np; ++n) {
+                    double pv, pg[3];
+                    poly_eval(P.basis[k][n], D, xi, pv, pg);
+                    double cf = U[(long)jc * Nd + P.dom_off[f] + n];
+                    v += cf * pv;
+                    for (int dd = 0; dd < D; ++dd) gr[dd] += cf * pg[dd];
+                }
+                double* Uo = side ? UB : UA;
+                double(*Go)[3] = side ? GB : GA;
+                Uo[f] = v * P.scaling;
+                for (int dd = 0; dd < D; ++dd) Go[f][dd] = gr[dd] * P.scaling * 2.0 / P.h[dd];
+            }
+        }
+        const double wq = w[q] * P.faceSG[d];
+        for (int e = 0; e < nc; ++e) {
+            double gA = 0, gB = 0, GAv[3] = {0, 0, 0}, GBv[3] = {0, 0, 0};
+            for (int ci = 0; ci < P.op.n_components; ++ci) {
+                const auto& cp = P.op.components[ci];
+                if (cp.codomain != e) continue;
+                if (jout >= 0) inner_edge_terms<double>(P, cp, jin, jout, UA, GA, UB, GB, nrm, gA, GAv, gB, GBv);
+                else boundary_edge_terms<double>(P, cp, jin, UA, GA, nrm, x, gA, GAv);
+            }
+            int k = P.op.codomain_degree[e], Np = P.cod_np[e];
+            for (int m = 0; m < Np; ++m) {
+                double pv, pg[3];
+                poly_eval(P.basis[k][m], D, xiIn, pv, pg);
+                double acc = gA * pv;
+                for (int dd = 0; dd < D; ++dd) acc += GAv[dd] * pg[dd] * 2.0 / P.h[dd];
+                Rin[P.cod_off[e] + m] += wq * P.scaling * acc;
+                if (jout >= 0) {
+                    poly_eval(P.basis[k][m], D, xiOut, pv, pg);
+                    double acc2 = gB * pv;
+                    for (int dd = 0; dd < D; ++dd) acc2 += GBv[dd] * pg[dd] * 2.0 / P.h[dd];
+                    Rout[P.cod_off[e] + m] += wq * P.scaling * acc2;
+                }
+            }
+        }
+    }
+}
+
 }  // namespace orc
+
+extern "C" int orc_xdg_evaluate(const bosss_op_desc* op, const bosss_grid_desc* g, const unsigned char* vol_flags,
+                                const unsigned char* face_flags, int64_t n_items, const int64_t* info,
+                                const int64_t* offs, const double* nodes, const double* weights, const double* U,
+                                double* out) {
+    using namespace orc;
+    Problem P;
+    g_err = setup(P, op, g);
+    if (!g_err.empty()) return BOSSS_ERR_BAD_ARG;
+    const int D = P.D, J = P.J, Nc = P.cod_per_cell;
+    std::memset(out, 0, sizeof(double) * (size_t)J * Nc);
+    std::vector<double> Rb(Nc), Ro(Nc);
+    for (int j = 0; j < J; ++j)
+        if (vol_flags[j] == 1) vol_integral(P, j, (int)P.vw.size(), P.vn.data(), P.vw.data(), U, out + (size_t)j * Nc);
+    for (int j = 0; j < J; ++j)
+        for (int d = 0; d < D; ++d)
+            for (int s = 0; s < 2; ++s) {
+                if (face_flags[(size_t)j * 2 * D + 2 * d + s] != 1) continue;
+                const int nb = neighbour(P, j, d, s);
+                if (nb >= 0 && s == 0) continue;   // interior faces from their lower cell
+                std::fill(Rb.begin(), Rb.end(), 0.0);
+                std::fill(Ro.begin(), Ro.end(), 0.0);
+                face_integral(P, j, nb, d, s ? 1.0 : -1.0, P.nQf, P.fn.data(), P.fw.data(), U, Rb.data(), Ro.data());
+                for (int i = 0; i < Nc; ++i) out[(size_t)j * Nc + i] += Rb[i];
+                if (nb >= 0)
+                    for (int i = 0; i < Nc; ++i) out[(size_t)nb * Nc + i] += Ro[i];
+            }
+    for (int64_t r = 0; r < n_items; ++r) {
+        const int j = (int)info[r * 5 + 0], dim = (int)info[r * 5 + 1], d = (int)info[r * 5 + 2], s = (int)info[r * 5 + 3];
+        const int64_t o0 = offs[r], o1 = offs[r + 1];
+        const int npts = (int)(o1 - o0);
+        std::vector<double> xi((size_t)npts * D), w(weights + o0, weights + o1);
+        if (dim == D) {
+            for (int q = 0; q < npts; ++q)
+                for (int k = 0; k < D; ++k) xi[(size_t)q * D + k] = nodes[(o0 + q) * 3 + k];
+            vol_integral(P, j, npts, xi.data(), w.data(), U, out + (size_t)j * Nc);
+        } else {
+            for (int q = 0; q < npts; ++q)
+                for (int k = 0; k < D - 1; ++k) xi[(size_t)q * (D - 1) + k] = nodes[(o0 + q) * 3 + k];
+            const int nb = neighbour(P, j, d, s);
+            std::fill(Rb.begin(), Rb.end(), 0.0);
+            std::fill(Ro.begin(), Ro.end(), 0.0);
+            face_integral(P, j, nb, d, s ? 1.0 : -1.0, npts, xi.data(), w.data(), U, Rb.data(), Ro.data());
+            for (int i = 0; i < Nc; ++i) out[(size_t)j * Nc + i] += Rb[i];
+            if (nb >= 0)
+                for (int i = 0; i < Nc; ++i) out[(size_t)nb * Nc + i] += Ro[i];
+        }
+    }
+    return 0;
+}
+
 
 using namespace orc;
 

@@ -35,6 +35,7 @@ def lib():
         L.orc_basis_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P]
         L.orc_basis_monomials.argtypes = [ctypes.c_int, ctypes.c_int, P, P]
         L.orc_threads.argtypes = [ctypes.c_int]
+        L.orc_xdg_evaluate.argtypes = [P, P, P, P, ctypes.c_int64, P, P, P, P, P, P]
         L.orc_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         _lib = L
     return _lib
@@ -151,4 +152,18 @@ def basis_monomials(D, k):
     out = []
     for p in range(Np):
         out.append([(coef[p, t], tuple(exps[p, t, :D])) for t in range(T) if coef[p, t] != 0.0])
+    return out
+
+
+def xdg_evaluate(opd, gd, rules, U):
+    """XDG bulk evaluation of one species with given rules (flags, cut items, nodes, weights)."""
+    nd, nc, _ = sizes(opd, gd)
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    out = np.zeros(nc)
+    info = np.ascontiguousarray(rules["info"], dtype=np.int64)
+    _check(lib().orc_xdg_evaluate(ctypes.byref(opd), ctypes.byref(gd), _p(np.ascontiguousarray(rules["vol_flags"])),
+                                  _p(np.ascontiguousarray(rules["face_flags"])), len(info), _p(info),
+                                  _p(np.ascontiguousarray(rules["offsets"], dtype=np.int64)),
+                                  _p(np.ascontiguousarray(rules["nodes"])), _p(np.ascontiguousarray(rules["weights"])),
+                                  _p(U), _p(out)))
     return out
