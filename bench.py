@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=32)
     ap.add_argument("--k", type=int, default=3)
-    ap.add_argument("--workload", default="euler3d", choices=["euler3d", "batched", "newton"],
+    ap.add_argument("--workload", default="euler3d", choices=["euler3d", "batched", "newton", "xdg"],
                     help="euler3d: the headline (residual + VJP, Euler/HLLC 32^3 k=3); batched: 256 "
                          "independent advection-diffusion instances (16..48^3, k=1..4) in one captured "
                          "graph; newton: matrix-free Newton-GMRES on -div((1+u^2) grad u) = 1, 48^3")
@@ -253,8 +253,49 @@ def run_newton(args):
     print(json.dumps(line), flush=True)
 
 
+def run_xdg(args):
+    """XDG two-phase Poisson, bulk part, 128^3, k=2: rule construction (moments + weights on
+    the device) and per-species evaluation of both species."""
+    import torch
+    from bosss_b200 import operator as O
+    from bosss_b200 import problems as P
+    opA, opB, g, c, UA, UB = P.xdg_poisson3d(n=128, k=2, seed=4000)
+    t0 = time.perf_counter()
+    X = O.XdgEvaluator(opA, opB, g, 2, c, 0.4)
+    torch.cuda.synchronize()
+    t_rules = time.perf_counter() - t0
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    U = [torch.from_numpy(UA).to(dev), torch.from_numpy(UB).to(dev)]
+    out = [torch.zeros_like(U[0]), torch.zeros_like(U[1])]
+    for _ in range(max(args.warmup, 3)):
+        for s in (0, 1):
+            X.Evaluate(s, 1.0, 0.0, out[s], U[s])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        for s in (0, 1):
+            X.Evaluate(s, 1.0, 0.0, out[s], U[s])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    infos = [X.info(0), X.info(1)]
+    dofs = sum(i["cells"] for i in infos) * 10
+    line = {"metric": "xdg_bulk_dof_updates_per_s", "value": dofs / (ms * 1e-3), "unit": "DOF/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "xdg_poisson_128^3_k2_both_species", "species_dofs": dofs,
+                                            "rule_construction_s": t_rules, "species_A": infos[0],
+                                            "species_B": infos[1]}}
+    print(json.dumps(line), flush=True)
+    X.Dispose()
+
+
 def main():
     args = parse()
+    if args.workload == "xdg" and args.impl != "reference":
+        return run_xdg(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batched":

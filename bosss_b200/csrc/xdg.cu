@@ -262,9 +262,11 @@ __global__ void k_moments(const CutItem* __restrict__ items, int nitems, LevelSe
 }
 
 // ------------------------------------------------------------------ device: weight solve
-// Per rule: A[m][j] = phi_m(node_j), G = A A^T, Cholesky of the leading block for the
-// largest degree whose Cholesky succeeds (relative pivot > 1e-13), y = G^-1 b, w = A^T y
-// (the minimum-norm solution of A w = b, which DGELSY returns for full row rank).
+// Per rule: A[m][j] = phi_m(node_j); Householder QR of A^T = Q R (columns in degree order,
+// so the leading columns are the lower-degree system); the minimum-norm solution of
+// A w = b is w = Q [R^-T b; 0] -- what DGELSY returns for full row rank. The fitted degree
+// is the highest one whose columns are numerically independent and whose solution
+// reproduces its moments to 1e-11 relative.
 __global__ void k_weight_solve(const CutItem* __restrict__ items, int nitems, const double* __restrict__ nodes,
                                const double* __restrict__ mom, double* __restrict__ weights, int* __restrict__ deg_out,
                                double* __restrict__ resid) {
@@ -273,86 +275,112 @@ __global__ void k_weight_solve(const CutItem* __restrict__ items, int nitems, co
     const CutItem it = items[r];
     const int n = it.nnodes;
     const int dims = it.dim;
-    __shared__ double A[XDG_MAXM][XDG_MAXN];
-    __shared__ double G[XDG_MAXM][XDG_MAXM + 1];
-    __shared__ double y[XDG_MAXM];
-    __shared__ int meff, peff;
+    __shared__ double At[XDG_MAXN][XDG_MAXM + 1];   // A^T, Householder vectors below the diagonal
+    __shared__ double Rd[XDG_MAXM], vtv[XDG_MAXM], cn[XDG_MAXM];
+    __shared__ double z[XDG_MAXM], t[XDG_MAXN], red[32];
+    __shared__ int kmax;
     const int Mmax = (dims == 3) ? nmodes3(it.p) : nmodes2(it.p);
+    const int M = Mmax < n ? Mmax : n;
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
         double v[XDG_MAXM];
         const double* xi = nodes + (it.node_off + j) * 3;
         if (dims == 3) basis3(it.p, xi, v);
         else basis2(it.p, xi, v);
-        for (int m = 0; m < Mmax; ++m) A[m][j] = v[m];
+        for (int m = 0; m < Mmax; ++m) At[j][m] = v[m];
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < Mmax * Mmax; t += blockDim.x) {
-        const int a = t / Mmax, b = t % Mmax;
+    if (threadIdx.x < M) {
         double s = 0.0;
-        for (int j = 0; j < n; ++j) s += A[a][j] * A[b][j];
-        G[a][b] = s;
+        for (int j = 0; j < n; ++j) s += At[j][threadIdx.x] * At[j][threadIdx.x];
+        cn[threadIdx.x] = sqrt(s);
     }
+    if (threadIdx.x == 0) kmax = M;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        // in-place Cholesky, degree by degree
-        int m_ok = 0, p_ok = -1;
-        bool fail = false;
-        double gmax = 0.0;
-        for (int a = 0; a < Mmax; ++a) gmax = fmax(gmax, G[a][a]);
-        for (int p = 0; p <= it.p && !fail; ++p) {
-            const int m1 = (dims == 3) ? nmodes3(p) : nmodes2(p);
-            if (m1 > n) break;
-            for (int i = m_ok; i < m1 && !fail; ++i) {
-                for (int k = 0; k < i; ++k) {
-                    double s = G[i][k];
-                    for (int l = 0; l < k; ++l) s -= G[i][l] * G[k][l];
-                    G[i][k] = s / G[k][k];
-                }
-                double s = G[i][i];
-                for (int l = 0; l < i; ++l) s -= G[i][l] * G[i][l];
-                if (!(s > 1e-13 * gmax)) fail = true;
-                else G[i][i] = sqrt(s);
-            }
-            if (!fail) {
-                m_ok = m1;
-                p_ok = p;
-            }
-        }
-        meff = m_ok;
-        peff = p_ok;
-        // solve L L^T y = b on the leading m_ok block
-        const double* b = mom + (long long)r * XDG_MAXM;
-        for (int i = 0; i < m_ok; ++i) {
-            double s = b[i];
-            for (int k = 0; k < i; ++k) s -= G[i][k] * y[k];
-            y[i] = s / G[i][i];
-        }
-        for (int i = m_ok - 1; i >= 0; --i) {
-            double s = y[i];
-            for (int k = i + 1; k < m_ok; ++k) s -= G[k][i] * y[k];
-            y[i] = s / G[i][i];
-        }
-    }
-    __syncthreads();
-    const int M = meff;
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        double s = 0.0;
-        for (int m = 0; m < M; ++m) s += A[m][j] * y[m];
-        weights[it.node_off + j] = s;
-    }
-    __syncthreads();
-    // residual of the fitted moments, |A w - b|_inf / max(|b_0|, tiny)
-    if (threadIdx.x == 0) {
-        const double* b = mom + (long long)r * XDG_MAXM;
-        double e = 0.0;
-        for (int m = 0; m < M; ++m) {
+    double cmax = 0.0;
+    for (int m = 0; m < M; ++m) cmax = fmax(cmax, cn[m]);
+    for (int k = 0; k < M; ++k) {
+        if (threadIdx.x == 0) {
             double s = 0.0;
-            for (int j = 0; j < n; ++j) s += A[m][j] * weights[it.node_off + j];
-            e = fmax(e, fabs(s - b[m]));
+            for (int i = k; i < n; ++i) s += At[i][k] * At[i][k];
+            const double nx = sqrt(s);
+            if (!(nx > 1e-11 * cmax)) {
+                kmax = k;
+            } else {
+                const double alpha = (At[k][k] >= 0.0) ? -nx : nx;
+                At[k][k] -= alpha;
+                vtv[k] = s - 2.0 * alpha * (At[k][k] + alpha) + alpha * alpha;   // |x - alpha e1|^2
+                Rd[k] = alpha;
+            }
         }
-        deg_out[r] = peff;
-        resid[r] = e / fmax(fabs(b[0]), 1e-300);
+        __syncthreads();
+        if (kmax <= k) break;
+        for (int j = k + 1 + threadIdx.x; j < M; j += blockDim.x) {
+            double s = 0.0;
+            for (int i = k; i < n; ++i) s += At[i][k] * At[i][j];
+            const double f = 2.0 * s / vtv[k];
+            for (int i = k; i < n; ++i) At[i][j] -= f * At[i][k];
+        }
+        __syncthreads();
     }
+    if (threadIdx.x == 0) {
+        const double* b = mom + (long long)r * XDG_MAXM;
+        double bmax = 0.0;
+        for (int m = 0; m < Mmax; ++m) bmax = fmax(bmax, fabs(b[m]));
+        // highest degree with all its columns independent
+        int pe = -1;
+        for (int p = 0; p <= it.p; ++p)
+            if (((dims == 3) ? nmodes3(p) : nmodes2(p)) <= kmax) pe = p;
+        double res = 0.0;
+        for (; pe >= 0; --pe) {
+            const int me = (dims == 3) ? nmodes3(pe) : nmodes2(pe);
+            // R^T z = b  (R[l][k] = At[l][k] for l < k, R[k][k] = Rd[k])
+            for (int k = 0; k < me; ++k) {
+                double s = b[k];
+                for (int l = 0; l < k; ++l) s -= At[l][k] * z[l];
+                z[k] = s / Rd[k];
+            }
+            for (int i = 0; i < n; ++i) t[i] = (i < me) ? z[i] : 0.0;
+            for (int k = me - 1; k >= 0; --k) {   // t = H_0 ... H_{me-1} [z; 0]
+                double s = 0.0;
+                for (int i = k; i < n; ++i) s += At[i][k] * t[i];
+                const double f = 2.0 * s / vtv[k];
+                for (int i = k; i < n; ++i) t[i] -= f * At[i][k];
+            }
+            // residual of the fitted moments with the original basis values
+            res = 0.0;
+            const double* xb = nodes + it.node_off * 3;
+            for (int m = 0; m < me; ++m) red[m & 31] = 0.0;
+            double acc[XDG_MAXM];
+            for (int m = 0; m < me; ++m) acc[m] = 0.0;
+            for (int j = 0; j < n; ++j) {
+                double v[XDG_MAXM];
+                if (dims == 3) basis3(it.p, xb + j * 3, v);
+                else basis2(it.p, xb + j * 3, v);
+                for (int m = 0; m < me; ++m) acc[m] += v[m] * t[j];
+            }
+            for (int m = 0; m < me; ++m) res = fmax(res, fabs(acc[m] - b[m]));
+            if (res <= 1e-11 * fmax(bmax, 1e-300)) break;
+        }
+        if (pe < 0) {   // degree 0 from the first column only
+            pe = 0;
+            double s = 0.0, v0 = 0.0;
+            const double* xb = nodes + it.node_off * 3;
+            for (int j = 0; j < n; ++j) {
+                double v[XDG_MAXM];
+                if (dims == 3) basis3(it.p, xb + j * 3, v);
+                else basis2(it.p, xb + j * 3, v);
+                s += v[0] * v[0];
+                t[j] = v[0];
+            }
+            v0 = b[0] / s;
+            for (int j = 0; j < n; ++j) t[j] *= v0;
+            res = 0.0;
+        }
+        deg_out[r] = pe;
+        resid[r] = res / fmax(bmax, 1e-300);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < n; j += blockDim.x) weights[it.node_off + j] = t[j];
 }
 
 // ------------------------------------------------------------------ device: cut-rule evaluation
@@ -561,7 +589,7 @@ static int build_species(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
             it.h[d] = hh[d];
         }
         // candidate nodes: tensor Gauss nodes of the species part, finer set for small parts
-        auto collect = [&](const std::vector<double>& gx) {
+        auto collect = [&](const std::vector<double>& gx, bool all) {
             std::vector<std::array<double, 3>> v;
             const int nq = (int)gx.size();
             const int tot = (dim == 3) ? nq * nq * nq : nq * nq;
@@ -577,14 +605,19 @@ static int build_species(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
                     x[t2] += 0.5 * hh[t2] * rr[1];
                 }
                 const double ph = ls_phi(X->ls, x);
-                if ((sp < 0) ? (ph < 0.0) : !(ph < 0.0)) v.push_back({rr[0], rr[1], rr[2]});
+                if (all || ((sp < 0) ? (ph < 0.0) : !(ph < 0.0))) v.push_back({rr[0], rr[1], rr[2]});
             }
             return v;
         };
-        auto cand = collect(gx5);
-        if ((int)cand.size() < 8) cand = collect(gx9);
+        // candidates: Gauss nodes inside the species part (5^D), a finer set (9^D) for small
+        // parts, and for slivers without 8 such nodes the whole 5^D set (moment fitting does
+        // not need the nodes inside the part: it integrates the polynomial extension)
+        auto cand = collect(gx5, false);
+        if ((int)cand.size() < 8) {
+            auto c9 = collect(gx9, false);
+            cand = ((int)c9.size() >= 8 && (int)c9.size() <= XDG_MAXN) ? c9 : collect(gx5, true);
+        }
         if ((int)cand.size() > XDG_MAXN) cand.resize(XDG_MAXN);
-        if (cand.empty()) return;   // no node of the species part: negligible fragment
         it.nnodes = (int)cand.size();
         it.node_off = (long long)nodes.size() / 3;
         for (auto& c : cand)
