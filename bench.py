@@ -49,10 +49,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=32)
     ap.add_argument("--k", type=int, default=3)
-    ap.add_argument("--workload", default="euler3d", choices=["euler3d", "batched", "newton", "xdg"],
+    ap.add_argument("--workload", default="euler3d", choices=["euler3d", "batched", "newton", "xdg", "rk"],
                     help="euler3d: the headline (residual + VJP, Euler/HLLC 32^3 k=3); batched: 256 "
                          "independent advection-diffusion instances (16..48^3, k=1..4) in one captured "
-                         "graph; newton: matrix-free Newton-GMRES on -div((1+u^2) grad u) = 1, 48^3")
+                         "graph; newton: matrix-free Newton-GMRES on -div((1+u^2) grad u) = 1, 48^3; rk: "
+                         "classical RK4 time steps of the Euler workload, one step captured in a CUDA graph")
     ap.add_argument("--instances", type=int, default=256)
     return ap.parse_args()
 
@@ -292,8 +293,78 @@ def run_xdg(args):
     X.Dispose()
 
 
+def run_rk(args):
+    """Classical RK4 time steps (RungeKutta.Perform) of the Euler 32^3 k=3 workload: each step
+    is four residual launches and four fused stage-combination launches, captured once into a
+    CUDA graph; value = DOF stage-updates/s (DOFs x 4 per step). Beside it: the same steps as
+    an uncaptured host loop of residual launches and torch vector updates."""
+    import torch
+    from bosss_b200 import problems as P
+    from bosss_b200 import timestepping as T
+    pr = P.euler3d(n=args.n, k=args.k, seed=2000)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ev = pr.evaluator()
+    scheme = T.RungeKuttaScheme.RungeKutta1901()
+    rk = T.RungeKutta(scheme, ev, None)
+    dt = 1e-4
+    U = torch.from_numpy(pr.U).to(dev)
+    nsteps = max(args.steps // 10, 5)
+    rk.PerformDevice(U, dt, nsteps=max(args.warmup, 3))
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rk.PerformDevice(U, dt, nsteps=nsteps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / nsteps
+
+    # uncaptured host loop: k_s = Op(u_s) with evaluate_device, stage sums with torch
+    a, b = scheme.a, scheme.b
+    K = [torch.empty_like(U) for _ in range(4)]
+    us = torch.empty_like(U)
+
+    def host_step():
+        for s_ in range(4):
+            us.copy_(U)
+            for r in range(s_):
+                if a[s_, r] != 0.0:
+                    us.add_(K[r], alpha=-dt * a[s_, r])
+            ev.Evaluate(1.0, 0.0, K[s_], us)
+        for s_ in range(4):
+            U.add_(K[s_], alpha=-dt * b[s_])
+
+    for _ in range(3):
+        host_step()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(nsteps):
+        host_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_host = e0.elapsed_time(e1) / nsteps
+    ev.Dispose()
+    value = 4 * pr.n_dofs / (ms * 1e-3)
+    line = {"metric": "rk4_dof_stage_updates_per_s", "value": value, "unit": "DOF/s", "n_gpus": 1,
+            "steps": nsteps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": pr.config["workload"] + "_rk4", "dofs": pr.n_dofs, "dt": dt,
+                       "launch": "one step captured in a CUDA graph: 4 residual + 4 stage-combination launches",
+                       "l2": "not flushed (working set of U, k_0..k_3 and u_s: 6 x %.0f MB)" % (pr.n_dofs * 8 / 1e6)},
+            "host_loop": {"ms_per_step": ms_host, "value": 4 * pr.n_dofs / (ms_host * 1e-3),
+                          "graph_speedup": ms_host / ms},
+            "gpu_launches": 8 * nsteps, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "rk" and args.impl != "reference":
+        return run_rk(args)
     if args.workload == "xdg" and args.impl != "reference":
         return run_xdg(args)
     if args.impl == "reference":
@@ -363,6 +434,28 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     value = world * DOF_PER_STEP_FACTOR * n * args.steps / (total_ms * 1e-3)
+
+    # ---- the plain fused FP64 kernel (generic, one CTA per tile) on the same state, for
+    # the chosen-vs-plain ratio
+    ev_plain = pr.evaluator(device=local, kernel=C.KERNEL_GENERIC)
+    hp = ev_plain.handle
+    for _ in range(3):
+        C.check(L.bosss_b200_evaluate_device(hp, 1.0, 0.0, C.ptr(U), C.ptr(R), 0.0, sptr))
+        C.check(L.bosss_b200_vjp_device(hp, C.ptr(U), C.ptr(W), C.ptr(G), 0.0, sptr))
+    torch.cuda.synchronize()
+    plain_ms = []
+    for i in range(min(args.steps, 50)):
+        flush.fill_(float(i))
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        C.check(L.bosss_b200_evaluate_device(hp, 1.0, 0.0, C.ptr(U), C.ptr(R), 0.0, sptr))
+        C.check(L.bosss_b200_vjp_device(hp, C.ptr(U), C.ptr(W), C.ptr(G), 0.0, sptr))
+        a1.record(stream)
+        plain_ms.append((a0, a1))
+    torch.cuda.synchronize()
+    plain_step_ms = float(np.mean([a.elapsed_time(b) for a, b in plain_ms]))
+    plain_value = world * DOF_PER_STEP_FACTOR * n / (plain_step_ms * 1e-3)
+    ev_plain.Dispose()
 
     # ---- end to end through the host-buffer C-ABI (pinned host memory)
     Uh = torch.from_numpy(pr.U.copy()).pin_memory()
@@ -439,6 +532,9 @@ def main():
                      "nominal_peak_tflops": 37.0,
                      "note": "FP64 pipe bound; flops per launch from the ncu capture in profiles/"},
             "per_kernel": per_kernel,
+            "plain_fp64": {"kernel": "dg_cell_kernel (generic fused FP64, one CTA per tile of cells)",
+                           "value": plain_value, "ms_per_step": plain_step_ms,
+                           "chosen_over_plain": value / plain_value},
             "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk,

@@ -194,6 +194,11 @@ SIGNATURES = {
                                                       ctypes.c_double, _P]),
     "bosss_b200_batch_evaluate_noalloc": (ctypes.c_int, [ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_double,
                                                          ctypes.c_double, _P, _P, _P, ctypes.c_double, _P]),
+    "bosss_b200_rk_work_size": (ctypes.c_int, [_P, ctypes.c_int32, _I64]),
+    "bosss_b200_rk_steps_device": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, ctypes.c_double, ctypes.c_int32,
+                                                  ctypes.c_double, _P, _P, ctypes.c_int32, _P]),
+    "bosss_b200_rk_steps": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, ctypes.c_double, ctypes.c_int32,
+                                           ctypes.c_double, _P]),
 }
 
 _lib = None

@@ -326,6 +326,26 @@ int bosss_b200_xdg_evaluate(bosss_xdg* X, int32_t species, double alpha, double 
 int bosss_b200_xdg_evaluate_device(bosss_xdg* X, int32_t species, double alpha, double beta, const double* U_dev,
                                    double* out_dev, double time, void* stream);
 
+/* ---- explicit Runge-Kutta time stepping ----
+ * RungeKutta.Perform / PerformStage (TimeStepping/RungeKutta.cs:240-330) with the change rate
+ * of ExplicitEuler.ComputeChangeRate (ExplicitEuler.cs:223-229): for s = 0..stages-1
+ *   u_s = U - dt * sum_{r<s} a[s][r] k_r,   k_s = Op(u_s)   (evaluated at time + c[s]*dt),
+ * then U <- U - dt * sum_s b[s] k_s. `a` is stages x stages row-major and strictly lower
+ * triangular (explicit), `b` and `c` have `stages` entries, stages <= 8. The operator must be
+ * square (domain DOFs == codomain DOFs). Named tableaus (RungeKuttaScheme.cs) are supplied by
+ * the caller; the Python mirror carries them. */
+int bosss_b200_rk_work_size(const bosss_handle* h, int32_t stages, int64_t* n_doubles);
+/* nsteps steps on device buffers: U_dev in/out, work_dev of bosss_b200_rk_work_size doubles.
+ * use_graph != 0: one step is captured into a CUDA graph once and the graph is launched nsteps
+ * times (one residual launch and one stage-combination launch per stage). Asynchronous on
+ * `stream` (NULL: the handle's stream). */
+int bosss_b200_rk_steps_device(bosss_handle* h, int32_t stages, const double* a, const double* b, const double* c,
+                               double dt, int32_t nsteps, double time, double* U_dev, double* work_dev,
+                               int32_t use_graph, void* stream);
+/* Same with a host state vector U (copied in, stepped with a captured graph, copied back). */
+int bosss_b200_rk_steps(bosss_handle* h, int32_t stages, const double* a, const double* b, const double* c, double dt,
+                        int32_t nsteps, double time, double* U);
+
 /* Batched evaluation that allocates no device memory (no counterpart in the reference).
  * For callers that cannot call cudaMalloc: hosts whose device memory belongs to another
  * allocator, or loops that must not synchronise the device with an allocation. Same

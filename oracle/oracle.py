@@ -167,3 +167,29 @@ def xdg_evaluate(opd, gd, rules, U):
                                   _p(np.ascontiguousarray(rules["nodes"])), _p(np.ascontiguousarray(rules["weights"])),
                                   _p(U), _p(out)))
     return out
+
+
+def rk_steps(opd, gd, U, a, b, c, dt, nsteps=1):
+    """Explicit Runge-Kutta steps of du/dt = -Op(u) on the oracle evaluator, restating
+    RungeKutta.Perform / PerformStage (TimeStepping/RungeKutta.cs:242-313): k_s = Op(u_s) into a
+    cleared k (ExplicitEuler.ComputeChangeRate, ExplicitEuler.cs:223-229), u_s = y0 -
+    dt*sum_{r<s} a[s,r] k_r, y1 = y0 - dt*sum_s b[s] k_s."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64).ravel()
+    S = b.size
+    a = a.reshape(S, S)
+    y = np.array(U, dtype=np.float64, copy=True)
+    for _ in range(nsteps):
+        k = []
+        for s in range(S):
+            u = y.copy()
+            for r in range(s):
+                if a[s, r] != 0.0:
+                    u += -dt * a[s, r] * k[r]
+            k.append(evaluate(opd, gd, u, 1.0, 1.0, np.zeros_like(u)))
+        upd = np.zeros_like(y)
+        for s in range(S):
+            if b[s] != 0.0:
+                upd += -b[s] * dt * k[s]
+        y = y + upd
+    return y
