@@ -439,22 +439,24 @@ def main():
     # the chosen-vs-plain ratio
     ev_plain = pr.evaluator(device=local, kernel=C.KERNEL_GENERIC)
     hp = ev_plain.handle
+    Rp, Gp = torch.empty_like(R), torch.empty_like(G)   # R, G keep the chosen kernel's results
     for _ in range(3):
-        C.check(L.bosss_b200_evaluate_device(hp, 1.0, 0.0, C.ptr(U), C.ptr(R), 0.0, sptr))
-        C.check(L.bosss_b200_vjp_device(hp, C.ptr(U), C.ptr(W), C.ptr(G), 0.0, sptr))
+        C.check(L.bosss_b200_evaluate_device(hp, 1.0, 0.0, C.ptr(U), C.ptr(Rp), 0.0, sptr))
+        C.check(L.bosss_b200_vjp_device(hp, C.ptr(U), C.ptr(W), C.ptr(Gp), 0.0, sptr))
     torch.cuda.synchronize()
     plain_ms = []
     for i in range(min(args.steps, 50)):
         flush.fill_(float(i))
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(stream)
-        C.check(L.bosss_b200_evaluate_device(hp, 1.0, 0.0, C.ptr(U), C.ptr(R), 0.0, sptr))
-        C.check(L.bosss_b200_vjp_device(hp, C.ptr(U), C.ptr(W), C.ptr(G), 0.0, sptr))
+        C.check(L.bosss_b200_evaluate_device(hp, 1.0, 0.0, C.ptr(U), C.ptr(Rp), 0.0, sptr))
+        C.check(L.bosss_b200_vjp_device(hp, C.ptr(U), C.ptr(W), C.ptr(Gp), 0.0, sptr))
         a1.record(stream)
         plain_ms.append((a0, a1))
     torch.cuda.synchronize()
     plain_step_ms = float(np.mean([a.elapsed_time(b) for a, b in plain_ms]))
     plain_value = world * DOF_PER_STEP_FACTOR * n / (plain_step_ms * 1e-3)
+    plain_diff = max(float((Rp - R).abs().max() / R.abs().max()), float((Gp - G).abs().max() / G.abs().max()))
     ev_plain.Dispose()
 
     # ---- end to end through the host-buffer C-ABI (pinned host memory)
@@ -534,7 +536,8 @@ def main():
             "per_kernel": per_kernel,
             "plain_fp64": {"kernel": "dg_cell_kernel (generic fused FP64, one CTA per tile of cells)",
                            "value": plain_value, "ms_per_step": plain_step_ms,
-                           "chosen_over_plain": value / plain_value},
+                           "chosen_over_plain": value / plain_value,
+                           "max_rel_diff": plain_diff},
             "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk,
