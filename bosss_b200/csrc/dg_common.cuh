@@ -65,7 +65,7 @@ struct DualN {
 };
 
 template <int N>
-__device__ __forceinline__ DualN<N> operator+(const DualN<N>& a, const DualN<N>& b) {
+__host__ __device__ __forceinline__ DualN<N> operator+(const DualN<N>& a, const DualN<N>& b) {
     DualN<N> r;
     r.v = a.v + b.v;
 #pragma unroll
@@ -73,7 +73,7 @@ __device__ __forceinline__ DualN<N> operator+(const DualN<N>& a, const DualN<N>&
     return r;
 }
 template <int N>
-__device__ __forceinline__ DualN<N> operator-(const DualN<N>& a, const DualN<N>& b) {
+__host__ __device__ __forceinline__ DualN<N> operator-(const DualN<N>& a, const DualN<N>& b) {
     DualN<N> r;
     r.v = a.v - b.v;
 #pragma unroll
@@ -81,7 +81,7 @@ __device__ __forceinline__ DualN<N> operator-(const DualN<N>& a, const DualN<N>&
     return r;
 }
 template <int N>
-__device__ __forceinline__ DualN<N> operator-(const DualN<N>& a) {
+__host__ __device__ __forceinline__ DualN<N> operator-(const DualN<N>& a) {
     DualN<N> r;
     r.v = -a.v;
 #pragma unroll
@@ -89,7 +89,7 @@ __device__ __forceinline__ DualN<N> operator-(const DualN<N>& a) {
     return r;
 }
 template <int N>
-__device__ __forceinline__ DualN<N> operator*(const DualN<N>& a, const DualN<N>& b) {
+__host__ __device__ __forceinline__ DualN<N> operator*(const DualN<N>& a, const DualN<N>& b) {
     DualN<N> r;
     r.v = a.v * b.v;
 #pragma unroll
@@ -97,7 +97,7 @@ __device__ __forceinline__ DualN<N> operator*(const DualN<N>& a, const DualN<N>&
     return r;
 }
 template <int N>
-__device__ __forceinline__ DualN<N> operator/(const DualN<N>& a, const DualN<N>& b) {
+__host__ __device__ __forceinline__ DualN<N> operator/(const DualN<N>& a, const DualN<N>& b) {
     DualN<N> r;
     double inv = 1.0 / b.v;
     r.v = a.v * inv;
@@ -105,23 +105,23 @@ __device__ __forceinline__ DualN<N> operator/(const DualN<N>& a, const DualN<N>&
     for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * inv;
     return r;
 }
-template <int N> __device__ __forceinline__ DualN<N> operator+(const DualN<N>& a, double b) { DualN<N> r = a; r.v += b; return r; }
-template <int N> __device__ __forceinline__ DualN<N> operator+(double b, const DualN<N>& a) { DualN<N> r = a; r.v += b; return r; }
-template <int N> __device__ __forceinline__ DualN<N> operator-(const DualN<N>& a, double b) { DualN<N> r = a; r.v -= b; return r; }
-template <int N> __device__ __forceinline__ DualN<N> operator-(double b, const DualN<N>& a) { DualN<N> r = -a; r.v += b; return r; }
+template <int N> __host__ __device__ __forceinline__ DualN<N> operator+(const DualN<N>& a, double b) { DualN<N> r = a; r.v += b; return r; }
+template <int N> __host__ __device__ __forceinline__ DualN<N> operator+(double b, const DualN<N>& a) { DualN<N> r = a; r.v += b; return r; }
+template <int N> __host__ __device__ __forceinline__ DualN<N> operator-(const DualN<N>& a, double b) { DualN<N> r = a; r.v -= b; return r; }
+template <int N> __host__ __device__ __forceinline__ DualN<N> operator-(double b, const DualN<N>& a) { DualN<N> r = -a; r.v += b; return r; }
 template <int N>
-__device__ __forceinline__ DualN<N> operator*(const DualN<N>& a, double b) {
+__host__ __device__ __forceinline__ DualN<N> operator*(const DualN<N>& a, double b) {
     DualN<N> r;
     r.v = a.v * b;
 #pragma unroll
     for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b;
     return r;
 }
-template <int N> __device__ __forceinline__ DualN<N> operator*(double b, const DualN<N>& a) { return a * b; }
+template <int N> __host__ __device__ __forceinline__ DualN<N> operator*(double b, const DualN<N>& a) { return a * b; }
 template <int N>
-__device__ __forceinline__ DualN<N> operator/(const DualN<N>& a, double b) { return a * (1.0 / b); }
+__host__ __device__ __forceinline__ DualN<N> operator/(const DualN<N>& a, double b) { return a * (1.0 / b); }
 template <int N>
-__device__ __forceinline__ DualN<N> operator/(double a, const DualN<N>& b) {
+__host__ __device__ __forceinline__ DualN<N> operator/(double a, const DualN<N>& b) {
     DualN<N> r;
     double inv = 1.0 / b.v;
     r.v = a * inv;
@@ -129,15 +129,15 @@ __device__ __forceinline__ DualN<N> operator/(double a, const DualN<N>& b) {
     for (int i = 0; i < N; ++i) r.d[i] = -r.v * b.d[i] * inv;
     return r;
 }
-template <int N> __device__ __forceinline__ DualN<N>& operator+=(DualN<N>& a, const DualN<N>& b) { a = a + b; return a; }
-template <int N> __device__ __forceinline__ DualN<N>& operator-=(DualN<N>& a, const DualN<N>& b) { a = a - b; return a; }
-template <int N> __device__ __forceinline__ DualN<N>& operator*=(DualN<N>& a, const DualN<N>& b) { a = a * b; return a; }
-template <int N> __device__ __forceinline__ DualN<N>& operator/=(DualN<N>& a, const DualN<N>& b) { a = a / b; return a; }
-template <int N> __device__ __forceinline__ DualN<N>& operator+=(DualN<N>& a, double b) { a.v += b; return a; }
-template <int N> __device__ __forceinline__ DualN<N>& operator-=(DualN<N>& a, double b) { a.v -= b; return a; }
+template <int N> __host__ __device__ __forceinline__ DualN<N>& operator+=(DualN<N>& a, const DualN<N>& b) { a = a + b; return a; }
+template <int N> __host__ __device__ __forceinline__ DualN<N>& operator-=(DualN<N>& a, const DualN<N>& b) { a = a - b; return a; }
+template <int N> __host__ __device__ __forceinline__ DualN<N>& operator*=(DualN<N>& a, const DualN<N>& b) { a = a * b; return a; }
+template <int N> __host__ __device__ __forceinline__ DualN<N>& operator/=(DualN<N>& a, const DualN<N>& b) { a = a / b; return a; }
+template <int N> __host__ __device__ __forceinline__ DualN<N>& operator+=(DualN<N>& a, double b) { a.v += b; return a; }
+template <int N> __host__ __device__ __forceinline__ DualN<N>& operator-=(DualN<N>& a, double b) { a.v -= b; return a; }
 
 template <int N>
-__device__ __forceinline__ DualN<N> dsqrt(const DualN<N>& a) {
+__host__ __device__ __forceinline__ DualN<N> dsqrt(const DualN<N>& a) {
     DualN<N> r;
     r.v = sqrt(a.v);
     double s = 0.5 / r.v;
@@ -145,9 +145,9 @@ __device__ __forceinline__ DualN<N> dsqrt(const DualN<N>& a) {
     for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * s;
     return r;
 }
-__device__ __forceinline__ double dsqrt(double a) { return sqrt(a); }
+__host__ __device__ __forceinline__ double dsqrt(double a) { return sqrt(a); }
 
-__device__ __forceinline__ double pval(double a) { return a; }
-template <int N> __device__ __forceinline__ double pval(const DualN<N>& a) { return a.v; }
+__host__ __device__ __forceinline__ double pval(double a) { return a; }
+template <int N> __host__ __device__ __forceinline__ double pval(const DualN<N>& a) { return a.v; }
 
 }  // namespace bosss

@@ -11,6 +11,8 @@
 // (residual), with DualN<1> (JVP) and with DualN<n> (gradient of the adjoint functional,
 // VJP). Outputs are accumulated (+=).
 #pragma once
+#include <cmath>
+
 #include "dg_common.cuh"
 
 namespace bosss {
@@ -28,7 +30,7 @@ struct PhysParams {
     double gamma, mach;   // HLLC
 };
 
-template <class T> __device__ __forceinline__ T tconst(double a) { return T(a); }
+template <class T> __host__ __device__ __forceinline__ T tconst(double a) { return T(a); }
 
 // --------------------------------------------------------------- scalar: transport + SIP + source
 // ScalarTransportFlux(3D)  ScalarTransport/TransportFlux.cs:29-191
@@ -42,6 +44,7 @@ struct PhysScalar {
     static constexpr bool VOL_G = true;
     static constexpr bool FACE_V = true;
     static constexpr bool FACE_G = SIP;     // symmetry term of SIP
+    static constexpr bool ADJOINT = false;  // VJP by forward mode over the node's state
 
     template <class T>
     __device__ static void volume(const PhysParams& p, const T* U, const T (*G)[D], const double* x, T* fV,
@@ -143,7 +146,7 @@ struct PhysEuler {
     static constexpr bool FACE_G = false;
 
     template <class T>
-    __device__ static void volume(const PhysParams& p, const T* U, const T (*G)[D], const double* x, T* fV,
+    __host__ __device__ static void volume(const PhysParams& p, const T* U, const T (*G)[D], const double* x, T* fV,
                                   T (*fG)[D]) {
         (void)G; (void)x; (void)fV;
         const double gMs = p.gamma * p.mach * p.mach;
@@ -173,7 +176,7 @@ struct PhysEuler {
     }
 
     template <class T>
-    __device__ static void inner(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D], const T* UB,
+    __host__ __device__ static void inner(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D], const T* UB,
                                  const T (*GB)[D], const double* n, const double* x, T* gA, T (*GAv)[D], T* gB,
                                  T (*GBv)[D]) {
         (void)pnlty; (void)GA; (void)GB; (void)x; (void)GAv; (void)GBv;
@@ -259,10 +262,221 @@ struct PhysEuler {
     }
 
     template <class T>
-    __device__ static void boundary(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
+    __host__ __device__ static void boundary(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
                                     const double* n, const double* x, T* gA, T (*GAv)[D]) {
         // no boundary-condition map on the device: create() rejects non-periodic Euler grids
         (void)p; (void)pnlty; (void)UA; (void)GA; (void)n; (void)x; (void)gA; (void)GAv;
+    }
+
+    // ---- reverse-mode adjoints (VJP): one primal sweep plus one reverse sweep per node in
+    // place of the NV-slot forward mode. Same functions as volume() / inner() above,
+    // differentiated by hand.
+    static constexpr bool ADJOINT = true;
+
+    // Ub[i] = d/dU_i sum_{e,d} fG[e][d] * Gw[e][d] with fG = -F(U) (volume flux)
+    __host__ __device__ static void volume_adj(const PhysParams& p, const double* U, const double (*Gw)[D],
+                                               double* Ub) {
+        const double g = p.gamma, gMs = g * p.mach * p.mach;
+        const double rho = U[0], E = U[D + 1], irho = 1.0 / rho;
+        double u[D], msq = 0.0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            u[d] = U[d + 1] * irho;
+            msq += U[d + 1] * U[d + 1];
+        }
+        const double pm = (E - msq * irho * (gMs * 0.5)) * ((g - 1.0) / gMs);
+        const double pe = gMs * pm;
+        double A = 0.0, gu = 0.0, uMu = 0.0, usq = 0.0;
+        double Mu[D], Mtu[D];
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            A += Gw[c + 1][c];
+            gu += Gw[D + 1][c] * u[c];
+            usq += u[c] * u[c];
+            Mu[c] = 0.0;
+            Mtu[c] = 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c < D; ++c)
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                Mu[c] += Gw[c + 1][d] * u[d];
+                Mtu[c] += Gw[d + 1][c] * u[d];
+            }
+#pragma unroll
+        for (int c = 0; c < D; ++c) uMu += u[c] * Mu[c];
+        const double Epe = (E + pe) * irho;
+        const double gm1 = g - 1.0;
+        const double s = A + gMs * gu;
+        Ub[0] = uMu - 0.5 * gm1 * usq * s + gu * Epe;
+#pragma unroll
+        for (int k = 0; k < D; ++k) Ub[k + 1] = -(Gw[0][k] + Mu[k] + Mtu[k] - gm1 * u[k] * s + Gw[D + 1][k] * Epe);
+        Ub[D + 1] = -(A * gm1 / gMs + gu * g);
+    }
+
+    // UAb / UBb = gradient of sum_c f_c(UA, UB) * fb[c] (f: the HLLC flux of inner())
+    __host__ __device__ static void inner_adj(const PhysParams& p, const double* UA, const double* UB,
+                                              const double* n, const double* fb, double* UAb, double* UBb) {
+        const double g = p.gamma, Ma = p.mach, MS = g * Ma * Ma, G2 = 0.5 * (g + 1.0) / g;
+        // ---- primal
+        const double rA = UA[0], rB = UB[0], EA = UA[D + 1], EB = UB[D + 1];
+        double msA = 0.0, msB = 0.0, unrA = 0.0, unrB = 0.0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            msA += UA[d + 1] * UA[d + 1];
+            msB += UB[d + 1] * UB[d + 1];
+            unrA += UA[d + 1] * n[d];
+            unrB += UB[d + 1] * n[d];
+        }
+        const double unA = unrA / rA, unB = unrB / rB;
+        const double kA = msA / rA, kB = msB / rB;
+        const double pA = (EA - kA * (MS * 0.5)) * (g - 1.0), pB = (EB - kB * (MS * 0.5)) * (g - 1.0);
+        const double yA = pA / rA, yB = pB / rB;
+        const double cA = sqrt(yA) / Ma, cB = sqrt(yB) / Ma;
+        const double rhoMean = (rA + rB) * 0.5, pMean = (pA + pB) * 0.5, cMean = (cA + cB) * 0.5;
+        const double vJ = unB - unA;
+        const double pSraw = pMean - vJ * cMean * rhoMean * (0.5 * MS);
+        const bool clamp = 0.0 > pSraw;
+        const double pS = clamp ? 0.0 : pSraw;
+        const bool qAact = pS > pA, qBact = pS > pB;
+        const double qA = qAact ? sqrt(1.0 + (pS / pA - 1.0) * G2) : 1.0;
+        const double qB = qBact ? sqrt(1.0 + (pS / pB - 1.0) * G2) : 1.0;
+        const double sA = unA - cA * qA, sB = unB + cB * qB;
+        const double CA = rA * (sA - unA), CB = rB * (sB - unB);
+        const double Dd = CB - CA;
+        const double S = (CB * unB - CA * unA + (pA - pB) / MS) / Dd;
+        const bool left = S > 0.0;
+        const bool star = left ? (sA <= 0.0) : (sB >= 0.0);
+        // ---- reverse: the upwind side's flux
+        const double* Us = left ? UA : UB;
+        const double r = Us[0], E = Us[D + 1], pp = left ? pA : pB, un = left ? unA : unB, s = left ? sA : sB;
+        double rb = fb[0] * un, unb = fb[0] * r, Eb = fb[D + 1] * un, pb = fb[D + 1] * un, sb = 0.0, Sb = 0.0;
+        double mb[D];
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            unb += fb[c + 1] * Us[c + 1];
+            mb[c] = fb[c + 1] * un;
+            pb += fb[c + 1] * n[c] / MS;
+        }
+        unb += fb[D + 1] * (E + pp);
+        if (star) {
+            const double a = s - un, b = s - S, rr = a / b, t = S - un;
+            double rrb = fb[0] * s * r, tb = 0.0;
+            sb += fb[0] * r * (rr - 1.0);
+            rb += fb[0] * s * (rr - 1.0);
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                const double w = fb[c + 1], ib = w * s;
+                sb += w * ((rr - 1.0) * Us[c + 1] + r * rr * t * n[c]);
+                rrb += ib * (Us[c + 1] + r * t * n[c]);
+                mb[c] += ib * (rr - 1.0);
+                rb += ib * rr * t * n[c];
+                tb += ib * r * rr * n[c];
+            }
+            const double factor = r * S * MS + pp / a;
+            const double modE = rr * (E + factor * t);
+            sb += fb[D + 1] * (modE - E);
+            const double mEb = fb[D + 1] * s;
+            Eb += mEb * rr - fb[D + 1] * s;
+            rrb += mEb * (E + factor * t);
+            const double fab = mEb * rr * t;
+            tb += mEb * rr * factor;
+            rb += fab * S * MS;
+            Sb += fab * r * MS;
+            pb += fab / a;
+            double ab = -fab * pp / (a * a) + rrb / b;
+            const double bb = -rrb * rr / b;
+            sb += ab + bb;
+            unb -= ab + tb;
+            Sb += tb - bb;
+        }
+        double rAb = 0.0, rBb = 0.0, EAb = 0.0, EBb = 0.0, pAb = 0.0, pBb = 0.0, unAb = 0.0, unBb = 0.0;
+        double sAb = 0.0, sBb = 0.0, mAb[D], mBb[D];
+#pragma unroll
+        for (int c = 0; c < D; ++c) mAb[c] = mBb[c] = 0.0;
+        if (left) {
+            rAb = rb; EAb = Eb; pAb = pb; unAb = unb; sAb = sb;
+#pragma unroll
+            for (int c = 0; c < D; ++c) mAb[c] = mb[c];
+        } else {
+            rBb = rb; EBb = Eb; pBb = pb; unBb = unb; sBb = sb;
+#pragma unroll
+            for (int c = 0; c < D; ++c) mBb[c] = mb[c];
+        }
+        // ---- reverse: contact speed S = (CB unB - CA unA + (pA - pB)/MS) / (CB - CA)
+        const double Nb = Sb / Dd, Ddb = -Sb * S / Dd;
+        double CAb = -Ddb - Nb * unA, CBb = Ddb + Nb * unB;
+        unBb += Nb * CB;
+        unAb -= Nb * CA;
+        pAb += Nb / MS;
+        pBb -= Nb / MS;
+        rAb += CAb * (sA - unA);
+        sAb += CAb * rA;
+        unAb -= CAb * rA;
+        rBb += CBb * (sB - unB);
+        sBb += CBb * rB;
+        unBb -= CBb * rB;
+        // wave speeds sA = unA - cA qA, sB = unB + cB qB
+        unAb += sAb;
+        unBb += sBb;
+        double cAb = -sAb * qA, cBb = sBb * qB;
+        const double qAb = -sAb * cA, qBb = sBb * cB;
+        double pSb = 0.0;
+        if (qAact) {
+            const double zb = qAb / (2.0 * qA);
+            pSb += zb * G2 / pA;
+            pAb -= zb * G2 * pS / (pA * pA);
+        }
+        if (qBact) {
+            const double zb = qBb / (2.0 * qB);
+            pSb += zb * G2 / pB;
+            pBb -= zb * G2 * pS / (pB * pB);
+        }
+        if (!clamp) {
+            const double h = 0.5 * MS;
+            pAb += 0.5 * pSb;
+            pBb += 0.5 * pSb;
+            const double vJb = -pSb * cMean * rhoMean * h;
+            unBb += vJb;
+            unAb -= vJb;
+            const double cMb = -pSb * vJ * rhoMean * h;
+            cAb += 0.5 * cMb;
+            cBb += 0.5 * cMb;
+            const double rMb = -pSb * vJ * cMean * h;
+            rAb += 0.5 * rMb;
+            rBb += 0.5 * rMb;
+        }
+        // ---- reverse: per-side primitives (c = sqrt(p/rho)/Ma, p, un)
+        {
+            const double ybA = cAb / (2.0 * Ma * Ma * cA);
+            pAb += ybA / rA;
+            rAb -= ybA * yA / rA;
+            EAb += pAb * (g - 1.0);
+            const double kbA = -pAb * (g - 1.0) * (MS * 0.5);
+            const double msbA = kbA / rA;
+            rAb -= kbA * kA / rA;
+            const double unrbA = unAb / rA;
+            rAb -= unAb * unA / rA;
+            UAb[0] = rAb;
+#pragma unroll
+            for (int d = 0; d < D; ++d) UAb[d + 1] = mAb[d] + unrbA * n[d] + 2.0 * msbA * UA[d + 1];
+            UAb[D + 1] = EAb;
+        }
+        {
+            const double ybB = cBb / (2.0 * Ma * Ma * cB);
+            pBb += ybB / rB;
+            rBb -= ybB * yB / rB;
+            EBb += pBb * (g - 1.0);
+            const double kbB = -pBb * (g - 1.0) * (MS * 0.5);
+            const double msbB = kbB / rB;
+            rBb -= kbB * kB / rB;
+            const double unrbB = unBb / rB;
+            rBb -= unBb * unB / rB;
+            UBb[0] = rBb;
+#pragma unroll
+            for (int d = 0; d < D; ++d) UBb[d + 1] = mBb[d] + unrbB * n[d] + 2.0 * msbB * UB[d + 1];
+            UBb[D + 1] = EBb;
+        }
     }
 };
 

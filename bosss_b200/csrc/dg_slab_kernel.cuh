@@ -149,6 +149,18 @@ __device__ __forceinline__ void volume_point(const PhysParams& ph, const double*
 #pragma unroll
                 for (int d = 0; d < D; ++d) out(e, 1 + d, fG[e][d].d[0] * fac * twoh[d]);
         }
+    } else if constexpr (Phys::ADJOINT) {
+        // reverse mode: gradient of sum fG . grad w with respect to the node state
+        double U[NV], Gw[NC][D], Ub[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) U[i] = in(i, 0);
+#pragma unroll
+        for (int e = 0; e < NC; ++e)
+#pragma unroll
+            for (int d = 0; d < D; ++d) Gw[e][d] = G2 ? in(NV + e, 1 + d) : 0.0;
+        Phys::volume_adj(ph, U, Gw, Ub);
+#pragma unroll
+        for (int i = 0; i < NV; ++i) out(i, 0, Ub[i] * fac);
     } else {
         constexpr int NS = NV * (Phys::GRAD_U ? 1 + D : 1);
         using T = DualN<NS>;
@@ -242,6 +254,25 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
 #pragma unroll
                 for (int d = 0; d < D; ++d)
                     out(e, 1 + d, (selfA ? GAv[e][d].d[0] : GBv[e][d].d[0]) * fac * twoh[d]);
+        }
+    } else if constexpr (Phys::ADJOINT) {
+        // reverse mode: gradient of sum_e f_e (w_IN,e - w_OUT,e) with respect to the own trace
+        // (the adjoint physics has no boundary terms: its grids are periodic)
+        if (inner) {
+            double UA[NV], UB[NV], fb[NC], UAb[NV], UBb[NV];
+#pragma unroll
+            for (int i = 0; i < NV; ++i) {
+                UA[i] = inA(i, 0);
+                UB[i] = inB(i, 0);
+            }
+#pragma unroll
+            for (int e = 0; e < NC; ++e) fb[e] = inA(NV + e, 0) - inB(NV + e, 0);
+            Phys::inner_adj(ph, UA, UB, nrm, fb, UAb, UBb);
+#pragma unroll
+            for (int i = 0; i < NV; ++i) out(i, 0, (selfA ? UAb[i] : UBb[i]) * fac);
+        } else {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) out(i, 0, 0.0);
         }
     } else {
         constexpr int NS = NV * (Phys::GRAD_U ? 1 + D : 1);
