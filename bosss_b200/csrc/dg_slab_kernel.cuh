@@ -47,7 +47,10 @@ struct SlabCfg {
     // faces: part s handles the lower (s=0) / upper (s=1) face. Measured on B200 (Euler
     // k=3): the split pays for the register-heavy VJP (more resident warps), not for the
     // residual/JVP
-    static constexpr int SPLIT = (MODE == MODE_VJP && Q >= 3) ? 2 : 1;
+#ifndef BOSSS_SLAB_SPLIT_VJP
+#define BOSSS_SLAB_SPLIT_VJP 2
+#endif
+    static constexpr int SPLIT = (MODE == MODE_VJP && Q >= 3) ? BOSSS_SLAB_SPLIT_VJP : 1;
     static constexpr int TPC = NO * Q * SPLIT;     // threads per cell
     static constexpr int NODEV = (NV * NCI0 + NF1 * NCI1V) * FV;   // interpolated node values
     static constexpr int S_CIN = NFI * NP;
@@ -71,11 +74,15 @@ struct SlabCfg {
 #ifndef BOSSS_SLAB_MINB
 #define BOSSS_SLAB_MINB 2
 #endif
-#ifndef BOSSS_SLAB_MINB_VJP
-#define BOSSS_SLAB_MINB_VJP 2
+    // VJP: resident blocks per SM by degree, measured on B200 (Euler, 32^3, k = 1..4): more
+    // resident warps beat the register spills this forces (k=3: 8 -> 16 warps, 1.27 -> 0.82 ms)
+#ifdef BOSSS_SLAB_MINB_VJP
+    static constexpr int MINB_VJP = BOSSS_SLAB_MINB_VJP;
+#else
+    static constexpr int MINB_VJP = K <= 1 ? 5 : (K <= 3 ? 4 : 3);
 #endif
     static constexpr int CPB_THR = ((MODE == MODE_VJP) ? BOSSS_SLAB_THREADS_VJP : BOSSS_SLAB_THREADS) / TPC;
-    static constexpr int MINB = (MODE == MODE_VJP) ? BOSSS_SLAB_MINB_VJP : BOSSS_SLAB_MINB;
+    static constexpr int MINB = (MODE == MODE_VJP) ? MINB_VJP : BOSSS_SLAB_MINB;
     static constexpr int CPB_MAX = (CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR) < 1 ? 1
                                    : (CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR);
     static constexpr int CPB = CPB_MAX;
