@@ -54,7 +54,10 @@ struct SlabCfg {
     static constexpr int TPC = NO * Q * SPLIT;     // threads per cell
     static constexpr int NODEV = (NV * NCI0 + NF1 * NCI1V) * FV;   // interpolated node values
     static constexpr int S_CIN = NFI * NP;
-    static constexpr int S_VOL = NODEV + NO * NCOV * FV;
+    // the pointwise outputs overwrite the node values in place: every node is read and
+    // written by one thread (all its inputs before any output), and output comp c of field o
+    // sits at block c*NO + o, so no node's inputs are overwritten by another node's outputs
+    static constexpr int S_VOL = NODEV > NO * NCOV * FV ? NODEV : NO * NCOV * FV;
     static constexpr int TRB = (NV * NCI0 + NF1 * NCI1F) * FF;      // one (face, side) trace block
     static constexpr int S_FACE = 2 * 2 * TRB + 2 * NO * NCOF * FF;
     static constexpr int S_RED = NO * SPLIT * Q * NP;
@@ -71,8 +74,11 @@ struct SlabCfg {
 #ifndef BOSSS_SLAB_THREADS_VJP
 #define BOSSS_SLAB_THREADS_VJP 128
 #endif
-#ifndef BOSSS_SLAB_MINB
-#define BOSSS_SLAB_MINB 2
+    // residual / JVP: resident blocks per SM (residual k <= 2: 3, measured as for the VJP)
+#ifdef BOSSS_SLAB_MINB
+    static constexpr int MINB_FWD = BOSSS_SLAB_MINB;
+#else
+    static constexpr int MINB_FWD = (MODE == MODE_RES && K <= 2) ? 3 : 2;
 #endif
     // VJP: resident blocks per SM by degree, measured on B200 (Euler, 32^3, k = 1..4): more
     // resident warps beat the register spills this forces (k=3: 8 -> 16 warps, 1.27 -> 0.82 ms)
@@ -82,7 +88,7 @@ struct SlabCfg {
     static constexpr int MINB_VJP = K <= 1 ? 5 : (K <= 3 ? 4 : 3);
 #endif
     static constexpr int CPB_THR = ((MODE == MODE_VJP) ? BOSSS_SLAB_THREADS_VJP : BOSSS_SLAB_THREADS) / TPC;
-    static constexpr int MINB = (MODE == MODE_VJP) ? MINB_VJP : BOSSS_SLAB_MINB;
+    static constexpr int MINB = (MODE == MODE_VJP) ? MINB_VJP : MINB_FWD;
     static constexpr int CPB_MAX = (CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR) < 1 ? 1
                                    : (CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR);
     static constexpr int CPB = CPB_MAX;
@@ -390,8 +396,8 @@ __device__ __forceinline__ void slab_interp(const Tables1D& T, const double* cf,
     }
 }
 
-// projection of the slab qz = q of one output field (block `ob`, comps) into R[NP]
-template <int K, int Q, bool OV, bool OG, int PART, int SPLIT>
+// projection of the slab qz = q of one output field (block `ob`, comps CS doubles apart) into R[NP]
+template <int K, int Q, bool OV, bool OG, int PART, int SPLIT, int CS>
 __device__ __forceinline__ void slab_project(const Tables1D& T, const double* ob, const double* Az, const double* dAz,
                                              int q, double* R) {
     constexpr int NPAIR = (K + 1) * (K + 2) / 2;
@@ -410,9 +416,9 @@ __device__ __forceinline__ void slab_project(const Tables1D& T, const double* ob
         for (int qx = 0; qx < Q; ++qx) {
             const int n = qy * Q + qx;
             const double s = OV ? base[n] : 0.0;
-            const double gx = OG ? base[G0 * FV + n] : 0.0;
-            const double gy = OG ? base[(G0 + 1) * FV + n] : 0.0;
-            const double gz = OG ? base[(G0 + 2) * FV + n] : 0.0;
+            const double gx = OG ? base[G0 * CS + n] : 0.0;
+            const double gy = OG ? base[(G0 + 1) * CS + n] : 0.0;
+            const double gz = OG ? base[(G0 + 2) * CS + n] : 0.0;
 #pragma unroll
             for (int a = 0; a <= K; ++a) {
                 P[a] += s * T.A[qx][a] + gx * T.dA[qx][a];
@@ -611,7 +617,7 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
     __syncthreads();
 
     // ---------------------------------------------------------- volume
-    constexpr int OUT0 = C::NODEV;
+    constexpr int OUT0 = 0;
     if (active) {
         if (part == 0) slab_volume_interp<Phys, K, Q, MODE, 0>(args, CIN(cl), WK(cl), o, q, Aq, dAq);
         else if constexpr (SPLIT > 1) slab_volume_interp<Phys, K, Q, MODE, 1>(args, CIN(cl), WK(cl), o, q, Aq, dAq);
@@ -637,14 +643,15 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
             args.ph, x, fac, g.twoh, [&](int f, int comp) { return nb[C::vnode(f) + comp * FV + off]; },
             [&](int oo, int comp, double v) {
                 const int cc = C::VOL_OV ? comp : comp - 1;
-                ob[(oo * C::NCOV + cc) * FV + off] = v;
+                ob[(cc * NO + oo) * FV + off] = v;
             });
     }
     __syncthreads();
     if (active) {
-        const double* ob = WK(cl) + OUT0 + o * C::NCOV * FV;
-        if (part == 0) slab_project<K, Q, C::VOL_OV, C::VOL_OG, 0, SPLIT>(T, ob, Aq, dAq, q, R);
-        else if constexpr (SPLIT > 1) slab_project<K, Q, C::VOL_OV, C::VOL_OG, 1, SPLIT>(T, ob, Aq, dAq, q, R);
+        const double* ob = WK(cl) + OUT0 + o * FV;
+        if (part == 0) slab_project<K, Q, C::VOL_OV, C::VOL_OG, 0, SPLIT, NO * FV>(T, ob, Aq, dAq, q, R);
+        else if constexpr (SPLIT > 1)
+            slab_project<K, Q, C::VOL_OV, C::VOL_OG, 1, SPLIT, NO * FV>(T, ob, Aq, dAq, q, R);
     }
     __syncthreads();
 
