@@ -357,9 +357,21 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     PhysParams ph;
     int rc = classify(*op, D, phys, ph);
     if (rc) return rc;
+    // part of a partitioned grid: global extent, offset and periodicity per direction
+    bool part = false;
+    for (int d = 0; d < D; ++d) part = part || grid->global_n[d] != 0;
+    int gper[3] = {0, 0, 0};
+    for (int d = 0; d < D; ++d) {
+        gper[d] = part ? (grid->global_periodic[d] ? 1 : 0) : (grid->periodic[d] ? 1 : 0);
+        if (part) {
+            if (grid->global_n[d] < grid->n[d]) return fail(BOSSS_ERR_BAD_ARG, "part larger than the global grid");
+            if (grid->periodic[d] && (!gper[d] || grid->n[d] != grid->global_n[d]))
+                return fail(BOSSS_ERR_BAD_ARG, "a part is periodic only in directions it spans completely");
+        }
+    }
     if (phys == PHYS_EULER)
         for (int d = 0; d < D; ++d)
-            if (!grid->periodic[d])
+            if (!gper[d])
                 return fail(BOSSS_ERR_BAD_ARG, "HLLC fluxes need a boundary-condition map: only periodic grids");
     if (phys == PHYS_SIP && ph.has_sip && K < 1)
         return fail(BOSSS_ERR_BAD_ARG, "SIP needs DG degree >= 1 (IsValidDomainDegreeCombination)");
@@ -368,6 +380,8 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     const int Q = std::max(1, (order + 2) / 2);   // smallest Gauss rule with 2Q-1 >= order
     ensure_registered();
     auto& reg = kernel_registry();
+    if (opt && opt->precision != BOSSS_PRECISION_FP64)
+        return fail(BOSSS_ERR_BAD_ARG, "only BOSSS_PRECISION_FP64 is built (no split-FP32 contractions)");
     const int want = opt ? opt->kernel : 0;
     if (want < 0 || want > 2) return fail(BOSSS_ERR_BAD_ARG, "bad kernel selector");
     int variant = VARIANT_GENERIC;
@@ -407,7 +421,12 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
         g.lo[d] = d < D ? grid->lo[d] : 0.0;
         g.h[d] = d < D ? (grid->hi[d] - grid->lo[d]) / grid->n[d] : 1.0;
         g.twoh[d] = 2.0 / g.h[d];
+        g.gn[d] = (part && d < D) ? grid->global_n[d] : g.n[d];
+        g.goff[d] = (part && d < D) ? grid->global_offset[d] : 0;
+        g.gper[d] = d < D ? gper[d] : 0;
     }
+    h->base.cbeg = 0;
+    h->base.cend = J;
     if (grid->cell_order == BOSSS_CELLS_GLOBALID) {
         g.stride[0] = 1;
         g.stride[1] = g.n[0];
@@ -482,6 +501,30 @@ int bosss_b200_evaluate_device(bosss_handle* h, double alpha, double beta, const
     int rc = run_mode(h, MODE_RES, alpha, beta, U_dev, nullptr, out_dev, time, s);
     if (rc) return rc;
     return check_nan(h, out_dev, h->ncod, s);
+}
+
+int bosss_b200_apply_device(bosss_handle* h, int32_t mode, double alpha, double beta, const double* U_dev,
+                            const double* V_dev, double* out_dev, double time, int64_t cell_begin, int64_t cell_end,
+                            void* stream) {
+    if (!h || !U_dev || !out_dev) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    if (mode < MODE_RES || mode > MODE_VJP) return fail(BOSSS_ERR_BAD_ARG, "bad mode");
+    if (mode != MODE_RES && !V_dev) return fail(BOSSS_ERR_BAD_ARG, "JVP / VJP need the second vector");
+    if (cell_begin < 0 || cell_end < cell_begin || cell_end > h->base.g.J)
+        return fail(BOSSS_ERR_BAD_ARG, "cell range outside the grid");
+    if (cell_end == cell_begin) return BOSSS_OK;
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    EvalArgs a = h->base;
+    a.U = U_dev;
+    a.V = V_dev;
+    a.out = out_dev;
+    a.alpha = alpha;
+    a.beta = beta;
+    a.time = time;
+    a.cbeg = cell_begin;
+    a.cend = cell_end;
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(h->kern[mode].launch(a, s));
+    return BOSSS_OK;
 }
 
 int bosss_b200_evaluate(bosss_handle* h, double alpha, double beta, const double* U, double* out, double time) {

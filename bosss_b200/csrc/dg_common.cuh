@@ -34,6 +34,9 @@ struct GridConst {
     double scaling;          // 1/sqrt(detJ)   (BasisData.cs:47-51)
     double detJ;             // prod h_d/2
     double faceSG[3];        // SqrtGramian of a face normal to d: prod_{d'!=d} h_d'/2
+    // global grid of which this grid is a part (partitioned evaluation); equal to n, 0 and
+    // periodic for a whole grid. Only the SIP cell length scale reads them.
+    int gn[3], goff[3], gper[3];
 };
 
 __host__ __device__ constexpr int np_of(int D, int k) {

@@ -21,7 +21,8 @@ cudaError_t launch_cell_kernel(const EvalArgs& a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         attr_done |= (1ull << (dev & 63));
     }
-    const long long blocks = ((long long)a.g.J + C::CPB - 1) / C::CPB;
+    const long long blocks = (a.cend - a.cbeg + C::CPB - 1) / C::CPB;
+    if (blocks <= 0) return cudaSuccess;
     dg_cell_kernel<Phys, K, Q, MODE><<<(unsigned)blocks, C::NT, C::SMEM_BYTES, s>>>(a);
     return cudaGetLastError();
 }
@@ -52,7 +53,8 @@ cudaError_t launch_slab_kernel(const EvalArgs& a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         attr_done |= (1ull << (dev & 63));
     }
-    const long long blocks = ((long long)a.g.J + C::CPB - 1) / C::CPB;
+    const long long blocks = (a.cend - a.cbeg + C::CPB - 1) / C::CPB;
+    if (blocks <= 0) return cudaSuccess;
     dg_slab_kernel<Phys, K, Q, MODE><<<(unsigned)blocks, C::NT, C::SMEM_BYTES, s>>>(a);
     return cudaGetLastError();
 }

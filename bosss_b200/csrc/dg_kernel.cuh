@@ -48,6 +48,8 @@ struct EvalArgs {
     // cut-cell rule by the explicit-rule kernel).
     const unsigned char* vol_flag;
     const unsigned char* face_flag;
+    // the launch evaluates the cells [cbeg, cend) (the whole grid: 0, J)
+    long long cbeg, cend;
 };
 
 template <class Phys, int K, int Q, int MODE>
@@ -123,8 +125,12 @@ __device__ __forceinline__ double cell_cj(const GridConst& g, const int* ijk) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         if (d >= g.D) break;
+        // boundary faces of the global grid count twice (GridData_CellData.cs:663-684)
         int nb = 0;
-        if (!g.periodic[d]) nb = (ijk[d] == 0) + (ijk[d] == g.n[d] - 1);
+        if (!g.gper[d]) {
+            const int gi = ijk[d] + g.goff[d];
+            nb = (gi == 0) + (gi == g.gn[d] - 1);
+        }
         cj += (2.0 + nb) / g.h[d];
     }
     return 0.5 * cj;
@@ -143,7 +149,7 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
 
     const GridConst& g = args.g;
     const int tid = threadIdx.x;
-    const int ncell = (int)((g.J - c0) < CPB ? (g.J - c0) : CPB);
+    const int ncell = (int)((args.cend - c0) < CPB ? (args.cend - c0) : CPB);
 
     // ---- carve shared memory
     Tables1D* tab = reinterpret_cast<Tables1D*>(smem);
@@ -891,7 +897,7 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
 template <class Phys, int K, int Q, int MODE>
 __global__ void __launch_bounds__(256) dg_cell_kernel(const __grid_constant__ EvalArgs args) {
     extern __shared__ double smem[];
-    cell_tile<Phys, K, Q, MODE>(args, (long long)blockIdx.x * Cfg<Phys, K, Q, MODE>::CPB, smem);
+    cell_tile<Phys, K, Q, MODE>(args, args.cbeg + (long long)blockIdx.x * Cfg<Phys, K, Q, MODE>::CPB, smem);
 }
 
 }  // namespace bosss

@@ -588,8 +588,8 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
     const GridConst& g = args.g;
     const Tables1D& T = args.tab;
     const int tid = threadIdx.x;
-    const long long c0 = (long long)blockIdx.x * CPB;
-    const int ncell = (int)((g.J - c0) < CPB ? (g.J - c0) : CPB);
+    const long long c0 = args.cbeg + (long long)blockIdx.x * CPB;
+    const int ncell = (int)((args.cend - c0) < CPB ? (args.cend - c0) : CPB);
     // own (part, cell, output field, slab); part is warp-uniform (parts padded to warps)
     const int part = tid / C::HALFP, r0 = tid % C::HALFP;
     const int q = r0 % Q, o = (r0 / Q) % NO, cl = (r0 < C::HALF) ? r0 / (Q * NO) : CPB;

@@ -124,11 +124,20 @@ typedef struct bosss_grid_desc {
     double hi[3];          /* domain upper corner */
     int32_t periodic[3];   /* 1 = periodic in that direction */
     int32_t cell_order;    /* enum bosss_cell_order */
+    /* Part of a partitioned grid (domain decomposition, Transceiver.cs): this grid is the
+     * cells [global_offset, global_offset + n) of a global grid with global_n cells and
+     * periodicity global_periodic per direction (the offset may be negative, or reach past
+     * global_n, where a ghost layer wraps around a periodic direction). Only the cell
+     * length scale of the SIP penalty (GridData_CellData.cs:663-684) reads these: it counts
+     * the global boundary, not the edge of the part. All zero: the grid is the whole grid. */
+    int32_t global_n[3];
+    int32_t global_offset[3];
+    int32_t global_periodic[3];
 } bosss_grid_desc;
 
 enum bosss_precision {
-    BOSSS_PRECISION_FP64 = 0,        /* plain FP64 path */
-    BOSSS_PRECISION_SPLIT_FP32 = 1   /* split-FP32 basis contractions, FP64 pointwise physics */
+    BOSSS_PRECISION_FP64 = 0,        /* plain FP64 path (the only one built) */
+    BOSSS_PRECISION_SPLIT_FP32 = 1   /* reserved: split-FP32 basis contractions; create() rejects it */
 };
 
 typedef struct bosss_options {
@@ -345,6 +354,17 @@ int bosss_b200_rk_steps_device(bosss_handle* h, int32_t stages, const double* a,
 /* Same with a host state vector U (copied in, stepped with a captured graph, copied back). */
 int bosss_b200_rk_steps(bosss_handle* h, int32_t stages, const double* a, const double* b, const double* c, double dt,
                         int32_t nsteps, double time, double* U);
+
+/* Residual (mode 0), JVP (1) or VJP (2) on the cells [cell_begin, cell_end) of the handle's
+ * grid only, device buffers, enqueued on `stream` (NULL: the handle's stream): the cells'
+ * outputs are written (out = beta*out + alpha*result), nothing else is. U and V hold the whole
+ * grid, so the cells' face neighbours are read. This is the building block of partitioned
+ * evaluation with ghost layers: the interior of a part is evaluated while the halo exchange
+ * of its ghost cells is in flight, the cells next to the ghosts afterwards
+ * (EvaluatorNonLin.Evaluate with MPI, DifferentialOperator.cs:1599-1627). */
+int bosss_b200_apply_device(bosss_handle* h, int32_t mode, double alpha, double beta, const double* U_dev,
+                            const double* V_dev, double* out_dev, double time, int64_t cell_begin,
+                            int64_t cell_end, void* stream);
 
 /* Batched evaluation that allocates no device memory (no counterpart in the reference).
  * For callers that cannot call cudaMalloc: hosts whose device memory belongs to another

@@ -323,6 +323,12 @@ static int neighbour(const Problem& P, int j, int d, int side) {
     return cell_index(P, ijk);
 }
 
+static int cell_index_along(const Problem& P, int j, int d) {
+    int ijk[3];
+    cell_ijk(P, j, ijk);
+    return ijk[d];
+}
+
 static void cell_center(const Problem& P, int j, double* c) {
     int ijk[3];
     cell_ijk(P, j, ijk);
@@ -418,6 +424,8 @@ static std::string setup(Problem& P, const bosss_op_desc* op, const bosss_grid_d
         P.fdphi.push_back(dphi);
     }
     // cj = (CellSurfaceArea + bndArea) * 0.5 / volume   (GridData_CellData.cs:663-684)
+    bool part = false;
+    for (int d = 0; d < P.D; ++d) part = part || g->global_n[d] != 0;
     P.cj.assign(P.J, 0.0);
     double vol = 1;
     for (int d = 0; d < P.D; ++d) vol *= P.h[d];
@@ -429,7 +437,13 @@ static std::string setup(Problem& P, const bosss_op_desc* op, const bosss_grid_d
                 if (d2 != d) area *= P.h[d2];
             for (int s = 0; s < 2; ++s) {
                 surf += area;
-                if (neighbour(P, j, d, s) < 0) bnd += area;
+                bool boundary = neighbour(P, j, d, s) < 0;
+                if (part) {
+                    // part of a partitioned grid: only the global boundary counts
+                    const int gi = cell_index_along(P, j, d) + g->global_offset[d];
+                    boundary = !g->global_periodic[d] && (s == 0 ? gi == 0 : gi == g->global_n[d] - 1);
+                }
+                if (boundary) bnd += area;
             }
         }
         P.cj[j] = (surf + bnd) * 0.5 / vol;
@@ -451,7 +465,7 @@ static std::string setup(Problem& P, const bosss_op_desc* op, const bosss_grid_d
             case BOSSS_COMP_HLLC_ENERGY_FLUX:
                 if (cp.n_args != P.D + 2) return "HLLC needs D+2 arguments";
                 for (int d = 0; d < P.D; ++d)
-                    if (!g->periodic[d]) return "HLLC: only periodic grids";
+                    if (!(part ? g->global_periodic[d] : g->periodic[d])) return "HLLC: only periodic grids";
                 break;
             default: return "unsupported component";
         }
