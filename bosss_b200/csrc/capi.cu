@@ -419,7 +419,8 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
         g.n[d] = d < D ? grid->n[d] : 1;
         g.periodic[d] = d < D ? (grid->periodic[d] ? 1 : 0) : 0;
         g.lo[d] = d < D ? grid->lo[d] : 0.0;
-        g.h[d] = d < D ? (grid->hi[d] - grid->lo[d]) / grid->n[d] : 1.0;
+        // a part's box is the global box: the cell width is the global one
+        g.h[d] = d < D ? (grid->hi[d] - grid->lo[d]) / (part ? grid->global_n[d] : grid->n[d]) : 1.0;
         g.twoh[d] = 2.0 / g.h[d];
         g.gn[d] = (part && d < D) ? grid->global_n[d] : g.n[d];
         g.goff[d] = (part && d < D) ? grid->global_offset[d] : 0;

@@ -326,7 +326,7 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
 #pragma unroll
             for (int d = 0; d < D; ++d) {
                 W *= tab->w[qi[d]];
-                x[d] = g.lo[d] + (ijk[d] + 0.5 + 0.5 * tab->xq[qi[d]]) * g.h[d];
+                x[d] = g.lo[d] + (ijk[d] + g.goff[d] + 0.5 + 0.5 * tab->xq[qi[d]]) * g.h[d];
             }
             const double* nv = NVAL(cl);
             double* no = NOUT(cl);
@@ -668,7 +668,7 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
             const double fac = Wf * g.faceSG[d] * scaling;
             double x[3] = {0, 0, 0};
 #pragma unroll
-            for (int dd = 0; dd < D; ++dd) x[dd] = g.lo[dd] + (ijk[dd] + 0.5) * g.h[dd];
+            for (int dd = 0; dd < D; ++dd) x[dd] = g.lo[dd] + (ijk[dd] + g.goff[dd] + 0.5) * g.h[dd];
             x[d] += (s ? 0.5 : -0.5) * g.h[d];
             x[t1] += 0.5 * g.h[t1] * tab->xq[q1];
             if (D == 3) x[t2] += 0.5 * g.h[t2] * tab->xq[q2];

@@ -632,7 +632,7 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
         cell_ijk(g, c0 + c, cijk);
         double x[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) x[d] = g.lo[d] + (cijk[d] + 0.5) * g.h[d];
+        for (int d = 0; d < 3; ++d) x[d] = g.lo[d] + (cijk[d] + g.goff[d] + 0.5) * g.h[d];
         x[0] += 0.5 * g.h[0] * T.xq[qx];
         x[1] += 0.5 * g.h[1] * T.xq[qy];
         x[2] += 0.5 * g.h[2] * T.xq[qz];
@@ -681,7 +681,7 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
             const bool inner = nbc >= 0;
             double x[3];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) x[d] = g.lo[d] + (cijk[d] + 0.5) * g.h[d];
+            for (int d = 0; d < 3; ++d) x[d] = g.lo[d] + (cijk[d] + g.goff[d] + 0.5) * g.h[d];
             x[DIR] += (s ? 0.5 : -0.5) * g.h[DIR];
             x[t1] += 0.5 * g.h[t1] * T.xq[q1];
             x[t2] += 0.5 * g.h[t2] * T.xq[q2];

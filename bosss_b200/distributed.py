@@ -63,7 +63,6 @@ class SlabPartition:
     def grid_desc(self):
         """``bosss_grid_desc`` of the part: owned planes plus ghost planes."""
         g = self.grid
-        h0 = (g.hi[0] - g.lo[0]) / g.n[0]
         x0 = self.first - self.ghost_lo
         d = C.GridDesc()
         d.dim = g.dim
@@ -74,9 +73,8 @@ class SlabPartition:
             d.periodic[k] = int(g.periodic[k]) if k < g.dim else 0
         d.cell_order = C.CELLS_GENERATOR
         if self.nranks > 1:
+            # lo/hi stay the global box: the library derives the global cell width from it
             d.n[0] = self.n_planes
-            d.lo[0] = g.lo[0] + x0 * h0
-            d.hi[0] = g.lo[0] + (x0 + self.n_planes) * h0
             d.periodic[0] = 0
             for k in range(g.dim):
                 d.global_n[k] = g.n[k]

@@ -127,9 +127,11 @@ typedef struct bosss_grid_desc {
     /* Part of a partitioned grid (domain decomposition, Transceiver.cs): this grid is the
      * cells [global_offset, global_offset + n) of a global grid with global_n cells and
      * periodicity global_periodic per direction (the offset may be negative, or reach past
-     * global_n, where a ghost layer wraps around a periodic direction). Only the cell
-     * length scale of the SIP penalty (GridData_CellData.cs:663-684) reads these: it counts
-     * the global boundary, not the edge of the part. All zero: the grid is the whole grid. */
+     * global_n, where a ghost layer wraps around a periodic direction). For a part, lo and hi
+     * are the box of the GLOBAL grid: cell widths and node coordinates are computed exactly
+     * as on the whole grid, so a part's results equal the whole grid's bit for bit. The SIP
+     * penalty's cell length scale (GridData_CellData.cs:663-684) counts the global boundary,
+     * not the edge of the part. All zero: the grid is the whole grid. */
     int32_t global_n[3];
     int32_t global_offset[3];
     int32_t global_periodic[3];

@@ -332,7 +332,7 @@ static int cell_index_along(const Problem& P, int j, int d) {
 static void cell_center(const Problem& P, int j, double* c) {
     int ijk[3];
     cell_ijk(P, j, ijk);
-    for (int d = 0; d < P.D; ++d) c[d] = P.g.lo[d] + (ijk[d] + 0.5) * P.h[d];
+    for (int d = 0; d < P.D; ++d) c[d] = P.g.lo[d] + (ijk[d] + P.g.global_offset[d] + 0.5) * P.h[d];
 }
 
 static std::string setup(Problem& P, const bosss_op_desc* op, const bosss_grid_desc* g) {
@@ -344,7 +344,8 @@ static std::string setup(Problem& P, const bosss_op_desc* op, const bosss_grid_d
     for (int d = 0; d < P.D; ++d) {
         if (g->n[d] < 1) return "bad n";
         P.J *= g->n[d];
-        P.h[d] = (g->hi[d] - g->lo[d]) / g->n[d];
+        // a part's box is the global box (bosss_grid_desc): the cell width is the global one
+        P.h[d] = (g->hi[d] - g->lo[d]) / (g->global_n[d] ? g->global_n[d] : g->n[d]);
     }
     P.detJ = 1;
     for (int d = 0; d < P.D; ++d) P.detJ *= 0.5 * P.h[d];
