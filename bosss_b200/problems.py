@@ -116,9 +116,12 @@ def project_nodal(dim, k, nq, h, nodal):
     return (nodal * W[None, :]) @ phi * (detJ * scaling)
 
 
-def euler3d(n=32, k=3, seed=2000, gamma=1.4, quad_order=None):
+def euler3d(n=32, k=3, seed=2000, gamma=1.4, quad_order=None, nx=None):
+    """``nx``: cells along x (default n) on [0, nx/n] -- the same cell size, an elongated
+    periodic box (the global grid of an x-slab partition with n planes per part)."""
     quad_order = 2 * k + 1 if quad_order is None else quad_order
-    g = O.Cartesian3DGrid(_linspace_nodes(n), _linspace_nodes(n), _linspace_nodes(n), True, True, True)
+    nx = n if nx is None else nx
+    g = O.Cartesian3DGrid(np.linspace(0.0, nx / n, nx + 1), _linspace_nodes(n), _linspace_nodes(n), True, True, True)
     names = ["rho", "m0", "m1", "m2", "rhoE"]
     op = O.DifferentialOperator(names, [], ["R_" + s for s in names], O.QuadOrderFunc.FixedOrder(quad_order))
     mat = O.Material(gamma)
@@ -145,7 +148,8 @@ def euler3d(n=32, k=3, seed=2000, gamma=1.4, quad_order=None):
     for f, val in enumerate(fields):
         U[:, f * Np:(f + 1) * Np] = project_nodal(3, k, nq, h, val)
     return Problem("euler3d", op, g, dom, cod, U.ravel(),
-                   {"workload": "euler3d_hllc_%d^3_k%d" % (n, k), "cells": J, "k": k, "seed": seed,
+                   {"workload": ("euler3d_hllc_%d^3_k%d" % (n, k)) if nx == n else
+                    ("euler3d_hllc_%dx%d^2_k%d" % (nx, n, k)), "cells": J, "k": k, "seed": seed,
                     "gamma": gamma, "quad_order": quad_order})
 
 
