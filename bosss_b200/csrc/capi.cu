@@ -201,6 +201,8 @@ static int classify(const bosss_op_desc& op, int D, int& phys, PhysParams& ph) {
         if (!(gamma > 1.0) || !(mach > 0.0)) return fail(BOSSS_ERR_BAD_ARG, "bad gamma/Mach");
         ph.gamma = gamma;
         ph.mach = mach;
+        ph.ims = 1.0 / (gamma * mach * mach);
+        ph.imach = 1.0 / mach;
         phys = PHYS_EULER;
         return 0;
     }

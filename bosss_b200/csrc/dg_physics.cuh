@@ -28,6 +28,7 @@ struct PhysParams {
     int has_source;
     double src;           // constant source value
     double gamma, mach;   // HLLC
+    double ims, imach;    // HLLC: 1/(gamma Ma^2), 1/Ma
 };
 
 template <class T> __host__ __device__ __forceinline__ T tconst(double a) { return T(a); }
@@ -145,44 +146,52 @@ struct PhysEuler {
     static constexpr bool FACE_V = true;
     static constexpr bool FACE_G = false;
 
+    // FP64 divisions are costly on the GPU (a reciprocal estimate plus Newton steps): every
+    // quotient by a state-dependent value below is a product with one reciprocal, and the
+    // constants 1/(gamma Ma^2), 1/Ma come precomputed in PhysParams (ims, imach)
     template <class T>
     __host__ __device__ static void volume(const PhysParams& p, const T* U, const T (*G)[D], const double* x, T* fV,
-                                  T (*fG)[D]) {
+                                           T (*fG)[D]) {
         (void)G; (void)x; (void)fV;
         const double gMs = p.gamma * p.mach * p.mach;
         T rho = U[0], E = U[D + 1];
-        T msq = U[1] * U[1];
-#pragma unroll
-        for (int d = 1; d < D; ++d) msq += U[d + 1] * U[d + 1];
         T irho = 1.0 / rho;
+        T u[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) u[d] = U[d + 1] * irho;
+        T kin = U[1] * u[0];                  // |m|^2 / rho
+#pragma unroll
+        for (int d = 1; d < D; ++d) kin += U[d + 1] * u[d];
         // density: F_d = m_d
 #pragma unroll
         for (int d = 0; d < D; ++d) fG[0][d] -= U[d + 1];
-        // momentum c: F_d = m_c m_d / rho + delta_cd p/(gamma Ma^2)
-        T pm = (E - msq * irho * (gMs * 0.5)) * ((p.gamma - 1.0) / gMs);
+        // momentum c: F_d = m_c u_d + delta_cd p/(gamma Ma^2)
+        T pm = (E - kin * (gMs * 0.5)) * ((p.gamma - 1.0) * p.ims);
 #pragma unroll
         for (int c = 0; c < D; ++c) {
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                T F = U[c + 1] * U[d + 1] / rho;
+                T F = U[c + 1] * u[d];
                 if (c == d) F += pm;
                 fG[c + 1][d] -= F;
             }
         }
-        // energy: F_d = m_d/rho (E + p)
-        T pe = (E - msq / rho * (gMs * 0.5)) * (p.gamma - 1.0);
+        // energy: F_d = u_d (E + p)
+        T pe = (E - kin * (gMs * 0.5)) * (p.gamma - 1.0);
 #pragma unroll
-        for (int d = 0; d < D; ++d) fG[D + 1][d] -= U[d + 1] / rho * (E + pe);
+        for (int d = 0; d < D; ++d) fG[D + 1][d] -= u[d] * (E + pe);
     }
 
     template <class T>
     __host__ __device__ static void inner(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D], const T* UB,
-                                 const T (*GB)[D], const double* n, const double* x, T* gA, T (*GAv)[D], T* gB,
-                                 T (*GBv)[D]) {
+                                          const T (*GB)[D], const double* n, const double* x, T* gA, T (*GAv)[D],
+                                          T* gB, T (*GBv)[D]) {
         (void)pnlty; (void)GA; (void)GB; (void)x; (void)GAv; (void)GBv;
-        const double gamma = p.gamma, Mach = p.mach;
-        const double MachScaling = gamma * Mach * Mach;
+        const double gamma = p.gamma;
+        const double MachScaling = gamma * p.mach * p.mach, iMS = p.ims;
+        const double G2 = 0.5 * (gamma + 1.0) / gamma;
         T rhoIn = UA[0], rhoOut = UB[0];
+        T irIn = 1.0 / rhoIn, irOut = 1.0 / rhoOut;
         T msIn = UA[1] * UA[1], msOut = UB[1] * UB[1];
         T unIn = UA[1] * n[0], unOut = UB[1] * n[0];
 #pragma unroll
@@ -192,13 +201,13 @@ struct PhysEuler {
             unIn += UA[d + 1] * n[d];
             unOut += UB[d + 1] * n[d];
         }
-        unIn = unIn / rhoIn;
-        unOut = unOut / rhoOut;
+        unIn = unIn * irIn;
+        unOut = unOut * irOut;
         T EIn = UA[D + 1], EOut = UB[D + 1];
-        T pIn = (EIn - msIn / rhoIn * (MachScaling * 0.5)) * (gamma - 1.0);
-        T pOut = (EOut - msOut / rhoOut * (MachScaling * 0.5)) * (gamma - 1.0);
-        T cInS = dsqrt(pIn / rhoIn) / Mach;
-        T cOutS = dsqrt(pOut / rhoOut) / Mach;
+        T pIn = (EIn - msIn * irIn * (MachScaling * 0.5)) * (gamma - 1.0);
+        T pOut = (EOut - msOut * irOut * (MachScaling * 0.5)) * (gamma - 1.0);
+        T cInS = dsqrt(pIn * irIn) * p.imach;
+        T cOutS = dsqrt(pOut * irOut) * p.imach;
         T rhoMean = (rhoIn + rhoOut) * 0.5;
         T pMean = (pIn + pOut) * 0.5;
         T cMean = (cInS + cOutS) * 0.5;
@@ -206,53 +215,40 @@ struct PhysEuler {
         T pStar = pMean - velJump * cMean * rhoMean * (0.5 * MachScaling);
         if (0.0 > pval(pStar)) pStar = T(0.0);           // Math.Max(0.0, pStar)
         T qIn = T(1.0), qOut = T(1.0);
-        if (pval(pStar) > pval(pIn)) qIn = dsqrt(1.0 + (pStar / pIn - 1.0) * (0.5 * (gamma + 1.0) / gamma));
-        if (pval(pStar) > pval(pOut)) qOut = dsqrt(1.0 + (pStar / pOut - 1.0) * (0.5 * (gamma + 1.0) / gamma));
+        if (pval(pStar) > pval(pIn)) qIn = dsqrt(1.0 + (pStar / pIn - 1.0) * G2);
+        if (pval(pStar) > pval(pOut)) qOut = dsqrt(1.0 + (pStar / pOut - 1.0) * G2);
         T sIn = unIn - cInS * qIn;
         T sOut = unOut + cOutS * qOut;
         T cIn = rhoIn * (sIn - unIn);
         T cOut = rhoOut * (sOut - unOut);
         T speedDiff = cOut * unOut - cIn * unIn;
         T dp = pIn - pOut;
-        T sStar = (speedDiff + dp / MachScaling) / (cOut - cIn);
+        T sStar = (speedDiff + dp * iMS) / (cOut - cIn);
 
+        // upwind side of the contact wave
+        const bool left = pval(sStar) > 0.0;
+        const T* Us = left ? UA : UB;
+        const T r = left ? rhoIn : rhoOut, ir = left ? irIn : irOut, E = left ? EIn : EOut;
+        const T pp = left ? pIn : pOut, un = left ? unIn : unOut, s = left ? sIn : sOut;
         T f[D + 2];
-        if (pval(sStar) > 0.0) {
-            f[0] = unIn * rhoIn;
+        f[0] = un * r;
+        const T pms = pp * iMS;
 #pragma unroll
-            for (int c = 0; c < D; ++c) f[c + 1] = unIn * UA[c + 1] + pIn / MachScaling * n[c];
-            f[D + 1] = unIn * (EIn + pIn);
-            if (pval(sIn) <= 0.0) {
-                T ratio = (sIn - unIn) / (sIn - sStar);
-                T modRho = rhoIn * ratio;
-                f[0] += sIn * (modRho - rhoIn);
+        for (int c = 0; c < D; ++c) f[c + 1] = un * Us[c + 1] + pms * n[c];
+        f[D + 1] = un * (E + pp);
+        if (left ? (pval(s) <= 0.0) : (pval(s) >= 0.0)) {
+            T ratio = (s - un) / (s - sStar);
+            T modRho = r * ratio;
+            f[0] += s * (modRho - r);
+            const T t = sStar - un;
 #pragma unroll
-                for (int c = 0; c < D; ++c) {
-                    T modM = rhoIn * ratio * (UA[c + 1] / rhoIn + (sStar - unIn) * n[c]);
-                    f[c + 1] += sIn * (modM - UA[c + 1]);
-                }
-                T factor = rhoIn * sStar * MachScaling + pIn / (sIn - unIn);
-                T modE = ratio * (EIn + factor * (sStar - unIn));
-                f[D + 1] += sIn * (modE - EIn);
+            for (int c = 0; c < D; ++c) {
+                T modM = r * ratio * (Us[c + 1] * ir + t * n[c]);
+                f[c + 1] += s * (modM - Us[c + 1]);
             }
-        } else {
-            f[0] = unOut * rhoOut;
-#pragma unroll
-            for (int c = 0; c < D; ++c) f[c + 1] = unOut * UB[c + 1] + pOut / MachScaling * n[c];
-            f[D + 1] = unOut * (EOut + pOut);
-            if (pval(sOut) >= 0.0) {
-                T ratio = (sOut - unOut) / (sOut - sStar);
-                T modRho = rhoOut * ratio;
-                f[0] += sOut * (modRho - rhoOut);
-#pragma unroll
-                for (int c = 0; c < D; ++c) {
-                    T modM = rhoOut * ratio * (UB[c + 1] / rhoOut + (sStar - unOut) * n[c]);
-                    f[c + 1] += sOut * (modM - UB[c + 1]);
-                }
-                T factor = rhoOut * sStar * MachScaling + pOut / (sOut - unOut);
-                T modE = ratio * (EOut + factor * (sStar - unOut));
-                f[D + 1] += sOut * (modE - EOut);
-            }
+            T factor = r * sStar * MachScaling + pp / (s - un);
+            T modE = ratio * (E + factor * t);
+            f[D + 1] += s * (modE - E);
         }
 #pragma unroll
         for (int c = 0; c < D + 2; ++c) {
@@ -263,7 +259,7 @@ struct PhysEuler {
 
     template <class T>
     __host__ __device__ static void boundary(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
-                                    const double* n, const double* x, T* gA, T (*GAv)[D]) {
+                                             const double* n, const double* x, T* gA, T (*GAv)[D]) {
         // no boundary-condition map on the device: create() rejects non-periodic Euler grids
         (void)p; (void)pnlty; (void)UA; (void)GA; (void)n; (void)x; (void)gA; (void)GAv;
     }
@@ -278,13 +274,13 @@ struct PhysEuler {
                                                double* Ub) {
         const double g = p.gamma, gMs = g * p.mach * p.mach;
         const double rho = U[0], E = U[D + 1], irho = 1.0 / rho;
-        double u[D], msq = 0.0;
+        double u[D], kin = 0.0;
 #pragma unroll
         for (int d = 0; d < D; ++d) {
             u[d] = U[d + 1] * irho;
-            msq += U[d + 1] * U[d + 1];
+            kin += U[d + 1] * u[d];
         }
-        const double pm = (E - msq * irho * (gMs * 0.5)) * ((g - 1.0) / gMs);
+        const double pm = (E - kin * (gMs * 0.5)) * ((g - 1.0) * p.ims);
         const double pe = gMs * pm;
         double A = 0.0, gu = 0.0, uMu = 0.0, usq = 0.0;
         double Mu[D], Mtu[D];
@@ -311,15 +307,16 @@ struct PhysEuler {
         Ub[0] = uMu - 0.5 * gm1 * usq * s + gu * Epe;
 #pragma unroll
         for (int k = 0; k < D; ++k) Ub[k + 1] = -(Gw[0][k] + Mu[k] + Mtu[k] - gm1 * u[k] * s + Gw[D + 1][k] * Epe);
-        Ub[D + 1] = -(A * gm1 / gMs + gu * g);
+        Ub[D + 1] = -(A * gm1 * p.ims + gu * g);
     }
 
     // UAb / UBb = gradient of sum_c f_c(UA, UB) * fb[c] (f: the HLLC flux of inner())
     __host__ __device__ static void inner_adj(const PhysParams& p, const double* UA, const double* UB,
                                               const double* n, const double* fb, double* UAb, double* UBb) {
-        const double g = p.gamma, Ma = p.mach, MS = g * Ma * Ma, G2 = 0.5 * (g + 1.0) / g;
-        // ---- primal
+        const double g = p.gamma, MS = g * p.mach * p.mach, iMS = p.ims, G2 = 0.5 * (g + 1.0) / g;
+        // ---- primal (as inner())
         const double rA = UA[0], rB = UB[0], EA = UA[D + 1], EB = UB[D + 1];
+        const double irA = 1.0 / rA, irB = 1.0 / rB;
         double msA = 0.0, msB = 0.0, unrA = 0.0, unrB = 0.0;
 #pragma unroll
         for (int d = 0; d < D; ++d) {
@@ -328,23 +325,24 @@ struct PhysEuler {
             unrA += UA[d + 1] * n[d];
             unrB += UB[d + 1] * n[d];
         }
-        const double unA = unrA / rA, unB = unrB / rB;
-        const double kA = msA / rA, kB = msB / rB;
+        const double unA = unrA * irA, unB = unrB * irB;
+        const double kA = msA * irA, kB = msB * irB;
         const double pA = (EA - kA * (MS * 0.5)) * (g - 1.0), pB = (EB - kB * (MS * 0.5)) * (g - 1.0);
-        const double yA = pA / rA, yB = pB / rB;
-        const double cA = sqrt(yA) / Ma, cB = sqrt(yB) / Ma;
+        const double yA = pA * irA, yB = pB * irB;
+        const double cA = sqrt(yA) * p.imach, cB = sqrt(yB) * p.imach;
         const double rhoMean = (rA + rB) * 0.5, pMean = (pA + pB) * 0.5, cMean = (cA + cB) * 0.5;
         const double vJ = unB - unA;
         const double pSraw = pMean - vJ * cMean * rhoMean * (0.5 * MS);
         const bool clamp = 0.0 > pSraw;
         const double pS = clamp ? 0.0 : pSraw;
         const bool qAact = pS > pA, qBact = pS > pB;
-        const double qA = qAact ? sqrt(1.0 + (pS / pA - 1.0) * G2) : 1.0;
-        const double qB = qBact ? sqrt(1.0 + (pS / pB - 1.0) * G2) : 1.0;
+        const double ipA = qAact ? 1.0 / pA : 0.0, ipB = qBact ? 1.0 / pB : 0.0;
+        const double qA = qAact ? sqrt(1.0 + (pS * ipA - 1.0) * G2) : 1.0;
+        const double qB = qBact ? sqrt(1.0 + (pS * ipB - 1.0) * G2) : 1.0;
         const double sA = unA - cA * qA, sB = unB + cB * qB;
         const double CA = rA * (sA - unA), CB = rB * (sB - unB);
-        const double Dd = CB - CA;
-        const double S = (CB * unB - CA * unA + (pA - pB) / MS) / Dd;
+        const double Dd = CB - CA, iDd = 1.0 / Dd;
+        const double S = (CB * unB - CA * unA + (pA - pB) * iMS) * iDd;
         const bool left = S > 0.0;
         const bool star = left ? (sA <= 0.0) : (sB >= 0.0);
         // ---- reverse: the upwind side's flux
@@ -356,24 +354,24 @@ struct PhysEuler {
         for (int c = 0; c < D; ++c) {
             unb += fb[c + 1] * Us[c + 1];
             mb[c] = fb[c + 1] * un;
-            pb += fb[c + 1] * n[c] / MS;
+            pb += fb[c + 1] * n[c] * iMS;
         }
         unb += fb[D + 1] * (E + pp);
         if (star) {
-            const double a = s - un, b = s - S, rr = a / b, t = S - un;
+            const double a = s - un, b = s - S, ia = 1.0 / a, ib = 1.0 / b, rr = a * ib, t = S - un;
             double rrb = fb[0] * s * r, tb = 0.0;
             sb += fb[0] * r * (rr - 1.0);
             rb += fb[0] * s * (rr - 1.0);
 #pragma unroll
             for (int c = 0; c < D; ++c) {
-                const double w = fb[c + 1], ib = w * s;
+                const double w = fb[c + 1], wb = w * s;
                 sb += w * ((rr - 1.0) * Us[c + 1] + r * rr * t * n[c]);
-                rrb += ib * (Us[c + 1] + r * t * n[c]);
-                mb[c] += ib * (rr - 1.0);
-                rb += ib * rr * t * n[c];
-                tb += ib * r * rr * n[c];
+                rrb += wb * (Us[c + 1] + r * t * n[c]);
+                mb[c] += wb * (rr - 1.0);
+                rb += wb * rr * t * n[c];
+                tb += wb * r * rr * n[c];
             }
-            const double factor = r * S * MS + pp / a;
+            const double factor = r * S * MS + pp * ia;
             const double modE = rr * (E + factor * t);
             sb += fb[D + 1] * (modE - E);
             const double mEb = fb[D + 1] * s;
@@ -383,9 +381,9 @@ struct PhysEuler {
             tb += mEb * rr * factor;
             rb += fab * S * MS;
             Sb += fab * r * MS;
-            pb += fab / a;
-            double ab = -fab * pp / (a * a) + rrb / b;
-            const double bb = -rrb * rr / b;
+            pb += fab * ia;
+            const double ab = -fab * pp * ia * ia + rrb * ib;
+            const double bb = -rrb * rr * ib;
             sb += ab + bb;
             unb -= ab + tb;
             Sb += tb - bb;
@@ -404,12 +402,12 @@ struct PhysEuler {
             for (int c = 0; c < D; ++c) mBb[c] = mb[c];
         }
         // ---- reverse: contact speed S = (CB unB - CA unA + (pA - pB)/MS) / (CB - CA)
-        const double Nb = Sb / Dd, Ddb = -Sb * S / Dd;
+        const double Nb = Sb * iDd, Ddb = -Sb * S * iDd;
         double CAb = -Ddb - Nb * unA, CBb = Ddb + Nb * unB;
         unBb += Nb * CB;
         unAb -= Nb * CA;
-        pAb += Nb / MS;
-        pBb -= Nb / MS;
+        pAb += Nb * iMS;
+        pBb -= Nb * iMS;
         rAb += CAb * (sA - unA);
         sAb += CAb * rA;
         unAb -= CAb * rA;
@@ -423,14 +421,14 @@ struct PhysEuler {
         const double qAb = -sAb * cA, qBb = sBb * cB;
         double pSb = 0.0;
         if (qAact) {
-            const double zb = qAb / (2.0 * qA);
-            pSb += zb * G2 / pA;
-            pAb -= zb * G2 * pS / (pA * pA);
+            const double zb = qAb * 0.5 / qA;
+            pSb += zb * G2 * ipA;
+            pAb -= zb * G2 * pS * ipA * ipA;
         }
         if (qBact) {
-            const double zb = qBb / (2.0 * qB);
-            pSb += zb * G2 / pB;
-            pBb -= zb * G2 * pS / (pB * pB);
+            const double zb = qBb * 0.5 / qB;
+            pSb += zb * G2 * ipB;
+            pBb -= zb * G2 * pS * ipB * ipB;
         }
         if (!clamp) {
             const double h = 0.5 * MS;
@@ -446,32 +444,33 @@ struct PhysEuler {
             rAb += 0.5 * rMb;
             rBb += 0.5 * rMb;
         }
-        // ---- reverse: per-side primitives (c = sqrt(p/rho)/Ma, p, un)
+        // ---- reverse: per-side primitives (c = sqrt(p/rho)/Ma, p, un); dc/dy = 1/(2 Ma^2 c)
+        const double i2M2 = 0.5 * p.imach * p.imach;
         {
-            const double ybA = cAb / (2.0 * Ma * Ma * cA);
-            pAb += ybA / rA;
-            rAb -= ybA * yA / rA;
+            const double ybA = cAb * i2M2 / cA;
+            pAb += ybA * irA;
+            rAb -= ybA * yA * irA;
             EAb += pAb * (g - 1.0);
             const double kbA = -pAb * (g - 1.0) * (MS * 0.5);
-            const double msbA = kbA / rA;
-            rAb -= kbA * kA / rA;
-            const double unrbA = unAb / rA;
-            rAb -= unAb * unA / rA;
+            const double msbA = kbA * irA;
+            rAb -= kbA * kA * irA;
+            const double unrbA = unAb * irA;
+            rAb -= unAb * unA * irA;
             UAb[0] = rAb;
 #pragma unroll
             for (int d = 0; d < D; ++d) UAb[d + 1] = mAb[d] + unrbA * n[d] + 2.0 * msbA * UA[d + 1];
             UAb[D + 1] = EAb;
         }
         {
-            const double ybB = cBb / (2.0 * Ma * Ma * cB);
-            pBb += ybB / rB;
-            rBb -= ybB * yB / rB;
+            const double ybB = cBb * i2M2 / cB;
+            pBb += ybB * irB;
+            rBb -= ybB * yB * irB;
             EBb += pBb * (g - 1.0);
             const double kbB = -pBb * (g - 1.0) * (MS * 0.5);
-            const double msbB = kbB / rB;
-            rBb -= kbB * kB / rB;
-            const double unrbB = unBb / rB;
-            rBb -= unBb * unB / rB;
+            const double msbB = kbB * irB;
+            rBb -= kbB * kB * irB;
+            const double unrbB = unBb * irB;
+            rBb -= unBb * unB * irB;
             UBb[0] = rBb;
 #pragma unroll
             for (int d = 0; d < D; ++d) UBb[d + 1] = mBb[d] + unrbB * n[d] + 2.0 * msbB * UB[d + 1];

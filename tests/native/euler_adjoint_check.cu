@@ -31,6 +31,8 @@ int main() {
     PhysParams ph{};
     ph.gamma = 1.4;
     ph.mach = 1.0 / std::sqrt(1.4);
+    ph.ims = 1.0 / (ph.gamma * ph.mach * ph.mach);
+    ph.imach = 1.0 / ph.mach;
     std::mt19937_64 g(1234);
     std::uniform_real_distribution<double> u(-1.0, 1.0);
     double worst = 0.0;
