@@ -34,6 +34,7 @@ static void ensure_registered() {
     std::call_once(once, [] {
         register_scalar2();
         register_scalar3();
+        register_scalar3_slab();
         register_euler2();
         register_euler3();
     });
@@ -269,6 +270,8 @@ int run_mode(bosss_handle* h, int mode, double alpha, double beta, const double*
     a.beta = beta;
     a.time = time;
     CUDA_TRY(cudaSetDevice(h->device));
+    if ((a.vol_flag || a.face_flag) && h->variant != VARIANT_GENERIC)
+        return fail(BOSSS_ERR_BAD_ARG, "species masks need the generic kernel");
     if (h->base.g.J > 0) CUDA_TRY(h->kern[mode].launch(a, s));
     return 0;
 }
@@ -386,15 +389,24 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
         return fail(BOSSS_ERR_BAD_ARG, "only BOSSS_PRECISION_FP64 is built (no split-FP32 contractions)");
     const int want = opt ? opt->kernel : 0;
     if (want < 0 || want > 2) return fail(BOSSS_ERR_BAD_ARG, "bad kernel selector");
-    int variant = VARIANT_GENERIC;
     bool have_slab = true, have_generic = true;
     for (int m = 0; m < 3; ++m) {
         have_slab = have_slab && reg.count(KernelKey(phys, D, K, Q, m, VARIANT_SLAB));
         have_generic = have_generic && reg.count(KernelKey(phys, D, K, Q, m, VARIANT_GENERIC));
     }
     if (want == 2 && !have_slab) return fail(BOSSS_ERR_BAD_ARG, "no slab kernel for this operator");
-    if (want == 2 || (want == 0 && have_slab)) variant = VARIANT_SLAB;
-    if (variant == VARIANT_GENERIC && !have_generic)
+    // automatic choice per mode, measured on B200 (32^3 / 48^3 grids): the slab kernel for 3D
+    // systems (Euler, 3-6x); for the scalar family (one field, Q threads per cell) the slab
+    // residual and VJP up to 5 nodes per direction (1.1-1.7x faster), the slab JVP up to 4
+    // (beyond, the generic tile is faster: up to 2x with 7 or 9 nodes)
+    int mode_variant[3];
+    for (int m = 0; m < 3; ++m) {
+        const bool slab_pays = phys == PHYS_EULER || Q <= (m == MODE_JVP ? 4 : 5);
+        mode_variant[m] = (want == 2 || (want == 0 && have_slab && slab_pays)) ? VARIANT_SLAB : VARIANT_GENERIC;
+    }
+    bool need_generic = false;
+    for (int m = 0; m < 3; ++m) need_generic = need_generic || mode_variant[m] == VARIANT_GENERIC;
+    if (need_generic && !have_generic)
         return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no device kernel for degree " + std::to_string(K) +
                                                          " with " + std::to_string(Q) + " Gauss nodes");
     int ndev = 0;
@@ -463,8 +475,11 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     const int NV = (phys == PHYS_EULER) ? D + 2 : 1;
     h->ndom = (int64_t)J * NV * np_of(D, K);
     h->ncod = h->ndom;
-    for (int m = 0; m < 3; ++m) h->kern[m] = reg[KernelKey(phys, D, K, Q, m, variant)];
-    h->variant = variant;
+    h->variant = VARIANT_GENERIC;   // generic unless some mode runs on the slab kernel
+    for (int m = 0; m < 3; ++m) {
+        h->kern[m] = reg[KernelKey(phys, D, K, Q, m, mode_variant[m])];
+        if (mode_variant[m] == VARIANT_SLAB) h->variant = VARIANT_SLAB;
+    }
     cudaError_t e = cudaSetDevice(dev);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {

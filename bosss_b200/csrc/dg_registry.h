@@ -22,6 +22,7 @@ std::map<KernelKey, KernelEntry>& kernel_registry();
 
 void register_scalar2();
 void register_scalar3();
+void register_scalar3_slab();
 void register_euler2();
 void register_euler3();
 }  // namespace bosss

@@ -739,9 +739,14 @@ int bosss_b200_xdg_create(const bosss_op_desc* opA, const bosss_op_desc* opB, co
         if (xopt->moment_degree >= 0) xo.moment_degree = xopt->moment_degree;
         if (xopt->subdivision > 0) xo.subdivision = xopt->subdivision;
     }
+    // the species masks of the bulk evaluation are read by the generic tile kernel only
+    bosss_options hopt{};
+    if (opt) hopt = *opt;
+    if (hopt.kernel == 2) return fail(BOSSS_ERR_BAD_ARG, "XDG evaluation runs on the generic kernel (species masks)");
+    hopt.kernel = 1;
     bosss_xdg* X = new bosss_xdg();
     for (int s = 0; s < 2; ++s) {
-        int rc = bosss_b200_create(s == 0 ? opA : opB, grid, opt, &X->h[s]);
+        int rc = bosss_b200_create(s == 0 ? opA : opB, grid, &hopt, &X->h[s]);
         if (rc) {
             bosss_b200_xdg_destroy(X);
             return rc;

@@ -111,6 +111,62 @@ def test_euler_full_size_slab_matches_generic():
     assert rel(r2, r1) <= TOL and rel(g2, g1) <= TOL
 
 
+def _transport3d(n, k, seed, periodic):
+    g = O.Cartesian3DGrid(*[np.linspace(0, 1, n + 1)] * 3, periodic, periodic, periodic)
+    op = O.DifferentialOperator(["u"], [], ["R"], O.QuadOrderFunc.FixedOrder(2 * k + 1))
+    op.EquationComponents["R"].Add(O.ScalarTransportFlux((0.7, -0.4, 0.3), "u"))
+    op.Commit()
+    U = np.random.default_rng(seed).uniform(-1, 1, g.NoOfCells * O.np_of(3, k))
+    return P.Problem("transport3d", op, g, [O.DGField(g, k, "u")], [O.DGField(g, k, "R")], U, {})
+
+
+SCALAR3D = ([("transport_k%d_%s" % (k, "per" if per else "bnd"), (lambda k=k, per=per: _transport3d(3, k, 60 + k, per)))
+             for k in (0, 1, 2, 3, 4) for per in (True, False)]
+            + [("sip_k%d" % k, (lambda k=k: P.nonlinear_diffusion3d(n=3, k=k, seed=70 + k, source=0.5)))
+               for k in (1, 2, 3, 4)]
+            + [("advdiff_k%d_%s" % (k, "per" if per else "bnd"),
+                (lambda k=k, per=per: P.advection_diffusion3d(n=3, k=k, seed=80 + k, periodic=per)))
+               for k in (1, 2, 3, 4) for per in (True, False)])
+
+
+@pytest.mark.parametrize("name,make", SCALAR3D, ids=[s[0] for s in SCALAR3D])
+@pytest.mark.parametrize("kernel", [C.KERNEL_GENERIC, C.KERNEL_SLAB], ids=["generic", "slab"])
+def test_scalar3d_kernel_variants(name, make, kernel):
+    """Both 3D kernels on the scalar family (transport, SIP with nu(u) and source,
+    advection-diffusion; periodic and boundary grids): residual with alpha/beta and JVP
+    against the oracle, VJP against the transposed oracle Jacobian."""
+    pr = make()
+    opd, gd = pr.descs()
+    r = np.random.default_rng(11)
+    V = r.uniform(-1, 1, pr.n_dofs)
+    W = r.uniform(-1, 1, pr.n_dofs)
+    out0 = r.uniform(-1, 1, pr.n_dofs)
+    ref = orc.evaluate(opd, gd, pr.U, alpha=0.5, beta=-1.5, out=out0)
+    jref = orc.jvp(opd, gd, pr.U, V)
+    A = orc.jacobian_dense(opd, gd, pr.U)
+    with pr.evaluator(kernel=kernel) as ev:
+        out = out0.copy()
+        ev.Evaluate(0.5, -1.5, out, pr.U)
+        jv = ev.jvp(pr.U, V)
+        jtw = ev.vjp(pr.U, W)
+    assert rel(out, ref) <= TOL, rel(out, ref)
+    assert rel(jv, jref) <= TOL, rel(jv, jref)
+    assert rel(jtw, A.T @ W) <= TOL, rel(jtw, A.T @ W)
+
+
+def test_sip_full_size_slab_matches_generic():
+    pr = P.nonlinear_diffusion3d(n=48, k=2, seed=3000)
+    r = np.random.default_rng(9)
+    V, W = r.uniform(-1, 1, pr.n_dofs), r.uniform(-1, 1, pr.n_dofs)
+    with pr.evaluator(kernel=C.KERNEL_GENERIC) as e1, pr.evaluator(kernel=C.KERNEL_SLAB) as e2:
+        r1, r2 = np.zeros(pr.n_dofs), np.zeros(pr.n_dofs)
+        e1.Evaluate(1.0, 0.0, r1, pr.U)
+        e2.Evaluate(1.0, 0.0, r2, pr.U)
+        assert rel(r2, r1) <= TOL
+        assert rel(e2.jvp(pr.U, V), e1.jvp(pr.U, V)) <= TOL
+        assert rel(e2.vjp(pr.U, W), e1.vjp(pr.U, W)) <= TOL
+
+
 def test_alpha_beta_semantics():
     pr = P.euler3d(n=3, k=2, seed=40)
     r = np.random.default_rng(3)
