@@ -214,7 +214,8 @@ class PartEvaluator:
         return ctypes.c_void_p(s if s else C.CUDA_STREAM_LEGACY)
 
     def apply(self, mode, U, V, out, cells, alpha=1.0, beta=0.0, time=0.0):
-        """``out = beta*out + alpha*mode(U[, V])`` on the cell range ``cells`` (CUDA tensors)."""
+        """Residual ``out = beta*out + alpha*Op(U)``, or the JVP / VJP product (alpha, beta unused),
+        on the cell range ``cells`` (CUDA tensors)."""
         a, b = cells
         C.check(C.lib().bosss_b200_apply_device(self.handle, int(mode), float(alpha), float(beta), C.ptr(U),
                                                 C.ptr(V), C.ptr(out), float(time), int(a), int(b), self._stream()))

@@ -359,7 +359,8 @@ int bosss_b200_rk_steps(bosss_handle* h, int32_t stages, const double* a, const 
 
 /* Residual (mode 0), JVP (1) or VJP (2) on the cells [cell_begin, cell_end) of the handle's
  * grid only, device buffers, enqueued on `stream` (NULL: the handle's stream): the cells'
- * outputs are written (out = beta*out + alpha*result), nothing else is. U and V hold the whole
+ * outputs are written (residual: out = beta*out + alpha*R; JVP / VJP: out = the product,
+ * alpha and beta unused), nothing else is. U and V hold the whole
  * grid, so the cells' face neighbours are read. This is the building block of partitioned
  * evaluation with ghost layers: the interior of a part is evaluated while the halo exchange
  * of its ghost cells is in flight, the cells next to the ghosts afterwards
