@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "dg_slab_kernel.cuh"
 #include "handle.h"
 
 namespace bosss {
@@ -37,33 +38,63 @@ struct WorkItem {
     long long c0;
 };
 
-// degrees with batched kernels: Q = K+1 (Linear(), order 2K / 2K+1) and 2K+1 (NonLinear(3))
+// degrees with batched kernels: Q = K+1 (Linear(), order 2K / 2K+1) and 2K+1 (NonLinear(3)).
+// Two tile kernels: the generic cell tile (every case) and the register-blocked slab tile
+// (cases with at most 5 nodes per direction, where it is the faster one).
 #define BOSSS_BATCH_CASES(X) X(1, 2) X(2, 3) X(3, 4) X(4, 5) X(1, 3) X(2, 5) X(3, 7)
+#define BOSSS_BATCH_SLAB_CASES(X) X(1, 2) X(2, 3) X(3, 4) X(4, 5) X(1, 3) X(2, 5)
 
-template <class Phys, int MODE>
+// tile configuration of a case in the generic (SLAB = false) or slab batched kernel
+template <class Phys, int K, int Q, int MODE, bool SLAB>
+struct BatchTile {
+    using G = Cfg<Phys, K, Q, MODE>;
+    using S = SlabCfg<Phys, K, Q, MODE>;
+    static constexpr int CPB = SLAB ? S::CPB : G::CPB;
+    static constexpr size_t SMEM_BYTES = SLAB ? S::SMEM_BYTES : G::SMEM_BYTES;
+    static constexpr int NT = SLAB ? S::NT : G::NT;
+};
+
+// threads per CTA and resident CTAs per SM the batched kernel is compiled for. One kernel
+// holds the tiles of every case, so its register budget is the largest case's: no
+// min-blocks bound beyond the register file (a tighter one spills kilobytes per thread)
+template <int MODE, bool SLAB>
+struct BatchBlock {
+    static constexpr int NT = (SLAB && MODE == MODE_VJP) ? 128 : 256;
+    static constexpr int MINB = (SLAB && MODE == MODE_VJP) ? 2 : 1;
+};
+
+template <class Phys, int MODE, bool SLAB>
 constexpr size_t batch_smem() {
     size_t m = 0;
-#define BOSSS_SMEM_MAX(K, Q) m = m > Cfg<Phys, K, Q, MODE>::SMEM_BYTES ? m : Cfg<Phys, K, Q, MODE>::SMEM_BYTES;
-    BOSSS_BATCH_CASES(BOSSS_SMEM_MAX)
+#define BOSSS_SMEM_MAX(K, Q)                                                                                   \
+    m = m > BatchTile<Phys, K, Q, MODE, SLAB>::SMEM_BYTES ? m : BatchTile<Phys, K, Q, MODE, SLAB>::SMEM_BYTES;
+    if constexpr (SLAB) {
+        BOSSS_BATCH_SLAB_CASES(BOSSS_SMEM_MAX)
+    } else {
+        BOSSS_BATCH_CASES(BOSSS_SMEM_MAX)
+    }
 #undef BOSSS_SMEM_MAX
     return m;
 }
 
-template <class Phys, int K, int Q, int MODE>
+template <class Phys, int K, int Q, int MODE, bool SLAB>
 __device__ __forceinline__ void run_item(const EvalArgs& a, const WorkItem& w, double* smem) {
-    constexpr int CPB = Cfg<Phys, K, Q, MODE>::CPB;
+    using BT = BatchTile<Phys, K, Q, MODE, SLAB>;
+    static_assert(BT::NT <= BatchBlock<MODE, SLAB>::NT, "tile needs more threads than the batched CTA has");
     for (int t = 0; t < w.ntiles; ++t) {
-        const long long c0 = w.c0 + (long long)t * CPB;
+        const long long c0 = w.c0 + (long long)t * BT::CPB;
         if (c0 >= a.g.J) break;
-        cell_tile<Phys, K, Q, MODE>(a, c0, smem);
+        if constexpr (SLAB) slab_tile<Phys, K, Q, MODE>(a, c0, smem);
+        else cell_tile<Phys, K, Q, MODE>(a, c0, smem);
         __syncthreads();
     }
 }
 
-template <class Phys, int MODE>
-__global__ void __launch_bounds__(256) batch_kernel(const BatchInst* __restrict__ inst, const WorkItem* __restrict__ items,
-                                                    int nitems, int* __restrict__ counter, const double* U, const double* V,
-                                                    double* out, double alpha, double beta, double time) {
+template <class Phys, int MODE, bool SLAB>
+__global__ void __launch_bounds__(BatchBlock<MODE, SLAB>::NT, BatchBlock<MODE, SLAB>::MINB)
+batch_kernel(const BatchInst* __restrict__ inst, const WorkItem* __restrict__ items, int nitems,
+             int* __restrict__ counter, const double* U, const double* V, double* out, double alpha, double beta,
+             double time) {
     extern __shared__ double smem[];
     __shared__ EvalArgs sa;
     __shared__ WorkItem w;
@@ -92,27 +123,39 @@ __global__ void __launch_bounds__(256) batch_kernel(const BatchInst* __restrict_
         }
         __syncthreads();
 #define BOSSS_CASE(KK, QQ) \
-    if (K == KK && Q == QQ) run_item<Phys, KK, QQ, MODE>(sa, w, smem);
-        BOSSS_BATCH_CASES(BOSSS_CASE)
+    if (K == KK && Q == QQ) run_item<Phys, KK, QQ, MODE, SLAB>(sa, w, smem);
+        if constexpr (SLAB) {
+            BOSSS_BATCH_SLAB_CASES(BOSSS_CASE)
+        } else {
+            BOSSS_BATCH_CASES(BOSSS_CASE)
+        }
 #undef BOSSS_CASE
         __syncthreads();
     }
 }
 
-template <class Phys, int MODE>
+template <class Phys, int MODE, bool SLAB>
 static bool batch_supported(int K, int Q) {
 #define BOSSS_SUP(KK, QQ) \
-    if (K == KK && Q == QQ) return Cfg<Phys, KK, QQ, MODE>::SMEM_BYTES <= 227 * 1024;
-    BOSSS_BATCH_CASES(BOSSS_SUP)
+    if (K == KK && Q == QQ) return BatchTile<Phys, KK, QQ, MODE, SLAB>::SMEM_BYTES <= 227 * 1024;
+    if constexpr (SLAB) {
+        BOSSS_BATCH_SLAB_CASES(BOSSS_SUP)
+    } else {
+        BOSSS_BATCH_CASES(BOSSS_SUP)
+    }
 #undef BOSSS_SUP
     return false;
 }
 
-template <class Phys, int MODE>
+template <class Phys, int MODE, bool SLAB>
 static int cpb_of(int K, int Q) {
 #define BOSSS_CPB(KK, QQ) \
-    if (K == KK && Q == QQ) return Cfg<Phys, KK, QQ, MODE>::CPB;
-    BOSSS_BATCH_CASES(BOSSS_CPB)
+    if (K == KK && Q == QQ) return BatchTile<Phys, KK, QQ, MODE, SLAB>::CPB;
+    if constexpr (SLAB) {
+        BOSSS_BATCH_SLAB_CASES(BOSSS_CPB)
+    } else {
+        BOSSS_BATCH_CASES(BOSSS_CPB)
+    }
 #undef BOSSS_CPB
     return 1;
 }
@@ -120,35 +163,38 @@ static int cpb_of(int K, int Q) {
 using BatchLaunch = cudaError_t (*)(const BatchInst*, const WorkItem*, int, int*, const double*, const double*, double*,
                                     double, double, double, int, cudaStream_t);
 
-template <class Phys, int MODE>
+template <class Phys, int MODE, bool SLAB>
 static cudaError_t launch_batch(const BatchInst* inst, const WorkItem* items, int nitems, int* counter, const double* U,
                                 const double* V, double* out, double alpha, double beta, double time, int grid,
                                 cudaStream_t s) {
-    constexpr size_t smem = batch_smem<Phys, MODE>();
+    constexpr size_t smem = batch_smem<Phys, MODE, SLAB>();
     static unsigned long long done = 0ull;
     int dev = 0;
     cudaGetDevice(&dev);
     if (!(done & (1ull << (dev & 63)))) {
-        cudaError_t e = cudaFuncSetAttribute(batch_kernel<Phys, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e =
+            cudaFuncSetAttribute(batch_kernel<Phys, MODE, SLAB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(batch_kernel<Phys, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        e = cudaFuncSetAttribute(batch_kernel<Phys, MODE, SLAB>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         done |= 1ull << (dev & 63);
     }
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
-    batch_kernel<Phys, MODE><<<grid, 256, smem, s>>>(inst, items, nitems, counter, U, V, out, alpha, beta, time);
+    batch_kernel<Phys, MODE, SLAB><<<grid, BatchBlock<MODE, SLAB>::NT, smem, s>>>(inst, items, nitems, counter, U, V, out,
+                                                                                  alpha, beta, time);
     return cudaGetLastError();
 }
 
-template <class Phys, int MODE>
+template <class Phys, int MODE, bool SLAB>
 static int resident_grid() {
     int dev = 0, nsm = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    constexpr size_t smem = batch_smem<Phys, MODE>();
-    cudaFuncSetAttribute(batch_kernel<Phys, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<Phys, MODE>, 256, smem);
+    constexpr size_t smem = batch_smem<Phys, MODE, SLAB>();
+    cudaFuncSetAttribute(batch_kernel<Phys, MODE, SLAB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(batch_kernel<Phys, MODE, SLAB>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel<Phys, MODE, SLAB>, BatchBlock<MODE, SLAB>::NT, smem);
     return std::max(1, per) * std::max(1, nsm);
 }
 
@@ -168,58 +214,49 @@ struct bosss_batch {
     int* d_counter = nullptr;                     // two queue counters (two kernels per graph)
     int grid[3] = {0, 0, 0};
     std::map<std::pair<int, int>, int> tiles;     // (K, Q) -> tiles per work item (autotuned)
+    bool slab[3] = {false, false, false};         // tile kernel per mode: slab or generic
     bool lpt = true;                              // longest-processing-time-first order
     cudaGraphExec_t graph = nullptr;
 };
 
 namespace bosss {
 
-static BatchLaunch batch_launcher(int phys, int D, int mode) {
-    if (D != 3) return nullptr;
-    if (phys == PHYS_SIP) {
-        if (mode == MODE_RES) return &launch_batch<PhysScalar<3, true>, MODE_RES>;
-        if (mode == MODE_JVP) return &launch_batch<PhysScalar<3, true>, MODE_JVP>;
-        return &launch_batch<PhysScalar<3, true>, MODE_VJP>;
-    }
-    if (phys == PHYS_TRANSPORT) {
-        if (mode == MODE_RES) return &launch_batch<PhysScalar<3, false>, MODE_RES>;
-        if (mode == MODE_JVP) return &launch_batch<PhysScalar<3, false>, MODE_JVP>;
-        return &launch_batch<PhysScalar<3, false>, MODE_VJP>;
-    }
-    return nullptr;
+// calls f(Phys{}, integral_constant<MODE>, bool_constant<SLAB>) for the batch's physics family
+template <class Fn>
+static auto batch_dispatch(int phys, int mode, bool slab, Fn&& f) {
+    auto by_mode = [&](auto P) {
+        auto by_slab = [&](auto M) { return slab ? f(P, M, std::true_type{}) : f(P, M, std::false_type{}); };
+        if (mode == MODE_RES) return by_slab(std::integral_constant<int, MODE_RES>{});
+        if (mode == MODE_JVP) return by_slab(std::integral_constant<int, MODE_JVP>{});
+        return by_slab(std::integral_constant<int, MODE_VJP>{});
+    };
+    if (phys == PHYS_SIP) return by_mode(PhysScalar<3, true>{});
+    return by_mode(PhysScalar<3, false>{});
 }
 
-static bool batch_ok(int phys, int mode, int K, int Q) {
-    if (phys == PHYS_SIP) {
-        if (mode == MODE_RES) return batch_supported<PhysScalar<3, true>, MODE_RES>(K, Q);
-        if (mode == MODE_JVP) return batch_supported<PhysScalar<3, true>, MODE_JVP>(K, Q);
-        return batch_supported<PhysScalar<3, true>, MODE_VJP>(K, Q);
-    }
-    if (mode == MODE_RES) return batch_supported<PhysScalar<3, false>, MODE_RES>(K, Q);
-    if (mode == MODE_JVP) return batch_supported<PhysScalar<3, false>, MODE_JVP>(K, Q);
-    return batch_supported<PhysScalar<3, false>, MODE_VJP>(K, Q);
+static BatchLaunch batch_launcher(int phys, int D, int mode, bool slab) {
+    if (D != 3 || (phys != PHYS_SIP && phys != PHYS_TRANSPORT)) return nullptr;
+    return batch_dispatch(phys, mode, slab, [](auto P, auto M, auto S) -> BatchLaunch {
+        return &launch_batch<decltype(P), decltype(M)::value, decltype(S)::value>;
+    });
 }
 
-static int batch_cpb(int phys, int mode, int K, int Q) {
-    if (phys == PHYS_SIP) {
-        if (mode == MODE_RES) return cpb_of<PhysScalar<3, true>, MODE_RES>(K, Q);
-        if (mode == MODE_JVP) return cpb_of<PhysScalar<3, true>, MODE_JVP>(K, Q);
-        return cpb_of<PhysScalar<3, true>, MODE_VJP>(K, Q);
-    }
-    if (mode == MODE_RES) return cpb_of<PhysScalar<3, false>, MODE_RES>(K, Q);
-    if (mode == MODE_JVP) return cpb_of<PhysScalar<3, false>, MODE_JVP>(K, Q);
-    return cpb_of<PhysScalar<3, false>, MODE_VJP>(K, Q);
+static bool batch_ok(int phys, int mode, int K, int Q, bool slab) {
+    return batch_dispatch(phys, mode, slab, [&](auto P, auto M, auto S) {
+        return batch_supported<decltype(P), decltype(M)::value, decltype(S)::value>(K, Q);
+    });
 }
 
-static int batch_grid(int phys, int mode) {
-    if (phys == PHYS_SIP) {
-        if (mode == MODE_RES) return resident_grid<PhysScalar<3, true>, MODE_RES>();
-        if (mode == MODE_JVP) return resident_grid<PhysScalar<3, true>, MODE_JVP>();
-        return resident_grid<PhysScalar<3, true>, MODE_VJP>();
-    }
-    if (mode == MODE_RES) return resident_grid<PhysScalar<3, false>, MODE_RES>();
-    if (mode == MODE_JVP) return resident_grid<PhysScalar<3, false>, MODE_JVP>();
-    return resident_grid<PhysScalar<3, false>, MODE_VJP>();
+static int batch_cpb(int phys, int mode, int K, int Q, bool slab) {
+    return batch_dispatch(phys, mode, slab, [&](auto P, auto M, auto S) {
+        return cpb_of<decltype(P), decltype(M)::value, decltype(S)::value>(K, Q);
+    });
+}
+
+static int batch_grid(int phys, int mode, bool slab) {
+    return batch_dispatch(phys, mode, slab, [](auto P, auto M, auto S) {
+        return resident_grid<decltype(P), decltype(M)::value, decltype(S)::value>();
+    });
 }
 
 // work items of one mode, ordered by the batch's schedule
@@ -231,7 +268,7 @@ static int build_items(bosss_batch* b, int mode) {
     std::vector<Tmp> v;
     for (int i = 0; i < b->n; ++i) {
         const bosss_handle* h = b->h[i];
-        const int cpb = batch_cpb(b->phys, mode, h->K, h->Q);
+        const int cpb = batch_cpb(b->phys, mode, h->K, h->Q, b->slab[mode]);
         int r = 1;
         auto it = b->tiles.find({h->K, h->Q});
         if (it != b->tiles.end()) r = it->second;
@@ -261,7 +298,7 @@ static int build_items(bosss_batch* b, int mode) {
 
 static int batch_run(bosss_batch* b, int mode, double alpha, double beta, const double* U, const double* V, double* out,
                      double time, cudaStream_t s, int counter_slot) {
-    BatchLaunch L = batch_launcher(b->phys, b->D, mode);
+    BatchLaunch L = batch_launcher(b->phys, b->D, mode, b->slab[mode]);
     if (!L) return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no batched kernel for this physics");
     CUDA_TRY(L(b->d_inst, b->d_items[mode], b->nitems[mode], b->d_counter + counter_slot, U, V, out, alpha, beta, time,
                b->grid[mode], s));
@@ -303,7 +340,7 @@ int bosss_b200_batch_create(int32_t n, const bosss_op_desc* ops, const bosss_gri
             return fail(BOSSS_ERR_BAD_ARG, "batch instances must share physics family, dimension and device");
         }
         for (int m = 0; m < 3; ++m)
-            if (!batch_ok(h->phys, m, h->K, h->Q)) {
+            if (!batch_ok(h->phys, m, h->K, h->Q, false)) {
                 bosss_b200_batch_destroy(b);
                 return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT,
                             "no batched kernel for degree " + std::to_string(h->K) + " with " + std::to_string(h->Q) +
@@ -312,9 +349,21 @@ int bosss_b200_batch_create(int32_t n, const bosss_op_desc* ops, const bosss_gri
         b->dom_off.push_back(b->dom_off.back() + h->ndom);
         b->cod_off.push_back(b->cod_off.back() + h->ncod);
     }
-    if (!batch_launcher(b->phys, b->D, MODE_RES)) {
+    if (!batch_launcher(b->phys, b->D, MODE_RES, false)) {
         bosss_b200_batch_destroy(b);
         return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "batched path: 3D scalar transport / advection-diffusion only");
+    }
+    // tile kernel per mode (the single-grid rule, measured on B200): slab tiles when every
+    // instance has at most 5 (residual, VJP) / 4 (JVP) nodes per direction; kernel selector 1
+    // keeps the generic tiles, 2 asks for slab tiles wherever the batch allows them
+    const int want = opt ? opt->kernel : 0;
+    for (int m = 0; m < 3; ++m) {
+        bool ok = want != 1;
+        for (auto* h : b->h) {
+            ok = ok && batch_ok(b->phys, m, h->K, h->Q, true);
+            if (want == 0) ok = ok && h->Q <= (m == MODE_JVP ? 4 : 5);
+        }
+        b->slab[m] = ok;
     }
     auto bail = [&](cudaError_t e) {
         bosss_b200_batch_destroy(b);
@@ -335,7 +384,7 @@ int bosss_b200_batch_create(int32_t n, const bosss_op_desc* ops, const bosss_gri
     if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(int) * 2);
     if (e != cudaSuccess) return bail(e);
     for (int m = 0; m < 3; ++m) {
-        b->grid[m] = batch_grid(b->phys, m);
+        b->grid[m] = batch_grid(b->phys, m, b->slab[m]);
         int rc = build_items(b, m);
         if (rc) {
             bosss_b200_batch_destroy(b);
@@ -497,7 +546,9 @@ int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double*
             classes.push_back({h->K, h->Q});
     int rc = 0;
     for (auto kq : classes) {
-        const std::string key = table_key(b->phys, b->D, kq.first, kq.second);
+        // tiles per item depend on the tile kernels of the timed pair (residual, VJP)
+        const std::string key = table_key(b->phys, b->D, kq.first, kq.second) + (b->slab[MODE_RES] ? "_slabR" : "") +
+                                (b->slab[MODE_VJP] ? "_slabV" : "");
         if (table.count(key)) {
             b->tiles[kq] = table[key];
             continue;
@@ -635,7 +686,7 @@ __global__ void __launch_bounds__(256) batch_kernel_noalloc(unsigned char* scrat
     if (K == KK && Q == QQ) {                                                 \
         WorkItem wt = w;                                                      \
         wt.c0 *= Cfg<Phys, KK, QQ, MODE>::CPB;                                 \
-        run_item<Phys, KK, QQ, MODE>(sa, wt, smem);                           \
+        run_item<Phys, KK, QQ, MODE, false>(sa, wt, smem);                           \
     }
         BOSSS_BATCH_CASES(BOSSS_CASE)
 #undef BOSSS_CASE
@@ -646,7 +697,7 @@ __global__ void __launch_bounds__(256) batch_kernel_noalloc(unsigned char* scrat
 template <class Phys, int MODE>
 static cudaError_t launch_noalloc(unsigned char* scratch, int n, const double* U, const double* V, double* out,
                                   double alpha, double beta, double time, size_t prefix_off, cudaStream_t s) {
-    constexpr size_t smem = batch_smem<Phys, MODE>();
+    constexpr size_t smem = batch_smem<Phys, MODE, false>();
     cudaError_t e = cudaFuncSetAttribute(batch_kernel_noalloc<Phys, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
@@ -709,7 +760,7 @@ extern "C" int bosss_b200_batch_evaluate_noalloc(int32_t n, bosss_handle* const*
         if (!h || h->phys != phys || h->D != D || h->device != dev)
             return fail(BOSSS_ERR_BAD_ARG, "instances must share physics family, dimension and device");
         for (int m = 0; m < 3; ++m)
-            if (!batch_ok(phys, m, h->K, h->Q))
+            if (!batch_ok(phys, m, h->K, h->Q, false))
                 return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no batched kernel for degree " + std::to_string(h->K) +
                                                                  " with " + std::to_string(h->Q) + " Gauss nodes");
         stage_inst[i].a = h->base;
@@ -719,7 +770,7 @@ extern "C" int bosss_b200_batch_evaluate_noalloc(int32_t n, bosss_handle* const*
         stage_inst[i].Q = h->Q;
         doff += h->ndom;
         coff += h->ncod;
-        const long long cpb = batch_cpb(phys, mode, h->K, h->Q);
+        const long long cpb = batch_cpb(phys, mode, h->K, h->Q, false);
         stage_prefix[i + 1] = stage_prefix[i] + (h->base.g.J + cpb - 1) / cpb;
     }
     if (stage_prefix[n] > 2000000000LL) return fail(BOSSS_ERR_BAD_ARG, "allocation-free batch: too many cell tiles");

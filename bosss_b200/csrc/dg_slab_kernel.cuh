@@ -578,30 +578,31 @@ __device__ __forceinline__ void slab_face_traces(const EvalArgs& args, const dou
     }
 }
 
+// Evaluates the tile of cells [c0, c0 + CPB) (clipped to args.cend); the first C::NT threads
+// of the CTA do the work, any further threads only take part in the barriers (the batched
+// persistent kernel runs tiles of several degrees in CTAs of one size).
 template <class Phys, int K, int Q, int MODE>
-__global__ void __launch_bounds__(SlabCfg<Phys, K, Q, MODE>::NT, SlabCfg<Phys, K, Q, MODE>::MINB)
-dg_slab_kernel(const __grid_constant__ EvalArgs args) {
+__device__ __forceinline__ void slab_tile(const EvalArgs& args, long long c0, double* smem) {
     using C = SlabCfg<Phys, K, Q, MODE>;
     constexpr int NP = C::NP, NV = C::NV, NO = C::NO, CPB = C::CPB, NT = C::NT, SPLIT = C::SPLIT;
     constexpr int SLV = C::SLV, FV = C::FV, SLF = C::SLF, FF = C::FF, QF = Q * Q;
-    extern __shared__ double smem[];
     const GridConst& g = args.g;
     const Tables1D& T = args.tab;
     const int tid = threadIdx.x;
-    const long long c0 = args.cbeg + (long long)blockIdx.x * CPB;
+    const int tt = tid < NT ? tid : (1 << 30);   // start of the strided loops (threads beyond NT: none)
     const int ncell = (int)((args.cend - c0) < CPB ? (args.cend - c0) : CPB);
     // own (part, cell, output field, slab); part is warp-uniform (parts padded to warps)
     const int part = tid / C::HALFP, r0 = tid % C::HALFP;
     const int q = r0 % Q, o = (r0 / Q) % NO, cl = (r0 < C::HALF) ? r0 / (Q * NO) : CPB;
-    const bool active = cl < ncell;
+    const bool active = tid < NT && cl < ncell;
     auto CIN = [&](int c) { return smem + (size_t)c * C::S_CELL; };
     auto WK = [&](int c) { return smem + (size_t)c * C::S_CELL + C::S_CIN; };
 
     constexpr int NVPC = NV * NP;
     constexpr int N1PC = C::NF1 * NP;
-    for (int i = tid; i < ncell * NVPC; i += NT) CIN(i / NVPC)[i % NVPC] = args.U[c0 * NVPC + i];
+    for (int i = tt; i < ncell * NVPC; i += NT) CIN(i / NVPC)[i % NVPC] = args.U[c0 * NVPC + i];
     if constexpr (C::NF1 > 0)
-        for (int i = tid; i < ncell * N1PC; i += NT) CIN(i / N1PC)[NVPC + i % N1PC] = args.V[c0 * N1PC + i];
+        for (int i = tt; i < ncell * N1PC; i += NT) CIN(i / N1PC)[NVPC + i % N1PC] = args.V[c0 * N1PC + i];
 
     double Aq[K + 1], dAq[K + 1];
 #pragma unroll
@@ -623,7 +624,7 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
         else if constexpr (SPLIT > 1) slab_volume_interp<Phys, K, Q, MODE, 1>(args, CIN(cl), WK(cl), o, q, Aq, dAq);
     }
     __syncthreads();
-    for (int it = tid; it < CPB * Q * Q * Q; it += NT) {
+    for (int it = tt; it < CPB * Q * Q * Q; it += NT) {
         const int n = it % (Q * Q * Q), c = it / (Q * Q * Q);
         if (c >= ncell) continue;
         const int qx = n % Q, qy = (n / Q) % Q, qz = n / (Q * Q);
@@ -670,7 +671,7 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
             }
         }
         __syncthreads();
-        for (int it = tid; it < CPB * 2 * QF; it += NT) {
+        for (int it = tt; it < CPB * 2 * QF; it += NT) {
             const int qf = it % QF, s = (it / QF) % 2, c = it / (2 * QF);
             if (c >= ncell) continue;
             const int q1 = qf % Q, q2 = qf / Q;
@@ -739,7 +740,7 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
         for (int n = 0; n < NP; ++n) red[n] = R[n];
     }
     __syncthreads();
-    for (int it = tid; it < ncell * NO * NP; it += NT) {
+    for (int it = tt; it < ncell * NO * NP; it += NT) {
         const int n = it % NP, oo = (it / NP) % NO, c = it / (NP * NO);
         double v = 0.0;
 #pragma unroll
@@ -751,6 +752,13 @@ dg_slab_kernel(const __grid_constant__ EvalArgs args) {
             args.out[gi] = v;
         }
     }
+}
+
+template <class Phys, int K, int Q, int MODE>
+__global__ void __launch_bounds__(SlabCfg<Phys, K, Q, MODE>::NT, SlabCfg<Phys, K, Q, MODE>::MINB)
+dg_slab_kernel(const __grid_constant__ EvalArgs args) {
+    extern __shared__ double smem[];
+    slab_tile<Phys, K, Q, MODE>(args, args.cbeg + (long long)blockIdx.x * SlabCfg<Phys, K, Q, MODE>::CPB, smem);
 }
 
 }  // namespace bosss

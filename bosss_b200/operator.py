@@ -510,7 +510,7 @@ class BatchEvaluator:
     :class:`bosss_b200.problems.Problem`. Vectors are the concatenation of the
     instances' vectors; ``offsets`` gives the instance boundaries."""
 
-    def __init__(self, problems, device=0):
+    def __init__(self, problems, device=0, kernel=C.KERNEL_AUTO):
         self.handle = None
         descs = [p.descs() for p in problems]
         self.n = len(descs)
@@ -518,6 +518,7 @@ class BatchEvaluator:
         self._grids = (C.GridDesc * self.n)(*[d[1] for d in descs])
         opt = C.Options()
         opt.device = int(device)
+        opt.kernel = int(kernel)   # tile kernel: 0 automatic, 1 generic tiles, 2 slab tiles where possible
         h = ctypes.c_void_p()
         C.check(C.lib().bosss_b200_batch_create(self.n, ctypes.byref(self._ops), ctypes.byref(self._grids),
                                                 ctypes.byref(opt), ctypes.byref(h)))

@@ -129,7 +129,8 @@ typedef struct bosss_grid_desc {
      * periodicity global_periodic per direction (the offset may be negative, or reach past
      * global_n, where a ghost layer wraps around a periodic direction). For a part, lo and hi
      * are the box of the GLOBAL grid: cell widths and node coordinates are computed exactly
-     * as on the whole grid, so a part's results equal the whole grid's bit for bit. The SIP
+     * as on the whole grid, so a part's results equal the whole grid's (to the last bit of the
+ * VJP, which can move with the tile a cell shares with its neighbours). The SIP
      * penalty's cell length scale (GridData_CellData.cs:663-684) counts the global boundary,
      * not the edge of the part. All zero: the grid is the whole grid. */
     int32_t global_n[3];
@@ -259,7 +260,10 @@ int bosss_b200_compute_jacobian(bosss_handle* h, const double* U, double time, b
  * queue in device memory. Vectors are the concatenation of the instances' vectors
  * (offsets from bosss_b200_batch_get_sizes). The residual + VJP pair can be captured once
  * into a CUDA graph and replayed; an autotuner picks the cell tiles per work item for each
- * (degree, quadrature nodes) class and the queue order, persisted in a small text table. */
+ * (degree, quadrature nodes) class and the queue order, persisted in a small text table.
+ * Tile kernel per mode (opt->kernel): 0 = automatic (register-blocked slab tiles when every
+ * instance has at most 5 nodes per direction, 4 for the JVP; else the generic tiles),
+ * 1 = generic tiles, 2 = slab tiles wherever every instance allows them. */
 typedef struct bosss_batch bosss_batch;
 
 enum bosss_eval_mode { BOSSS_MODE_RESIDUAL = 0, BOSSS_MODE_JVP = 1, BOSSS_MODE_VJP = 2 };

@@ -23,12 +23,14 @@ def small_batch():
     return P.batched_advection_diffusion(n_instances=10, seed=77, sizes=(3, 4, 5), degrees=(1, 2, 3, 4))
 
 
-def test_batch_matches_single_and_oracle():
+@pytest.mark.parametrize("kernel", [C.KERNEL_AUTO, C.KERNEL_GENERIC, C.KERNEL_SLAB],
+                         ids=["auto", "generic_tiles", "slab_tiles"])
+def test_batch_matches_single_and_oracle(kernel):
     probs = small_batch()
     U = np.concatenate([p.U for p in probs])
     r = np.random.default_rng(1)
     V = r.uniform(-1, 1, U.size)
-    with O.BatchEvaluator(probs) as b:
+    with O.BatchEvaluator(probs, kernel=kernel) as b:
         off = b.dom_offsets
         R = b.evaluate(C.MODE_RESIDUAL, U)
         JV = b.evaluate(C.MODE_JVP, U, V)
@@ -42,7 +44,7 @@ def test_batch_matches_single_and_oracle():
             assert rel(G[sl], ev.vjp(p.U, V[sl])) <= 1e-13
             single = np.zeros(p.n_dofs)
             ev.Evaluate(1.0, 0.0, single, p.U)
-            assert rel(R[sl], single) <= 1e-14
+            assert rel(R[sl], single) <= 1e-13
 
 
 def test_batch_graph_replay_and_autotune(tmp_path):
