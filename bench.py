@@ -230,6 +230,39 @@ def run_batched(args):
     ms = [a.elapsed_time(c) for a, c in ts]
     total_ms = float(np.sum(ms))
     value = 2 * n * args.steps / (total_ms * 1e-3)
+
+    # plain FP64 path: every instance through its own evaluator on the generic kernel, one
+    # residual and one VJP launch per instance (what a caller does without the batched path)
+    from bosss_b200 import _capi as C
+    import ctypes
+    L = C.lib()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    evs = [p.evaluator(kernel=C.KERNEL_GENERIC) for p in probs]
+    off = b.dom_offsets
+    Rp, Gp = torch.zeros_like(R), torch.zeros_like(G)
+
+    def plain_step():
+        for i, e in enumerate(evs):
+            a0, a1 = int(off[i]), int(off[i + 1])
+            C.check(L.bosss_b200_evaluate_device(e.handle, 1.0, 0.0, C.ptr(U[a0:a1]), C.ptr(Rp[a0:a1]), 0.0, sp))
+            C.check(L.bosss_b200_vjp_device(e.handle, C.ptr(U[a0:a1]), C.ptr(W[a0:a1]), C.ptr(Gp[a0:a1]), 0.0, sp))
+
+    plain_step()
+    torch.cuda.synchronize()
+    plain_ms = []
+    for i in range(min(args.steps, 5)):
+        flush.fill_(float(i))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plain_step()
+        e1.record(stream)
+        plain_ms.append((e0, e1))
+    torch.cuda.synchronize()
+    plain_step_ms = float(np.mean([a.elapsed_time(c) for a, c in plain_ms]))
+    plain_value = 2 * n / (plain_step_ms * 1e-3)
+    plain_diff = max(float((Rp - R).abs().max() / R.abs().max()), float((Gp - G).abs().max() / G.abs().max()))
+    for e in evs:
+        e.Dispose()
     hbm = (load_json(os.path.join(ROOT, "MEASURED_PEAKS.json")) or {}).get("hbm_gbs", 6650.0)
     bytes_step = 8.0 * (2 * n + 3 * n)   # residual: U in, R out; VJP: U, W in, G out
     achieved = bytes_step / (np.mean(ms) * 1e-3) / 1e9
@@ -239,11 +272,17 @@ def run_batched(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "batched_advdiff_%d_instances_residual+vjp" % len(probs), "dofs": n,
                        "instances": len(probs), "k_hist": {str(k): ks.count(k) for k in sorted(set(ks))},
-                       "launch": "one CUDA graph: two persistent launches (residual, VJP)",
+                       "launch": "one CUDA graph per step: residual then VJP, schedule chosen by the autotuner "
+                                 "(persistent queue lpt/fifo, or one launch per (k, Q) class)",
+                       "schedule": b.tiles(1, 2)[1],
                        "l2": "flushed between steps", "autotune_s": tune_s},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": None, "kernel": "batch_kernel<PhysScalar<3,true>> (RES + VJP)"},
-            "gpu_launches": 2 * args.steps, "clocks": clk}
+            "plain_fp64": {"kernel": "dg_cell_kernel per instance (generic fused FP64, 2 launches per instance)",
+                           "value": plain_value, "ms_per_step": plain_step_ms, "chosen_over_plain": value / plain_value,
+                           "max_rel_diff": plain_diff},
+            "gpu_launches": (2 * len({p.config["k"] for p in probs}) if b.tiles(1, 2)[1] == "classes" else 2) * args.steps,
+            "clocks": clk}
     print(json.dumps(line), flush=True)
     b.Dispose()
 

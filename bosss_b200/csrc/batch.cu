@@ -84,7 +84,7 @@ __device__ __forceinline__ void run_item(const EvalArgs& a, const WorkItem& w, d
     for (int t = 0; t < w.ntiles; ++t) {
         const long long c0 = w.c0 + (long long)t * BT::CPB;
         if (c0 >= a.g.J) break;
-        if constexpr (SLAB) slab_tile<Phys, K, Q, MODE>(a, c0, smem);
+        if constexpr (SLAB) slab_tile<Phys, K, Q, MODE>(a, a.tab, c0, smem);
         else cell_tile<Phys, K, Q, MODE>(a, c0, smem);
         __syncthreads();
     }
@@ -198,6 +198,79 @@ static int resident_grid() {
     return std::max(1, per) * std::max(1, nsm);
 }
 
+// ---- per-class schedule: one launch per (K, Q) class over the tiles of all its instances, one
+// tile per CTA, with the single-grid kernel's launch configuration (threads, resident CTAs per
+// SM) and the class's 1D tables in the kernel-parameter bank (they depend on K and Q only)
+template <class Phys, int K, int Q, int MODE, bool SLAB>
+struct ClassBlock {
+    static constexpr int NT = SLAB ? SlabCfg<Phys, K, Q, MODE>::NT : Cfg<Phys, K, Q, MODE>::NT;
+    static constexpr int MINB = SLAB ? SlabCfg<Phys, K, Q, MODE>::MINB : 1;
+};
+
+template <class Phys, int K, int Q, int MODE, bool SLAB>
+__global__ void __launch_bounds__(ClassBlock<Phys, K, Q, MODE, SLAB>::NT, ClassBlock<Phys, K, Q, MODE, SLAB>::MINB)
+batch_class_kernel(const __grid_constant__ Tables1D tab, const BatchInst* __restrict__ inst,
+                   const WorkItem* __restrict__ items, const double* U, const double* V, double* out, double alpha,
+                   double beta, double time) {
+    extern __shared__ double smem[];
+    __shared__ EvalArgs sa;
+    const WorkItem w = items[blockIdx.x];
+    const BatchInst* b = inst + w.inst;
+    for (int i = threadIdx.x; i < (int)(sizeof(EvalArgs) / 8); i += blockDim.x)
+        reinterpret_cast<double*>(&sa)[i] = reinterpret_cast<const double*>(&b->a)[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        sa.U = U + b->dom_off;
+        sa.V = V ? V + ((MODE == MODE_VJP) ? b->cod_off : b->dom_off) : nullptr;
+        sa.out = out + ((MODE == MODE_VJP) ? b->dom_off : b->cod_off);
+        sa.alpha = alpha;
+        sa.beta = beta;
+        sa.time = time;
+    }
+    __syncthreads();
+    if constexpr (SLAB) slab_tile<Phys, K, Q, MODE>(sa, tab, w.c0, smem);
+    else cell_tile<Phys, K, Q, MODE>(sa, w.c0, smem);
+}
+
+using ClassLaunch = cudaError_t (*)(const Tables1D&, const BatchInst*, const WorkItem*, int, const double*,
+                                    const double*, double*, double, double, double, cudaStream_t);
+
+template <class Phys, int K, int Q, int MODE, bool SLAB>
+static cudaError_t launch_class(const Tables1D& tab, const BatchInst* inst, const WorkItem* items, int n,
+                                const double* U, const double* V, double* out, double alpha, double beta, double time,
+                                cudaStream_t s) {
+    constexpr size_t smem = BatchTile<Phys, K, Q, MODE, SLAB>::SMEM_BYTES;
+    static unsigned long long done = 0ull;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(done & (1ull << (dev & 63)))) {
+        cudaError_t e = cudaFuncSetAttribute(batch_class_kernel<Phys, K, Q, MODE, SLAB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(batch_class_kernel<Phys, K, Q, MODE, SLAB>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
+        done |= 1ull << (dev & 63);
+    }
+    if (n <= 0) return cudaSuccess;
+    batch_class_kernel<Phys, K, Q, MODE, SLAB><<<n, ClassBlock<Phys, K, Q, MODE, SLAB>::NT, smem, s>>>(
+        tab, inst, items, U, V, out, alpha, beta, time);
+    return cudaGetLastError();
+}
+
+template <class Phys, int MODE, bool SLAB>
+static ClassLaunch class_launch_of(int K, int Q) {
+#define BOSSS_CL(KK, QQ) \
+    if (K == KK && Q == QQ) return &launch_class<Phys, KK, QQ, MODE, SLAB>;
+    if constexpr (SLAB) {
+        BOSSS_BATCH_SLAB_CASES(BOSSS_CL)
+    } else {
+        BOSSS_BATCH_CASES(BOSSS_CL)
+    }
+#undef BOSSS_CL
+    return nullptr;
+}
+
 }  // namespace bosss
 
 using namespace bosss;
@@ -216,6 +289,15 @@ struct bosss_batch {
     std::map<std::pair<int, int>, int> tiles;     // (K, Q) -> tiles per work item (autotuned)
     bool slab[3] = {false, false, false};         // tile kernel per mode: slab or generic
     bool lpt = true;                              // longest-processing-time-first order
+    // per-class schedule (one launch per (K, Q) class and mode) instead of the persistent queue
+    struct ClassRun {
+        int K, Q;
+        bool slab;
+        int first, count;   // range of this class's tiles in d_class_items[mode]
+    };
+    bool classes = false;
+    std::vector<ClassRun> runs[3];
+    WorkItem* d_class_items[3] = {nullptr, nullptr, nullptr};
     cudaGraphExec_t graph = nullptr;
 };
 
@@ -296,8 +378,60 @@ static int build_items(bosss_batch* b, int mode) {
     return BOSSS_OK;
 }
 
+static ClassLaunch class_launcher(int phys, int mode, int K, int Q, bool slab) {
+    return batch_dispatch(phys, mode, slab, [&](auto P, auto M, auto S) {
+        return class_launch_of<decltype(P), decltype(M)::value, decltype(S)::value>(K, Q);
+    });
+}
+
+// tiles of the per-class schedule of one mode: instances grouped by (K, Q), one tile per item
+static int build_class_items(bosss_batch* b, int mode, int want) {
+    std::vector<WorkItem> w;
+    b->runs[mode].clear();
+    std::vector<std::pair<int, int>> classes;
+    for (auto* h : b->h)
+        if (std::find(classes.begin(), classes.end(), std::make_pair(h->K, h->Q)) == classes.end())
+            classes.push_back({h->K, h->Q});
+    for (auto kq : classes) {
+        bosss_batch::ClassRun r;
+        r.K = kq.first;
+        r.Q = kq.second;
+        r.slab = want != 1 && batch_ok(b->phys, mode, r.K, r.Q, true) &&
+                 (want == 2 || r.Q <= (mode == MODE_JVP ? 4 : 5));
+        r.first = (int)w.size();
+        const int cpb = batch_cpb(b->phys, mode, r.K, r.Q, r.slab);
+        for (int i = 0; i < b->n; ++i) {
+            const bosss_handle* h = b->h[i];
+            if (h->K != r.K || h->Q != r.Q) continue;
+            for (long long c0 = 0; c0 < h->base.g.J; c0 += cpb) w.push_back(WorkItem{i, 1, c0});
+        }
+        r.count = (int)w.size() - r.first;
+        b->runs[mode].push_back(r);
+    }
+    cudaFree(b->d_class_items[mode]);
+    b->d_class_items[mode] = nullptr;
+    CUDA_TRY(cudaMalloc(&b->d_class_items[mode], sizeof(WorkItem) * std::max<size_t>(w.size(), 1)));
+    CUDA_TRY(cudaMemcpy(b->d_class_items[mode], w.data(), sizeof(WorkItem) * w.size(), cudaMemcpyHostToDevice));
+    return BOSSS_OK;
+}
+
 static int batch_run(bosss_batch* b, int mode, double alpha, double beta, const double* U, const double* V, double* out,
                      double time, cudaStream_t s, int counter_slot) {
+    if (b->classes) {
+        for (const auto& r : b->runs[mode]) {
+            ClassLaunch CL = class_launcher(b->phys, mode, r.K, r.Q, r.slab);
+            if (!CL) return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no batched class kernel for this degree");
+            const bosss_handle* h0 = nullptr;
+            for (auto* h : b->h)
+                if (h->K == r.K && h->Q == r.Q) {
+                    h0 = h;
+                    break;
+                }
+            CUDA_TRY(CL(h0->base.tab, b->d_inst, b->d_class_items[mode] + r.first, r.count, U, V, out, alpha, beta,
+                        time, s));
+        }
+        return BOSSS_OK;
+    }
     BatchLaunch L = batch_launcher(b->phys, b->D, mode, b->slab[mode]);
     if (!L) return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no batched kernel for this physics");
     CUDA_TRY(L(b->d_inst, b->d_items[mode], b->nitems[mode], b->d_counter + counter_slot, U, V, out, alpha, beta, time,
@@ -386,6 +520,7 @@ int bosss_b200_batch_create(int32_t n, const bosss_op_desc* ops, const bosss_gri
     for (int m = 0; m < 3; ++m) {
         b->grid[m] = batch_grid(b->phys, m, b->slab[m]);
         int rc = build_items(b, m);
+        if (!rc) rc = build_class_items(b, m, want);
         if (rc) {
             bosss_b200_batch_destroy(b);
             return rc;
@@ -400,7 +535,10 @@ int bosss_b200_batch_destroy(bosss_batch* b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    for (int m = 0; m < 3; ++m) cudaFree(b->d_items[m]);
+    for (int m = 0; m < 3; ++m) {
+        cudaFree(b->d_items[m]);
+        cudaFree(b->d_class_items[m]);
+    }
     cudaFree(b->d_inst);
     cudaFree(b->d_counter);
     for (auto* h : b->h) bosss_b200_destroy(h);
@@ -499,7 +637,7 @@ int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double*
     CUDA_TRY(cudaSetDevice(b->device));
     // persisted table: "<key> <tiles>" per line, plus "schedule lpt|fifo"
     std::map<std::string, int> table;
-    bool have_sched = false, lpt = true;
+    bool have_sched = false, lpt = true, per_class = false;
     if (table_path && *table_path) {
         std::ifstream f(table_path);
         std::string k;
@@ -509,12 +647,14 @@ int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double*
                 std::string sv;
                 f >> sv;
                 have_sched = true;
-                lpt = (sv == "lpt");
+                lpt = (sv != "fifo");
+                per_class = (sv == "classes");
             } else if (f >> v) {
                 table[k] = v;
             }
         }
     }
+    b->classes = false;   // tiles per item are timed on the persistent queue
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
@@ -572,15 +712,24 @@ int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double*
     if (!rc) {
         if (have_sched) {
             b->lpt = lpt;
+            b->classes = per_class;
         } else {
-            float ms_l = 0.f, ms_f = 0.f;
+            // persistent queue longest-first, persistent queue in instance order, or one launch
+            // per (K, Q) class: the fastest of the three
+            float ms_l = 0.f, ms_f = 0.f, ms_c = 0.f;
             b->lpt = true;
             rc = time_once(ms_l);
             if (!rc) {
                 b->lpt = false;
                 rc = time_once(ms_f);
             }
+            if (!rc) {
+                b->classes = true;
+                rc = time_once(ms_c);
+                b->classes = false;
+            }
             b->lpt = rc ? true : (ms_l <= ms_f);
+            b->classes = !rc && ms_c < std::min(ms_l, ms_f);
         }
         for (int m = 0; m < 3 && !rc; ++m) rc = build_items(b, m);
     }
@@ -590,7 +739,7 @@ int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double*
     if (table_path && *table_path) {
         std::ofstream f(table_path);
         for (auto& kv : table) f << kv.first << " " << kv.second << "\n";
-        f << "schedule " << (b->lpt ? "lpt" : "fifo") << "\n";
+        f << "schedule " << (b->classes ? "classes" : (b->lpt ? "lpt" : "fifo")) << "\n";
     }
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
@@ -603,7 +752,7 @@ int bosss_b200_batch_tiles(const bosss_batch* b, int32_t K, int32_t Q, int32_t* 
     if (!b) return fail(BOSSS_ERR_BAD_ARG, "null batch");
     auto it = b->tiles.find({K, Q});
     if (tiles) *tiles = (it == b->tiles.end()) ? 1 : it->second;
-    if (lpt) *lpt = b->lpt ? 1 : 0;
+    if (lpt) *lpt = b->classes ? 2 : (b->lpt ? 1 : 0);
     return BOSSS_OK;
 }
 

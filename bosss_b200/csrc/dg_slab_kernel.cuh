@@ -529,7 +529,8 @@ __device__ __forceinline__ void face_project(const Tables1D& T, const double* ob
 
 // ------------------------------------------------------------------ the kernel
 template <class Phys, int K, int Q, int MODE, int PART>
-__device__ __forceinline__ void slab_volume_interp(const EvalArgs& args, const double* cin, double* wk, int o, int q,
+__device__ __forceinline__ void slab_volume_interp(const EvalArgs& args, const Tables1D& T, const double* cin, double* wk,
+                                                   int o, int q,
                                                    const double* Aq, const double* dAq) {
     using C = SlabCfg<Phys, K, Q, MODE>;
     constexpr int NP = C::NP;
@@ -538,14 +539,15 @@ __device__ __forceinline__ void slab_volume_interp(const EvalArgs& args, const d
 #pragma unroll
         for (int n = 0; n < NP; ++n) cf[n] = cin[f * NP + n];
         double* nb = wk + C::vnode(f);
-        if (f < C::NV) slab_interp<K, Q, C::G_STATE, PART, C::SPLIT>(args.tab, cf, Aq, dAq, q, args.g.scaling, args.g.twoh, nb);
-        else slab_interp<K, Q, C::G_SECOND_VOL, PART, C::SPLIT>(args.tab, cf, Aq, dAq, q, args.g.scaling, args.g.twoh, nb);
+        if (f < C::NV) slab_interp<K, Q, C::G_STATE, PART, C::SPLIT>(T, cf, Aq, dAq, q, args.g.scaling, args.g.twoh, nb);
+        else slab_interp<K, Q, C::G_SECOND_VOL, PART, C::SPLIT>(T, cf, Aq, dAq, q, args.g.scaling, args.g.twoh, nb);
     }
 }
 
 // traces of all interpolated fields at face (DIR, s): own (side 0) and neighbour (side 1)
 template <class Phys, int K, int Q, int MODE, int DIR, int S>
-__device__ __forceinline__ void slab_face_traces(const EvalArgs& args, const double* cin, double* wk, int o, int q,
+__device__ __forceinline__ void slab_face_traces(const EvalArgs& args, const Tables1D& T, const double* cin, double* wk,
+                                                 int o, int q,
                                                  const int* ijk, const double* Aq, const double* dAq) {
     using C = SlabCfg<Phys, K, Q, MODE>;
     constexpr int NP = C::NP, NV = C::NV, SLF = C::SLF;
@@ -558,8 +560,8 @@ __device__ __forceinline__ void slab_face_traces(const EvalArgs& args, const dou
 #pragma unroll
             for (int n = 0; n < NP; ++n) cf[n] = cin[f * NP + n];
             double* t0 = wk + (S * 2 + 0) * C::TRB + C::fnode(f) + q * SLF;
-            if (fg) face_interp<DIR, K, Q, GG>(args.tab, cf, S, Aq, dAq, args.g.scaling, args.g.twoh, t0);
-            else face_interp<DIR, K, Q, false>(args.tab, cf, S, Aq, dAq, args.g.scaling, args.g.twoh, t0);
+            if (fg) face_interp<DIR, K, Q, GG>(T, cf, S, Aq, dAq, args.g.scaling, args.g.twoh, t0);
+            else face_interp<DIR, K, Q, false>(T, cf, S, Aq, dAq, args.g.scaling, args.g.twoh, t0);
         }
         {   // neighbour across the face
             double cn[NP];
@@ -572,22 +574,22 @@ __device__ __forceinline__ void slab_face_traces(const EvalArgs& args, const dou
                 for (int n = 0; n < NP; ++n) cn[n] = 0.0;
             }
             double* t1 = wk + (S * 2 + 1) * C::TRB + C::fnode(f) + q * SLF;
-            if (fg) face_interp<DIR, K, Q, GG>(args.tab, cn, 1 - S, Aq, dAq, args.g.scaling, args.g.twoh, t1);
-            else face_interp<DIR, K, Q, false>(args.tab, cn, 1 - S, Aq, dAq, args.g.scaling, args.g.twoh, t1);
+            if (fg) face_interp<DIR, K, Q, GG>(T, cn, 1 - S, Aq, dAq, args.g.scaling, args.g.twoh, t1);
+            else face_interp<DIR, K, Q, false>(T, cn, 1 - S, Aq, dAq, args.g.scaling, args.g.twoh, t1);
         }
     }
 }
 
 // Evaluates the tile of cells [c0, c0 + CPB) (clipped to args.cend); the first C::NT threads
 // of the CTA do the work, any further threads only take part in the barriers (the batched
-// persistent kernel runs tiles of several degrees in CTAs of one size).
+// persistent kernel runs tiles of several degrees in CTAs of one size). T: the 1D tables,
+// passed apart from args so that a caller can keep them in the kernel-parameter bank.
 template <class Phys, int K, int Q, int MODE>
-__device__ __forceinline__ void slab_tile(const EvalArgs& args, long long c0, double* smem) {
+__device__ __forceinline__ void slab_tile(const EvalArgs& args, const Tables1D& T, long long c0, double* smem) {
     using C = SlabCfg<Phys, K, Q, MODE>;
     constexpr int NP = C::NP, NV = C::NV, NO = C::NO, CPB = C::CPB, NT = C::NT, SPLIT = C::SPLIT;
     constexpr int SLV = C::SLV, FV = C::FV, SLF = C::SLF, FF = C::FF, QF = Q * Q;
     const GridConst& g = args.g;
-    const Tables1D& T = args.tab;
     const int tid = threadIdx.x;
     const int tt = tid < NT ? tid : (1 << 30);   // start of the strided loops (threads beyond NT: none)
     const int ncell = (int)((args.cend - c0) < CPB ? (args.cend - c0) : CPB);
@@ -620,8 +622,8 @@ __device__ __forceinline__ void slab_tile(const EvalArgs& args, long long c0, do
     // ---------------------------------------------------------- volume
     constexpr int OUT0 = 0;
     if (active) {
-        if (part == 0) slab_volume_interp<Phys, K, Q, MODE, 0>(args, CIN(cl), WK(cl), o, q, Aq, dAq);
-        else if constexpr (SPLIT > 1) slab_volume_interp<Phys, K, Q, MODE, 1>(args, CIN(cl), WK(cl), o, q, Aq, dAq);
+        if (part == 0) slab_volume_interp<Phys, K, Q, MODE, 0>(args, T, CIN(cl), WK(cl), o, q, Aq, dAq);
+        else if constexpr (SPLIT > 1) slab_volume_interp<Phys, K, Q, MODE, 1>(args, T, CIN(cl), WK(cl), o, q, Aq, dAq);
     }
     __syncthreads();
     for (int it = tt; it < CPB * Q * Q * Q; it += NT) {
@@ -663,11 +665,11 @@ __device__ __forceinline__ void slab_tile(const EvalArgs& args, long long c0, do
         constexpr int OUTF0 = 2 * 2 * C::TRB;
         if (active) {
             if constexpr (SPLIT > 1) {
-                if (part == 0) slab_face_traces<Phys, K, Q, MODE, DIR, 0>(args, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
-                else slab_face_traces<Phys, K, Q, MODE, DIR, 1>(args, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
+                if (part == 0) slab_face_traces<Phys, K, Q, MODE, DIR, 0>(args, T, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
+                else slab_face_traces<Phys, K, Q, MODE, DIR, 1>(args, T, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
             } else {
-                slab_face_traces<Phys, K, Q, MODE, DIR, 0>(args, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
-                slab_face_traces<Phys, K, Q, MODE, DIR, 1>(args, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
+                slab_face_traces<Phys, K, Q, MODE, DIR, 0>(args, T, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
+                slab_face_traces<Phys, K, Q, MODE, DIR, 1>(args, T, CIN(cl), WK(cl), o, q, ijk, Aq, dAq);
             }
         }
         __syncthreads();
@@ -758,7 +760,7 @@ template <class Phys, int K, int Q, int MODE>
 __global__ void __launch_bounds__(SlabCfg<Phys, K, Q, MODE>::NT, SlabCfg<Phys, K, Q, MODE>::MINB)
 dg_slab_kernel(const __grid_constant__ EvalArgs args) {
     extern __shared__ double smem[];
-    slab_tile<Phys, K, Q, MODE>(args, args.cbeg + (long long)blockIdx.x * SlabCfg<Phys, K, Q, MODE>::CPB, smem);
+    slab_tile<Phys, K, Q, MODE>(args, args.tab, args.cbeg + (long long)blockIdx.x * SlabCfg<Phys, K, Q, MODE>::CPB, smem);
 }
 
 }  // namespace bosss

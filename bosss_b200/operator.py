@@ -570,10 +570,13 @@ class BatchEvaluator:
         C.check(C.lib().bosss_b200_batch_autotune(self.handle, C.ptr(U), C.ptr(W), C.ptr(R), C.ptr(G),
                                                   table_path.encode() if table_path else None))
 
+    SCHEDULES = {0: "fifo", 1: "lpt", 2: "classes"}
+
     def tiles(self, K, Q):
-        t, lpt = ctypes.c_int32(), ctypes.c_int32()
-        C.check(C.lib().bosss_b200_batch_tiles(self.handle, K, Q, ctypes.byref(t), ctypes.byref(lpt)))
-        return t.value, bool(lpt.value)
+        """(tiles per work item of the (K, Q) class, schedule: "lpt" | "fifo" | "classes")."""
+        t, sched = ctypes.c_int32(), ctypes.c_int32()
+        C.check(C.lib().bosss_b200_batch_tiles(self.handle, K, Q, ctypes.byref(t), ctypes.byref(sched)))
+        return t.value, BatchEvaluator.SCHEDULES[sched.value]
 
 
 class XdgEvaluator:

@@ -286,6 +286,9 @@ int bosss_b200_batch_replay(bosss_batch* b, void* stream);
  * buffers; reads/writes the text table at table_path (NULL: no persistence) */
 int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double* W_dev, double* R_dev, double* G_dev,
                               const char* table_path);
+/* The autotuned choice: tiles per work item of the (K, Q) class, and the schedule in *lpt:
+ * 1 = persistent queue longest first, 0 = persistent queue in instance order, 2 = one launch
+ * per (K, Q) class with the single-grid launch configuration. */
 int bosss_b200_batch_tiles(const bosss_batch* b, int32_t K, int32_t Q, int32_t* tiles, int32_t* lpt);
 
 /* ---- XDG: per-species bulk evaluation with moment-fitted cut-cell rules ----

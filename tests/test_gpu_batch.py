@@ -71,3 +71,36 @@ def test_batch_graph_replay_and_autotune(tmp_path):
     with O.BatchEvaluator(probs) as b2:
         b2.autotune(U, W, R, G, table)
         assert {kq: b2.tiles(*kq) for kq in tiles} == tiles
+
+
+@pytest.mark.parametrize("schedule", ["classes", "lpt", "fifo"])
+def test_batch_schedules_match_single_instances(tmp_path, schedule):
+    """Each schedule (persisted in the autotuner's table) gives the single-instance results."""
+    import torch
+    probs = small_batch()
+    U = torch.from_numpy(np.concatenate([p.U for p in probs])).cuda()
+    W = torch.from_numpy(np.random.default_rng(4).uniform(-1, 1, U.numel())).cuda()
+    R = torch.zeros_like(U)
+    G = torch.zeros_like(U)
+    table = tmp_path / "tiles.txt"
+    table.write_text("schedule %s\n" % schedule)
+    with O.BatchEvaluator(probs) as b:
+        b.autotune(U, W, R, G, str(table))
+        assert b.tiles(1, 2)[1] == schedule
+        Rb = b.evaluate(C.MODE_RESIDUAL, U)
+        JV = b.evaluate(C.MODE_JVP, U, W)
+        Gb = b.evaluate(C.MODE_VJP, U, W)
+        torch.cuda.synchronize()
+        off = b.dom_offsets
+    for i, p in enumerate(probs):
+        sl = slice(int(off[i]), int(off[i + 1]))
+        Ui, Wi = U[sl], W[sl]
+        with p.evaluator() as ev:
+            Rs = torch.zeros_like(Ui)
+            ev.Evaluate(1.0, 0.0, Rs, Ui)
+            JVs = ev.jvp(Ui, Wi)
+            Gs = ev.vjp(Ui, Wi)
+            torch.cuda.synchronize()
+        assert rel(Rb[sl].cpu().numpy(), Rs.cpu().numpy()) <= 1e-13
+        assert rel(JV[sl].cpu().numpy(), JVs.cpu().numpy()) <= 1e-13
+        assert rel(Gb[sl].cpu().numpy(), Gs.cpu().numpy()) <= 1e-13
