@@ -10,9 +10,10 @@ product J(U)^T W at the same state; DOF-updates per step = 2 x 3,276,800.
   launching stream around each step; L2 (126 MB) is flushed between steps by
   writing a 512 MB buffer outside the timed events (the working set, 105 MB,
   would otherwise stay L2-resident).
-* ``e2e``: the same steps through the host-buffer C-ABI entry points
-  (bosss_b200_evaluate / bosss_b200_vjp) from pinned host memory: every call copies
-  its inputs host->device and its result device->host inside the timed region.
+* ``e2e``: the same steps through the host-buffer C-ABI entry point
+  bosss_b200_residual_vjp from pinned host memory: every step copies U and W host->device
+  and R and J^T W device->host inside the timed region (streamed by chunks of x-planes,
+  overlapped with the evaluation).
 * ``roofline``: the residual kernel (the dominant launch) -- algorithmic bytes
   (8 B x (inputs + outputs)) over its CUDA-event duration, against the measured HBM
   copy bandwidth; the FP64 pipe figure is reported beside it (nominal peak).
@@ -645,16 +646,16 @@ def main():
     Wh = torch.from_numpy(W.cpu().numpy()).pin_memory()
     Rh = torch.zeros(n, dtype=torch.float64).pin_memory()
     Gh = torch.zeros(n, dtype=torch.float64).pin_memory()
+    # one host call per step: residual and VJP at the same state, U and W uploaded once,
+    # transfers streamed by chunks of x-planes and overlapped with the evaluation
     for _ in range(2):
-        C.check(L.bosss_b200_evaluate(h, 1.0, 0.0, C.ptr(Uh), C.ptr(Rh), 0.0))
-        C.check(L.bosss_b200_vjp(h, C.ptr(Uh), C.ptr(Wh), C.ptr(Gh), 0.0))
+        C.check(L.bosss_b200_residual_vjp(h, 1.0, 0.0, C.ptr(Uh), C.ptr(Rh), C.ptr(Wh), C.ptr(Gh), 0.0))
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for i in range(args.steps):
-        C.check(L.bosss_b200_evaluate(h, 1.0, 0.0, C.ptr(Uh), C.ptr(Rh), 0.0))
-        C.check(L.bosss_b200_vjp(h, C.ptr(Uh), C.ptr(Wh), C.ptr(Gh), 0.0))
+        C.check(L.bosss_b200_residual_vjp(h, 1.0, 0.0, C.ptr(Uh), C.ptr(Rh), C.ptr(Wh), C.ptr(Gh), 0.0))
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if world > 1:
@@ -662,8 +663,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e = world * DOF_PER_STEP_FACTOR * n * args.steps / e2e_s
-    # residual: U in, R out; vjp: U and W in, result out
-    h2d = 8 * (n + 2 * n)
+    # U and W in, R and J^T W out
+    h2d = 8 * (n + n)
     d2h = 8 * (n + n)
     # the host-buffer path must agree with the device-resident one
     assert np.allclose(Rh.numpy(), R.cpu().numpy(), rtol=0, atol=0)

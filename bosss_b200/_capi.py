@@ -197,6 +197,8 @@ SIGNATURES = {
                                                       ctypes.c_double, _P]),
     "bosss_b200_batch_evaluate_noalloc": (ctypes.c_int, [ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_double,
                                                          ctypes.c_double, _P, _P, _P, ctypes.c_double, _P]),
+    "bosss_b200_residual_vjp": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _P, _P, _P, _P,
+                                               ctypes.c_double]),
     "bosss_b200_apply_device": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_double, _P, _P, _P,
                                                ctypes.c_double, ctypes.c_int64, ctypes.c_int64, _P]),
     "bosss_b200_rk_work_size": (ctypes.c_int, [_P, ctypes.c_int32, _I64]),

@@ -498,6 +498,13 @@ int bosss_b200_destroy(bosss_handle* h) {
     cudaFree(h->dV);
     cudaFree(h->dOut);
     cudaFree(h->dFlag);
+    cudaFree(h->dOut2);
+    for (int c = 0; c < bosss_handle::MAX_CHUNKS; ++c) {
+        if (h->ev_in[c]) cudaEventDestroy(h->ev_in[c]);
+        if (h->ev_done[c]) cudaEventDestroy(h->ev_done[c]);
+    }
+    if (h->s_in) cudaStreamDestroy(h->s_in);
+    if (h->s_out) cudaStreamDestroy(h->s_out);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return BOSSS_OK;
@@ -545,21 +552,118 @@ int bosss_b200_apply_device(bosss_handle* h, int32_t mode, double alpha, double 
     return BOSSS_OK;
 }
 
+// Host-buffer evaluation pipelined over chunks of planes of the slowest-varying grid direction
+// (the cells of a plane are contiguous in both cell orders): the inputs stream in on one copy
+// stream, each chunk's cells are evaluated on the handle's stream as soon as its planes and the
+// first plane of the next chunk have arrived (the face neighbours; the last plane comes first
+// when that direction is periodic), and each chunk's outputs stream out on a second copy stream
+// while later chunks are still computing. Small problems, and the opt-in NaN check, run as one
+// chunk. Returns after the last output has reached the host.
+struct HostJob {
+    int mode;
+    double alpha, beta;
+    double* Y;     // host output
+    double* dY;    // device staging of the output
+};
+
+static int host_pipelined(bosss_handle* h, const HostJob* jobs, int njobs, const double* U, const double* X,
+                          double time) {
+    int rc = ensure_staging(h);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(h->device));
+    const GridConst& g = h->base.g;
+    const long long J = g.J;
+    const int sd = (g.stride[0] >= g.stride[g.D - 1]) ? 0 : g.D - 1;   // slowest direction
+    const long long planes = g.n[sd], pc = J / planes;                 // cells per plane
+    const long long nU = h->ndom / J;                                  // DOFs per cell
+    long long nX = 0;
+    for (int k = 0; k < njobs; ++k)
+        if (jobs[k].mode != MODE_RES) nX = (jobs[k].mode == MODE_JVP) ? h->ndom / J : h->ncod / J;
+    auto nY = [&](const HostJob& jb) { return (jb.mode == MODE_VJP ? h->ndom : h->ncod) / J; };
+    auto y_in = [&](const HostJob& jb) { return jb.mode == MODE_RES && jb.beta != 0.0; };
+    size_t bytes = sizeof(double) * (size_t)J * (nU + (X ? nX : 0));
+    for (int k = 0; k < njobs; ++k) bytes += sizeof(double) * (size_t)J * nY(jobs[k]);
+    int nch = (int)std::min<long long>(bosss_handle::MAX_CHUNKS / 2, planes / 2);
+    if (bytes < (size_t)16 << 20 || h->check_nan) nch = 1;
+    if (nch < 1) nch = 1;
+    if (!h->s_in) CUDA_TRY(cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking));
+    if (!h->s_out) CUDA_TRY(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking));
+    for (int c = 0; c < nch; ++c) {
+        if (!h->ev_in[c]) CUDA_TRY(cudaEventCreateWithFlags(&h->ev_in[c], cudaEventDisableTiming));
+        if (!h->ev_done[c]) CUDA_TRY(cudaEventCreateWithFlags(&h->ev_done[c], cudaEventDisableTiming));
+    }
+    cudaStream_t s = h->stream, si = h->s_in, so = h->s_out;
+    auto first_plane = [&](int c) { return (long long)c * planes / nch; };
+    auto copy_in = [&](long long p0, long long p1) -> cudaError_t {
+        const long long c0 = p0 * pc, n = (p1 - p0) * pc;
+        cudaError_t e = cudaMemcpyAsync(h->dU + c0 * nU, U + c0 * nU, sizeof(double) * n * nU, cudaMemcpyHostToDevice, si);
+        if (e == cudaSuccess && X)
+            e = cudaMemcpyAsync(h->dV + c0 * nX, X + c0 * nX, sizeof(double) * n * nX, cudaMemcpyHostToDevice, si);
+        for (int k = 0; k < njobs && e == cudaSuccess; ++k)
+            if (y_in(jobs[k])) {
+                const long long m = nY(jobs[k]);
+                e = cudaMemcpyAsync(jobs[k].dY + c0 * m, jobs[k].Y + c0 * m, sizeof(double) * n * m,
+                                    cudaMemcpyHostToDevice, si);
+            }
+        return e;
+    };
+    auto finish = [&](int code) {
+        cudaStreamSynchronize(si);
+        cudaStreamSynchronize(s);
+        cudaStreamSynchronize(so);
+        return code;
+    };
+    // the copy streams start after whatever the handle's stream has pending
+    CUDA_TRY(cudaEventRecord(h->ev_done[0], s));
+    CUDA_TRY(cudaStreamWaitEvent(si, h->ev_done[0], 0));
+    CUDA_TRY(cudaStreamWaitEvent(so, h->ev_done[0], 0));
+    cudaError_t e = cudaSuccess;
+    if (nch > 1 && g.periodic[sd]) e = copy_in(planes - 1, planes);
+    for (int c = 0; c < nch && e == cudaSuccess; ++c) {
+        e = copy_in(first_plane(c), first_plane(c + 1));
+        if (e == cudaSuccess) e = cudaEventRecord(h->ev_in[c], si);
+    }
+    if (e != cudaSuccess) return finish(fail(BOSSS_ERR_CUDA, cudaGetErrorString(e)));
+    for (int c = 0; c < nch; ++c) {
+        e = cudaStreamWaitEvent(s, h->ev_in[std::min(c + 1, nch - 1)], 0);
+        for (int k = 0; k < njobs && e == cudaSuccess; ++k) {
+            EvalArgs a = h->base;
+            a.U = h->dU;
+            a.V = jobs[k].mode != MODE_RES ? h->dV : nullptr;
+            a.out = jobs[k].dY;
+            a.alpha = jobs[k].alpha;
+            a.beta = jobs[k].beta;
+            a.time = time;
+            a.cbeg = first_plane(c) * pc;
+            a.cend = first_plane(c + 1) * pc;
+            e = h->kern[jobs[k].mode].launch(a, s);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(h->ev_done[c], s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(so, h->ev_done[c], 0);
+        for (int k = 0; k < njobs && e == cudaSuccess; ++k) {
+            const long long c0 = first_plane(c) * pc, n = (first_plane(c + 1) - first_plane(c)) * pc, m = nY(jobs[k]);
+            e = cudaMemcpyAsync(jobs[k].Y + c0 * m, jobs[k].dY + c0 * m, sizeof(double) * n * m, cudaMemcpyDeviceToHost,
+                                so);
+        }
+        if (e != cudaSuccess) return finish(fail(BOSSS_ERR_CUDA, cudaGetErrorString(e)));
+    }
+    if (h->check_nan)
+        for (int k = 0; k < njobs; ++k) {
+            rc = check_nan(h, jobs[k].dY, nY(jobs[k]) * J, s);
+            if (rc) return finish(rc);
+        }
+    e = cudaStreamSynchronize(so);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return finish(fail(BOSSS_ERR_CUDA, cudaGetErrorString(e)));
+    return BOSSS_OK;
+}
+
 int bosss_b200_evaluate(bosss_handle* h, double alpha, double beta, const double* U, double* out, double time) {
     if (!h || !U || !out) return fail(BOSSS_ERR_BAD_ARG, "null argument");
     int rc = ensure_staging(h);
     if (rc) return rc;
-    CUDA_TRY(cudaSetDevice(h->device));
-    cudaStream_t s = h->stream;
-    CUDA_TRY(cudaMemcpyAsync(h->dU, U, sizeof(double) * h->ndom, cudaMemcpyHostToDevice, s));
-    if (beta != 0.0) CUDA_TRY(cudaMemcpyAsync(h->dOut, out, sizeof(double) * h->ncod, cudaMemcpyHostToDevice, s));
-    rc = run_mode(h, MODE_RES, alpha, beta, h->dU, nullptr, h->dOut, time, s);
-    if (rc) return rc;
-    rc = check_nan(h, h->dOut, h->ncod, s);
-    if (rc) return rc;
-    CUDA_TRY(cudaMemcpyAsync(out, h->dOut, sizeof(double) * h->ncod, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    return BOSSS_OK;
+    const HostJob job{MODE_RES, alpha, beta, out, h->dOut};
+    return host_pipelined(h, &job, 1, U, nullptr, time);
 }
 
 int bosss_b200_jvp_device(bosss_handle* h, const double* U_dev, const double* V_dev, double* JV_dev, double time,
@@ -580,17 +684,8 @@ static int host_pair(bosss_handle* h, int mode, const double* U, const double* X
     if (!h || !U || !X || !Y) return fail(BOSSS_ERR_BAD_ARG, "null argument");
     int rc = ensure_staging(h);
     if (rc) return rc;
-    CUDA_TRY(cudaSetDevice(h->device));
-    cudaStream_t s = h->stream;
-    const int64_t nx = (mode == MODE_JVP) ? h->ndom : h->ncod;
-    const int64_t ny = (mode == MODE_JVP) ? h->ncod : h->ndom;
-    CUDA_TRY(cudaMemcpyAsync(h->dU, U, sizeof(double) * h->ndom, cudaMemcpyHostToDevice, s));
-    CUDA_TRY(cudaMemcpyAsync(h->dV, X, sizeof(double) * nx, cudaMemcpyHostToDevice, s));
-    rc = run_mode(h, mode, 1.0, 0.0, h->dU, h->dV, h->dOut, time, s);
-    if (rc) return rc;
-    CUDA_TRY(cudaMemcpyAsync(Y, h->dOut, sizeof(double) * ny, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    return BOSSS_OK;
+    const HostJob job{mode, 1.0, 0.0, Y, h->dOut};
+    return host_pipelined(h, &job, 1, U, X, time);
 }
 
 int bosss_b200_jvp(bosss_handle* h, const double* U, const double* V, double* JV, double time) {
@@ -599,6 +694,16 @@ int bosss_b200_jvp(bosss_handle* h, const double* U, const double* V, double* JV
 
 int bosss_b200_vjp(bosss_handle* h, const double* U, const double* W, double* JTW, double time) {
     return host_pair(h, MODE_VJP, U, W, JTW, time);
+}
+
+int bosss_b200_residual_vjp(bosss_handle* h, double alpha, double beta, const double* U, double* R, const double* W,
+                            double* JTW, double time) {
+    if (!h || !U || !R || !W || !JTW) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    int rc = ensure_staging(h);
+    if (rc) return rc;
+    if (!h->dOut2) CUDA_TRY(cudaMalloc(&h->dOut2, sizeof(double) * std::max<int64_t>(h->ndom, 1)));
+    const HostJob jobs[2] = {{MODE_RES, alpha, beta, R, h->dOut}, {MODE_VJP, 1.0, 0.0, JTW, h->dOut2}};
+    return host_pipelined(h, jobs, 2, U, W, time);
 }
 
 int bosss_b200_synchronize(bosss_handle* h) {

@@ -21,7 +21,12 @@ struct bosss_handle {
     double* dU = nullptr;
     double* dV = nullptr;
     double* dOut = nullptr;
+    double* dOut2 = nullptr;   // second output of the combined residual + VJP entry point
     int* dFlag = nullptr;
+    // copy streams and chunk events of the pipelined host-buffer entry points
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    static constexpr int MAX_CHUNKS = 16;
+    cudaEvent_t ev_in[MAX_CHUNKS]{}, ev_done[MAX_CHUNKS]{};
 };
 
 struct bosss_bsr {

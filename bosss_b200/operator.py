@@ -488,6 +488,17 @@ class Evaluator:
         C.check(C.lib().bosss_b200_newton_solve(self.handle, C.ptr(U), self.time, ctypes.byref(o), ctypes.byref(r)))
         return U, _report(r)
 
+    def residual_vjp(self, U, W, R=None, G=None, alpha=1.0, beta=0.0):
+        """Host arrays: ``R = beta*R + alpha*Op(U)`` and ``G = J(U)^T W`` in one pipelined call
+        (U and W cross PCIe once). Returns (R, G)."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        R = np.zeros(self.n_codomain) if R is None else R
+        G = np.empty(self.n_domain) if G is None else G
+        C.check(C.lib().bosss_b200_residual_vjp(self.handle, alpha, beta, C.ptr(U), C.ptr(R), C.ptr(W), C.ptr(G),
+                                                self.time))
+        return R, G
+
     def vjp(self, U, W, out=None):
         """J(U)^T W (adjoint product)."""
         if self._is_cuda(U):

@@ -172,7 +172,9 @@ int bosss_b200_get_sizes(const bosss_handle* h, int64_t* n_domain_dofs, int64_t*
                          int32_t* quad_nodes_1d);
 
 /* EvaluatorNonLin.Evaluate (DifferentialOperator.cs:1584-1661):
- *   out = beta*out + alpha*Op(U),  host buffers (copies in and out inside the call). */
+ *   out = beta*out + alpha*Op(U),  host buffers (copies in and out inside the call; above
+ *   16 MB they stream by chunks of planes of the slowest grid direction on two copy streams,
+ *   overlapped with the evaluation of the chunks whose neighbour planes have arrived). */
 int bosss_b200_evaluate(bosss_handle* h, double alpha, double beta, const double* U,
                         double* out, double time);
 /* Same, device-resident buffers (U, out are device pointers), enqueued on `stream`
@@ -187,6 +189,14 @@ int bosss_b200_jvp(bosss_handle* h, const double* U, const double* V, double* JV
  * EvaluatorLinear.ComputeMatrix / FDJacobianBuilder assemble, DifferentialOperator.cs:1740-1838,
  * 2558-2858). Host buffers. */
 int bosss_b200_vjp(bosss_handle* h, const double* U, const double* W, double* JTW, double time);
+/* Residual and adjoint product at the same state in one call, host buffers:
+ * R = beta*R + alpha*Op(U) and JTW = J(U)^T W. U and W cross PCIe once for both products;
+ * like the single-product host entry points, inputs and outputs stream by chunks of grid
+ * planes, overlapped with the evaluation (residual + adjoint pair of an adjoint-based
+ * optimisation step; in the reference, EvaluatorNonLin.Evaluate plus the transpose of
+ * EvaluatorLinear.ComputeMatrix applied to W, DifferentialOperator.cs:1584-1661, 1766-1838). */
+int bosss_b200_residual_vjp(bosss_handle* h, double alpha, double beta, const double* U, double* R, const double* W,
+                            double* JTW, double time);
 int bosss_b200_jvp_device(bosss_handle* h, const double* U_dev, const double* V_dev, double* JV_dev,
                           double time, void* stream);
 int bosss_b200_vjp_device(bosss_handle* h, const double* U_dev, const double* W_dev, double* JTW_dev,

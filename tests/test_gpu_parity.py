@@ -332,3 +332,39 @@ def test_block_sparse_spmv_matches_dense():
         assert np.array_equal(v2, vals)
     finally:
         C.lib().bosss_b200_bsr_destroy(A)
+
+
+@pytest.mark.parametrize("case", ["euler_32", "sip_48_dirichlet", "advdiff_globalid"])
+def test_host_pipeline_matches_device_path(case):
+    """The host-buffer entry points stream their inputs and outputs by chunks of planes; the
+    results equal the device-resident entry points' (residual with alpha/beta, JVP, VJP)."""
+    import torch
+    if case == "euler_32":
+        pr = P.euler3d(n=32, k=3, seed=2000)
+    elif case == "sip_48_dirichlet":
+        pr = P.nonlinear_diffusion3d(n=48, k=2, seed=3000, source=1.0)
+    else:
+        n = 40
+        g = O.Cartesian3DGrid(*[np.linspace(0, 1, n + 1)] * 3, True, False, True, cell_order=C.CELLS_GLOBALID)
+        base = P.advection_diffusion3d(n=4, k=3, seed=5)
+        U = np.random.default_rng(6).uniform(-1, 1, g.NoOfCells * O.np_of(3, 3))
+        pr = P.Problem("advdiff_gid", base.op, g, [O.DGField(g, 3, "u")], [O.DGField(g, 3, "R")], U, {})
+    r = np.random.default_rng(12)
+    V = r.uniform(-1, 1, pr.n_dofs)
+    out0 = r.uniform(-1, 1, pr.n_dofs)
+    with pr.evaluator() as ev:
+        host_r = out0.copy()
+        ev.Evaluate(0.5, -1.5, host_r, pr.U)
+        host_jv = ev.jvp(pr.U, V)
+        host_g = ev.vjp(pr.U, V)
+        Ud, Vd = torch.from_numpy(pr.U).cuda(), torch.from_numpy(V).cuda()
+        dev_r = torch.from_numpy(out0).cuda()
+        ev.Evaluate(0.5, -1.5, dev_r, Ud)
+        dev_jv = ev.jvp(Ud, Vd)
+        dev_g = ev.vjp(Ud, Vd)
+        torch.cuda.synchronize()
+    with pr.evaluator() as ev:
+        comb_r, comb_g = ev.residual_vjp(pr.U, V, R=out0.copy(), alpha=0.5, beta=-1.5)
+    for a, b in ((host_r, dev_r), (host_jv, dev_jv), (host_g, dev_g), (comb_r, dev_r), (comb_g, dev_g)):
+        b = b.cpu().numpy()
+        assert np.max(np.abs(a - b)) <= 1e-14 * np.max(np.abs(b))
