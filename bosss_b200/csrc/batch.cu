@@ -396,8 +396,7 @@ static int build_class_items(bosss_batch* b, int mode, int want) {
         bosss_batch::ClassRun r;
         r.K = kq.first;
         r.Q = kq.second;
-        r.slab = want != 1 && batch_ok(b->phys, mode, r.K, r.Q, true) &&
-                 (want == 2 || r.Q <= (mode == MODE_JVP ? 4 : 5));
+        r.slab = want != 1 && batch_ok(b->phys, mode, r.K, r.Q, true) && (want == 2 || r.Q <= 5);
         r.first = (int)w.size();
         const int cpb = batch_cpb(b->phys, mode, r.K, r.Q, r.slab);
         for (int i = 0; i < b->n; ++i) {
@@ -488,14 +487,14 @@ int bosss_b200_batch_create(int32_t n, const bosss_op_desc* ops, const bosss_gri
         return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "batched path: 3D scalar transport / advection-diffusion only");
     }
     // tile kernel per mode (the single-grid rule, measured on B200): slab tiles when every
-    // instance has at most 5 (residual, VJP) / 4 (JVP) nodes per direction; kernel selector 1
+    // instance has at most 5 nodes per direction; kernel selector 1
     // keeps the generic tiles, 2 asks for slab tiles wherever the batch allows them
     const int want = opt ? opt->kernel : 0;
     for (int m = 0; m < 3; ++m) {
         bool ok = want != 1;
         for (auto* h : b->h) {
             ok = ok && batch_ok(b->phys, m, h->K, h->Q, true);
-            if (want == 0) ok = ok && h->Q <= (m == MODE_JVP ? 4 : 5);
+            if (want == 0) ok = ok && h->Q <= 5;
         }
         b->slab[m] = ok;
     }

@@ -395,13 +395,13 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
         have_generic = have_generic && reg.count(KernelKey(phys, D, K, Q, m, VARIANT_GENERIC));
     }
     if (want == 2 && !have_slab) return fail(BOSSS_ERR_BAD_ARG, "no slab kernel for this operator");
-    // automatic choice per mode, measured on B200 (32^3 / 48^3 grids): the slab kernel for 3D
-    // systems (Euler, 3-6x); for the scalar family (one field, Q threads per cell) the slab
-    // residual and VJP up to 5 nodes per direction (1.1-1.7x faster), the slab JVP up to 4
-    // (beyond, the generic tile is faster: up to 2x with 7 or 9 nodes)
+    // automatic choice per mode, measured on B200 (16^3-48^3 grids): the slab kernel for 3D
+    // systems (Euler, 3-6x); for the scalar family (two threads per node row) the slab residual
+    // at every rule (1.1-1.7x faster) and the slab JVP / VJP up to 5 nodes per direction
+    // (1.2-1.6x faster; with 7 or 9 nodes the generic tile is 1.4-1.5x faster)
     int mode_variant[3];
     for (int m = 0; m < 3; ++m) {
-        const bool slab_pays = phys == PHYS_EULER || Q <= (m == MODE_JVP ? 4 : 5);
+        const bool slab_pays = phys == PHYS_EULER || m == MODE_RES || Q <= 5;
         mode_variant[m] = (want == 2 || (want == 0 && have_slab && slab_pays)) ? VARIANT_SLAB : VARIANT_GENERIC;
     }
     bool need_generic = false;

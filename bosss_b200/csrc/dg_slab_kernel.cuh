@@ -50,7 +50,12 @@ struct SlabCfg {
 #ifndef BOSSS_SLAB_SPLIT_VJP
 #define BOSSS_SLAB_SPLIT_VJP 2
 #endif
-    static constexpr int SPLIT = (MODE == MODE_VJP && Q >= 3) ? BOSSS_SLAB_SPLIT_VJP : 1;
+#ifndef BOSSS_SLAB_SPLIT_SCALAR
+#define BOSSS_SLAB_SPLIT_SCALAR 2
+#endif
+    static constexpr int SPLIT = (Q < 3) ? 1
+                                 : (MODE == MODE_VJP) ? BOSSS_SLAB_SPLIT_VJP
+                                 : (Phys::NV == 1) ? BOSSS_SLAB_SPLIT_SCALAR : 1;
     static constexpr int TPC = NO * Q * SPLIT;     // threads per cell
     static constexpr int NODEV = (NV * NCI0 + NF1 * NCI1V) * FV;   // interpolated node values
     static constexpr int S_CIN = NFI * NP;

@@ -272,7 +272,7 @@ int bosss_b200_compute_jacobian(bosss_handle* h, const double* U, double time, b
  * into a CUDA graph and replayed; an autotuner picks the cell tiles per work item for each
  * (degree, quadrature nodes) class and the queue order, persisted in a small text table.
  * Tile kernel per mode (opt->kernel): 0 = automatic (register-blocked slab tiles when every
- * instance has at most 5 nodes per direction, 4 for the JVP; else the generic tiles),
+ * instance has at most 5 nodes per direction; else the generic tiles),
  * 1 = generic tiles, 2 = slab tiles wherever every instance allows them. */
 typedef struct bosss_batch bosss_batch;
 
