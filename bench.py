@@ -14,7 +14,7 @@ product J(U)^T W at the same state; DOF-updates per step = 2 x 3,276,800.
   bosss_b200_residual_vjp from pinned host memory: every step copies U and W host->device
   and R and J^T W device->host inside the timed region (streamed by chunks of x-planes,
   overlapped with the evaluation).
-* ``roofline``: the residual kernel (the dominant launch) -- algorithmic bytes
+* ``roofline``: the VJP kernel (the dominant launch) -- algorithmic bytes
   (8 B x (inputs + outputs)) over its CUDA-event duration, against the measured HBM
   copy bandwidth; the FP64 pipe figure is reported beside it (nominal peak).
 * ``cpu_baseline``: the CPU FP64 oracle (a C++/OpenMP restatement of the reference
