@@ -195,6 +195,11 @@ SIGNATURES = {
                                                ctypes.c_double]),
     "bosss_b200_xdg_evaluate_device": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_double, _P, _P,
                                                       ctypes.c_double, _P]),
+    "bosss_b200_xdg_interface_setup": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                      ctypes.c_int32, ctypes.c_int32]),
+    "bosss_b200_xdg_interface_get_rules": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "bosss_b200_xdg_interface_evaluate": (ctypes.c_int, [_P, ctypes.c_double, _P, _P, _P, _P]),
+    "bosss_b200_xdg_interface_evaluate_device": (ctypes.c_int, [_P, ctypes.c_double, _P, _P, _P, _P, _P]),
     "bosss_b200_batch_evaluate_noalloc": (ctypes.c_int, [ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_double,
                                                          ctypes.c_double, _P, _P, _P, ctypes.c_double, _P]),
     "bosss_b200_residual_vjp": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _P, _P, _P, _P,

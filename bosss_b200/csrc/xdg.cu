@@ -536,6 +536,190 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
     }
 }
 
+// ------------------------------------------------------------------ level-set interface term
+// XLaplace_Interface.InnerEdgeForm (XNSECommon/XLaplace.cs:229-297) integrated over the sphere
+// surface inside each cut cell, scattered into both species' rows of the cell as
+// NECQuadratureLevelSet.SaveIntegrationResults does (NECQuadratureLevelSet.cs:622-661): the form
+// with (vA, vB) = (phi_n, 0) goes to species A, with (0, phi_n) to species B, both added. The
+// normal is the level-set normal grad(phi)/|grad(phi)|, pointing from A (phi < 0) to B.
+// One block per cut cell; every cell occurs once, so the block adds its sums without atomics.
+struct IfaceArgs {
+    double muA, muB;     // species diffusivities
+    double omA, omB;     // flux weights (SIP 1/2, 1/2; SWIP muB/(muA+muB), muA/(muA+muB))
+    double pen;          // penalty_base * penalty_deg * penalty_muFactor (times 1/length scale per cell)
+    double alpha;
+};
+
+template <int K>
+__global__ void k_interface_eval(const long long* __restrict__ cells, const long long* __restrict__ node_off,
+                                 const double* __restrict__ nodes, const double* __restrict__ weights,
+                                 const double* __restrict__ normals, int ncells, GridConst g, IfaceArgs f,
+                                 const double* __restrict__ UA, const double* __restrict__ UB, double* outA,
+                                 double* outB) {
+    constexpr int NP = np_of(3, K);
+    const int r = blockIdx.x;
+    if (r >= ncells) return;
+    const long long cell = cells[r];
+    __shared__ double cA[NP], cB[NP], RA[NP], RB[NP];
+    for (int n = threadIdx.x; n < NP; n += blockDim.x) {
+        cA[n] = UA[cell * NP + n];
+        cB[n] = UB[cell * NP + n];
+        RA[n] = 0.0;
+        RB[n] = 0.0;
+    }
+    __syncthreads();
+    int ijk[3];
+    cell_ijk(g, cell, ijk);
+    const double pen = f.pen * cell_cj(g, ijk);
+    const double sc = g.scaling;
+    double rA[NP], rB[NP];
+    for (int n = 0; n < NP; ++n) rA[n] = rB[n] = 0.0;
+    const long long j0 = node_off[r], j1 = node_off[r + 1];
+    for (long long j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        const double* xi = nodes + 3 * j;
+        const double* N = normals + 3 * j;
+        double L[3][K + 1], dL[3][K + 1];
+        for (int d = 0; d < 3; ++d) legendre_vals(K, xi[d], L[d], dL[d]);
+        double ph[NP], gn[NP];   // basis value and normal derivative (physical, without sc)
+        double uA = 0.0, uB = 0.0, gA = 0.0, gB = 0.0;
+        {
+            int nn = 0;
+            for (int deg = 0; deg <= K; ++deg)
+                for (int aa = 0; aa <= deg; ++aa)
+                    for (int bb = 0; bb <= deg - aa; ++bb) {
+                        const int cc = deg - aa - bb;
+                        ph[nn] = L[0][aa] * L[1][bb] * L[2][cc];
+                        gn[nn] = dL[0][aa] * L[1][bb] * L[2][cc] * g.twoh[0] * N[0] +
+                                 L[0][aa] * dL[1][bb] * L[2][cc] * g.twoh[1] * N[1] +
+                                 L[0][aa] * L[1][bb] * dL[2][cc] * g.twoh[2] * N[2];
+                        uA += cA[nn] * ph[nn];
+                        uB += cB[nn] * ph[nn];
+                        gA += cA[nn] * gn[nn];
+                        gB += cB[nn] * gn[nn];
+                        ++nn;
+                    }
+        }
+        uA *= sc;
+        uB *= sc;
+        gA *= sc;
+        gB *= sc;
+        const double jump = uA - uB;
+        const double flux = f.muA * f.omA * gA + f.muB * f.omB * gB - pen * jump;
+        const double w = weights[j] * sc;
+        const double symA = f.muA * f.omA * jump, symB = f.muB * f.omB * jump;
+        for (int n = 0; n < NP; ++n) {
+            rA[n] += w * (flux * ph[n] + symA * gn[n]);
+            rB[n] += w * (-flux * ph[n] + symB * gn[n]);
+        }
+    }
+    for (int n = 0; n < NP; ++n) {
+        atomicAdd(&RA[n], rA[n]);
+        atomicAdd(&RB[n], rB[n]);
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < NP; n += blockDim.x) {
+        outA[cell * NP + n] += f.alpha * RA[n];
+        outB[cell * NP + n] += f.alpha * RB[n];
+    }
+}
+
+// Surface rule of the sphere |x - c| = R inside the box [lo, hi] (physical coordinates), by
+// height-function quadrature with analytic roots (the approach of Saye's high-order rules,
+// Quadrature/SayeGaussRule_*.cs, specialised to the quadric): a height direction m with c_m
+// outside [lo_m, hi_m] makes the surface one graph x_m = c_m + s sqrt(R^2 - rho^2) over the base
+// plane (a, b); the inner integral over b runs over the intervals where the root lies in the box,
+// the outer integral over a is split where those intervals change shape, and each outer piece is
+// mapped by a = a0 + (a1 - a0)(3u^2 - 2u^3) so that square-root behaviour at its ends becomes
+// smooth. dS = R / |x_m - c_m| dA. Boxes with no admissible height direction are halved in every
+// direction. Appends (x[3], w, n[3]) per node.
+static void sphere_surface_box(const double* lo, const double* hi, const double* c, double R,
+                               const std::vector<double>& gx, const std::vector<double>& gw, int depth,
+                               std::vector<double>& out) {
+    LevelSetDev L{};
+    L.type = BOSSS_LEVELSET_SPHERE;
+    for (int d = 0; d < 3; ++d) L.c[d] = c[d];
+    L.r = R;
+    if (ls_box(L, lo, hi, 7) != 0) return;
+    int m = -1;
+    double best = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        const double dist = std::max(lo[d] - c[d], c[d] - hi[d]);
+        if (dist > best) {
+            best = dist;
+            m = d;
+        }
+    }
+    if (m < 0) {
+        if (depth >= 6) return;
+        double mid[3];
+        for (int d = 0; d < 3; ++d) mid[d] = 0.5 * (lo[d] + hi[d]);
+        for (int q = 0; q < 8; ++q) {
+            double l2[3], h2[3];
+            for (int d = 0; d < 3; ++d) {
+                const bool up = (q >> d) & 1;
+                l2[d] = up ? mid[d] : lo[d];
+                h2[d] = up ? hi[d] : mid[d];
+            }
+            sphere_surface_box(l2, h2, c, R, gx, gw, depth + 1, out);
+        }
+        return;
+    }
+    const int a = (m == 0) ? 1 : 0, b = (m == 2) ? 1 : 2;
+    const double s = (lo[m] > c[m]) ? 1.0 : -1.0;
+    const double dlo = best;
+    const double dhi = std::max(std::fabs(lo[m] - c[m]), std::fabs(hi[m] - c[m]));
+    // break points of the outer direction
+    std::vector<double> br = {lo[a], hi[a]};
+    const double ds[2] = {dlo, dhi};
+    const double es[3] = {lo[b] - c[b], hi[b] - c[b], 0.0};
+    for (double dd : ds)
+        for (double ee : es) {
+            const double q = R * R - dd * dd - ee * ee;
+            if (q <= 0.0) continue;
+            const double t = std::sqrt(q);
+            for (double xa : {c[a] - t, c[a] + t})
+                if (xa > lo[a] && xa < hi[a]) br.push_back(xa);
+        }
+    std::sort(br.begin(), br.end());
+    const int n = (int)gx.size();
+    for (size_t ia = 0; ia + 1 < br.size(); ++ia) {
+        const double a0 = br[ia], a1 = br[ia + 1];
+        if (!(a1 > a0)) continue;
+        for (int i = 0; i < n; ++i) {
+            const double u = 0.5 * (gx[i] + 1.0);
+            const double xa = a0 + (a1 - a0) * u * u * (3.0 - 2.0 * u);
+            const double wa = 0.5 * gw[i] * (a1 - a0) * 6.0 * u * (1.0 - u);
+            const double A = R * R - (xa - c[a]) * (xa - c[a]);
+            const double ro2 = A - dlo * dlo;
+            if (ro2 <= 0.0) continue;
+            const double ro = std::sqrt(ro2), ri = std::sqrt(std::max(0.0, A - dhi * dhi));
+            const double iv[2][2] = {{c[b] - ro, c[b] - ri}, {c[b] + ri, c[b] + ro}};
+            for (int k = 0; k < 2; ++k) {
+                const double b0 = std::max(iv[k][0], lo[b]), b1 = std::min(iv[k][1], hi[b]);
+                if (!(b1 > b0)) continue;
+                for (int jn = 0; jn < n; ++jn) {
+                    const double xb = 0.5 * (b0 + b1) + 0.5 * (b1 - b0) * gx[jn];
+                    const double wb = 0.5 * (b1 - b0) * gw[jn];
+                    const double D = A - (xb - c[b]) * (xb - c[b]);
+                    const double hgt = std::sqrt(std::max(D, dlo * dlo));
+                    double x[3];
+                    x[a] = xa;
+                    x[b] = xb;
+                    x[m] = c[m] + s * std::min(std::max(hgt, dlo), dhi);
+                    const double rr = std::sqrt((x[0] - c[0]) * (x[0] - c[0]) + (x[1] - c[1]) * (x[1] - c[1]) +
+                                                (x[2] - c[2]) * (x[2] - c[2]));
+                    const double w = wa * wb * R / std::fabs(x[m] - c[m]);
+                    out.push_back(x[0]);
+                    out.push_back(x[1]);
+                    out.push_back(x[2]);
+                    out.push_back(w);
+                    for (int d = 0; d < 3; ++d) out.push_back((x[d] - c[d]) / rr);
+                }
+            }
+        }
+    }
+}
+
 }  // namespace bosss
 
 using namespace bosss;
@@ -558,6 +742,16 @@ struct bosss_xdg {
     std::vector<double> fit_resid[2];
     std::vector<double> moments[2];   // XDG_MAXM per item
     long long n_cells[2] = {0, 0};
+    // level-set interface term (set by bosss_b200_xdg_interface_setup)
+    bool iface = false;
+    IfaceArgs ifa{};
+    std::vector<long long> if_cells, if_off;
+    std::vector<double> if_nodes, if_w, if_n;   // reference coordinates, weights, normals
+    long long* d_if_cells = nullptr;
+    long long* d_if_off = nullptr;
+    double* d_if_nodes = nullptr;
+    double* d_if_w = nullptr;
+    double* d_if_n = nullptr;
 };
 
 namespace bosss {
@@ -795,6 +989,11 @@ int bosss_b200_xdg_destroy(bosss_xdg* X) {
         cudaFree(X->d_weights[s]);
         bosss_b200_destroy(X->h[s]);
     }
+    cudaFree(X->d_if_cells);
+    cudaFree(X->d_if_off);
+    cudaFree(X->d_if_nodes);
+    cudaFree(X->d_if_w);
+    cudaFree(X->d_if_n);
     delete X;
     return BOSSS_OK;
 }
@@ -903,6 +1102,165 @@ int bosss_b200_xdg_evaluate(bosss_xdg* X, int32_t species, double alpha, double 
     if (rc) return rc;
     CUDA_TRY(cudaMemcpyAsync(out, h->dOut, sizeof(double) * h->ncod, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    return BOSSS_OK;
+}
+
+
+// ---- level-set interface term: XLaplace_Interface on the sphere surface (NECQuadratureLevelSet)
+int bosss_b200_xdg_interface_setup(bosss_xdg* X, double mu_A, double mu_B, double penalty_base, int32_t mode,
+                                   int32_t nodes_1d) {
+    if (!X) return fail(BOSSS_ERR_BAD_ARG, "null handle");
+    if (mode != BOSSS_IFACE_SWIP && mode != BOSSS_IFACE_SIP) return fail(BOSSS_ERR_BAD_ARG, "mode: SWIP (0) or SIP (1)");
+    // ComputeScaling asserts sign(muA) == sign(muB) (XLaplace.cs:302-322)
+    if (!(mu_A * mu_B > 0.0) || !std::isfinite(mu_A) || !std::isfinite(mu_B))
+        return fail(BOSSS_ERR_BAD_ARG, "mu_A and mu_B must be finite, nonzero and of the same sign");
+    if (!std::isfinite(penalty_base)) return fail(BOSSS_ERR_BAD_ARG, "penalty_base must be finite");
+    if (nodes_1d <= 0) nodes_1d = 6;
+    if (nodes_1d > 16) return fail(BOSSS_ERR_BAD_ARG, "nodes_1d: 1..16");
+    const int K = X->K;
+    IfaceArgs f{};
+    f.muA = mu_A;
+    f.muB = mu_B;
+    double pen_mu;
+    if (mode == BOSSS_IFACE_SWIP) {
+        f.omA = mu_B / (mu_A + mu_B);
+        f.omB = mu_A / (mu_A + mu_B);
+        pen_mu = 2.0 * mu_A * mu_B / (mu_A + mu_B);
+    } else {
+        f.omA = 0.5;
+        f.omB = 0.5;
+        pen_mu = std::max(std::fabs(mu_A), std::fabs(mu_B)) * (mu_A > 0.0 ? 1.0 : -1.0);
+    }
+    // CoefficientUpdate (XLaplace.cs:331-341): max of the simplex and the cube formula, D = 3
+    const double pdeg = std::max((K + 1.0) * (K + 3.0) / 3.0, (K + 1.0) * (K + 1.0));
+    f.pen = penalty_base * pdeg * pen_mu;
+    f.alpha = 1.0;
+    std::vector<double> gx, gw;
+    gauss(nodes_1d, gx, gw);
+    const GridConst& g = X->h[0]->base.g;
+    std::vector<long long> cells, off = {0};
+    std::vector<double> xi, w, nr, tmp;
+    const double c[3] = {X->ls.c[0], X->ls.c[1], X->ls.c[2]};
+    for (int i = 0; i < g.n[0]; ++i)
+        for (int j = 0; j < g.n[1]; ++j)
+            for (int k = 0; k < g.n[2]; ++k) {
+                const int ijk[3] = {i, j, k};
+                double lo[3], hi[3];
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = g.lo[d] + ijk[d] * g.h[d];
+                    hi[d] = lo[d] + g.h[d];
+                }
+                if (ls_box(X->ls, lo, hi, 7) != 0) continue;
+                tmp.clear();
+                sphere_surface_box(lo, hi, c, X->ls.r, gx, gw, 0, tmp);
+                if (tmp.empty()) continue;
+                const size_t nn = tmp.size() / 7;
+                for (size_t q = 0; q < nn; ++q) {
+                    for (int d = 0; d < 3; ++d) xi.push_back(2.0 * (tmp[7 * q + d] - lo[d]) / g.h[d] - 1.0);
+                    w.push_back(tmp[7 * q + 3]);
+                    for (int d = 0; d < 3; ++d) nr.push_back(tmp[7 * q + 4 + d]);
+                }
+                cells.push_back((long long)i * g.stride[0] + (long long)j * g.stride[1] + (long long)k * g.stride[2]);
+                off.push_back(off.back() + (long long)nn);
+            }
+    CUDA_TRY(cudaSetDevice(X->device));
+    cudaFree(X->d_if_cells);
+    cudaFree(X->d_if_off);
+    cudaFree(X->d_if_nodes);
+    cudaFree(X->d_if_w);
+    cudaFree(X->d_if_n);
+    X->d_if_cells = nullptr;
+    X->d_if_off = nullptr;
+    X->d_if_nodes = X->d_if_w = X->d_if_n = nullptr;
+    X->iface = false;
+    const size_t nc = cells.size(), nq = w.size();
+    CUDA_TRY(cudaMalloc(&X->d_if_cells, sizeof(long long) * std::max<size_t>(nc, 1)));
+    CUDA_TRY(cudaMalloc(&X->d_if_off, sizeof(long long) * (nc + 1)));
+    CUDA_TRY(cudaMalloc(&X->d_if_nodes, sizeof(double) * 3 * std::max<size_t>(nq, 1)));
+    CUDA_TRY(cudaMalloc(&X->d_if_w, sizeof(double) * std::max<size_t>(nq, 1)));
+    CUDA_TRY(cudaMalloc(&X->d_if_n, sizeof(double) * 3 * std::max<size_t>(nq, 1)));
+    if (nc) CUDA_TRY(cudaMemcpy(X->d_if_cells, cells.data(), sizeof(long long) * nc, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(X->d_if_off, off.data(), sizeof(long long) * (nc + 1), cudaMemcpyHostToDevice));
+    if (nq) {
+        CUDA_TRY(cudaMemcpy(X->d_if_nodes, xi.data(), sizeof(double) * 3 * nq, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(X->d_if_w, w.data(), sizeof(double) * nq, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(X->d_if_n, nr.data(), sizeof(double) * 3 * nq, cudaMemcpyHostToDevice));
+    }
+    X->if_cells.swap(cells);
+    X->if_off.swap(off);
+    X->if_nodes.swap(xi);
+    X->if_w.swap(w);
+    X->if_n.swap(nr);
+    X->ifa = f;
+    X->iface = true;
+    return BOSSS_OK;
+}
+
+int bosss_b200_xdg_interface_get_rules(const bosss_xdg* X, int64_t* counts, int64_t* cells, int64_t* node_offsets,
+                                       double* nodes, double* weights, double* normals) {
+    if (!X || !counts) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    if (!X->iface) return fail(BOSSS_ERR_BAD_ARG, "interface term not set up (bosss_b200_xdg_interface_setup)");
+    const size_t nc = X->if_cells.size(), nq = X->if_w.size();
+    counts[0] = (int64_t)nc;
+    counts[1] = (int64_t)nq;
+    if (cells) for (size_t i = 0; i < nc; ++i) cells[i] = X->if_cells[i];
+    if (node_offsets) for (size_t i = 0; i <= nc; ++i) node_offsets[i] = X->if_off[i];
+    if (nodes) std::memcpy(nodes, X->if_nodes.data(), sizeof(double) * 3 * nq);
+    if (weights) std::memcpy(weights, X->if_w.data(), sizeof(double) * nq);
+    if (normals) std::memcpy(normals, X->if_n.data(), sizeof(double) * 3 * nq);
+    return BOSSS_OK;
+}
+
+int bosss_b200_xdg_interface_evaluate_device(bosss_xdg* X, double alpha, const double* UA_dev, const double* UB_dev,
+                                             double* outA_dev, double* outB_dev, void* stream) {
+    if (!X || !UA_dev || !UB_dev || !outA_dev || !outB_dev) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    if (!X->iface) return fail(BOSSS_ERR_BAD_ARG, "interface term not set up (bosss_b200_xdg_interface_setup)");
+    CUDA_TRY(cudaSetDevice(X->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : X->h[0]->stream;
+    const int n = (int)X->if_cells.size();
+    if (n == 0) return BOSSS_OK;
+    IfaceArgs f = X->ifa;
+    f.alpha = alpha;
+    const GridConst& g = X->h[0]->base.g;
+    switch (X->K) {
+#define BOSSS_IFACE_LAUNCH(KK)                                                                                  \
+    case KK:                                                                                                    \
+        k_interface_eval<KK><<<n, 64, 0, st>>>(X->d_if_cells, X->d_if_off, X->d_if_nodes, X->d_if_w, X->d_if_n, \
+                                               n, g, f, UA_dev, UB_dev, outA_dev, outB_dev);                   \
+        break;
+        BOSSS_IFACE_LAUNCH(1)
+        BOSSS_IFACE_LAUNCH(2)
+        BOSSS_IFACE_LAUNCH(3)
+        BOSSS_IFACE_LAUNCH(4)
+#undef BOSSS_IFACE_LAUNCH
+        default: return fail(BOSSS_ERR_BAD_ARG, "degree 1..4");
+    }
+    CUDA_TRY(cudaGetLastError());
+    return BOSSS_OK;
+}
+
+int bosss_b200_xdg_interface_evaluate(bosss_xdg* X, double alpha, const double* UA, const double* UB, double* outA,
+                                      double* outB) {
+    if (!X || !UA || !UB || !outA || !outB) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    if (!X->iface) return fail(BOSSS_ERR_BAD_ARG, "interface term not set up (bosss_b200_xdg_interface_setup)");
+    CUDA_TRY(cudaSetDevice(X->device));
+    const size_t nb = sizeof(double) * (size_t)X->h[0]->ncod;
+    double* buf = nullptr;
+    CUDA_TRY(cudaMalloc(&buf, 4 * nb));
+    double *dUA = buf, *dUB = buf + X->h[0]->ncod, *dA = buf + 2 * X->h[0]->ncod, *dB = buf + 3 * X->h[0]->ncod;
+    cudaStream_t st = X->h[0]->stream;
+    cudaError_t e = cudaMemcpyAsync(dUA, UA, nb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dUB, UB, nb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dA, outA, nb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dB, outB, nb, cudaMemcpyHostToDevice, st);
+    int rc = BOSSS_OK;
+    if (e == cudaSuccess) rc = bosss_b200_xdg_interface_evaluate_device(X, alpha, dUA, dUB, dA, dB, st);
+    if (e == cudaSuccess && rc == BOSSS_OK) e = cudaMemcpyAsync(outA, dA, nb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && rc == BOSSS_OK) e = cudaMemcpyAsync(outB, dB, nb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(buf);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(BOSSS_ERR_CUDA, cudaGetErrorString(e));
     return BOSSS_OK;
 }
 

@@ -666,3 +666,41 @@ class XdgEvaluator:
         U = np.ascontiguousarray(U, dtype=np.float64)
         C.check(C.lib().bosss_b200_xdg_evaluate(self.handle, species, alpha, beta, C.ptr(U), C.ptr(output), 0.0))
         return output
+
+    # ---- level-set interface term (XLaplace_Interface through NECQuadratureLevelSet)
+    SWIP, SIP = 0, 1   # XLaplace_Interface.Mode, reference order
+
+    def SetInterface(self, muA, muB, penalty_base, mode=SIP, nodes_1d=6):
+        """Adds the interface component ``XLaplace_Interface(muA, muB, penalty_base, mode)``
+        (XLaplace.cs:214-220) and builds the surface rules of the sphere in the cut cells."""
+        C.check(C.lib().bosss_b200_xdg_interface_setup(self.handle, float(muA), float(muB), float(penalty_base),
+                                                       int(mode), int(nodes_1d)))
+
+    def interface_rules(self):
+        """Surface rules: cut cells, node offsets, nodes (reference coordinates of the cell),
+        weights (physical surface measure) and unit normals from A into B."""
+        cnt = (ctypes.c_int64 * 2)()
+        C.check(C.lib().bosss_b200_xdg_interface_get_rules(self.handle, cnt, None, None, None, None, None))
+        nc, nq = cnt[0], cnt[1]
+        cells = np.zeros(nc, dtype=np.int64)
+        offs = np.zeros(nc + 1, dtype=np.int64)
+        nodes, w, nrm = np.zeros(nq * 3), np.zeros(nq), np.zeros(nq * 3)
+        C.check(C.lib().bosss_b200_xdg_interface_get_rules(self.handle, cnt, C.ptr(cells), C.ptr(offs), C.ptr(nodes),
+                                                           C.ptr(w), C.ptr(nrm)))
+        return {"cells": cells, "offsets": offs, "nodes": nodes.reshape(nq, 3), "weights": w,
+                "normals": nrm.reshape(nq, 3)}
+
+    def EvaluateInterface(self, alpha, UA, UB, outA, outB):
+        """outA += alpha * (interface term tested with species A), outB likewise."""
+        if hasattr(UA, "is_cuda") and UA.is_cuda:
+            import torch
+            s = torch.cuda.current_stream().cuda_stream
+            C.check(C.lib().bosss_b200_xdg_interface_evaluate_device(
+                self.handle, alpha, C.ptr(UA), C.ptr(UB), C.ptr(outA), C.ptr(outB),
+                ctypes.c_void_p(s if s else C.CUDA_STREAM_LEGACY)))
+            return outA, outB
+        UA = np.ascontiguousarray(UA, dtype=np.float64)
+        UB = np.ascontiguousarray(UB, dtype=np.float64)
+        C.check(C.lib().bosss_b200_xdg_interface_evaluate(self.handle, alpha, C.ptr(UA), C.ptr(UB), C.ptr(outA),
+                                                          C.ptr(outB)))
+        return outA, outB

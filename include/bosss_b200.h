@@ -354,6 +354,31 @@ int bosss_b200_xdg_evaluate(bosss_xdg* X, int32_t species, double alpha, double 
 int bosss_b200_xdg_evaluate_device(bosss_xdg* X, int32_t species, double alpha, double beta, const double* U_dev,
                                    double* out_dev, double time, void* stream);
 
+/* Level-set interface term of the two-phase Poisson problem: XLaplace_Interface.InnerEdgeForm
+ * (src/L3-solution/BoSSS.Solution.XNSECommon/XLaplace.cs:205-345) integrated over the level-set
+ * surface of every cut cell, as NECQuadratureLevelSet.EvaluateEx / SaveIntegrationResults do
+ * (src/L2-foundation/BoSSS.Foundation.XDG/NECQuadratureLevelSet.cs:35-664).
+ * setup: mu_A (phi < 0), mu_B (phi > 0), penalty base factor and mode as the XLaplace_Interface
+ * constructor (mode BOSSS_IFACE_SWIP or BOSSS_IFACE_SIP, the reference's enum order); builds the
+ * surface rules of the sphere on the host (nodes_1d Gauss nodes per interval; <= 0: 6).
+ * The penalty's cell length scale is the uncut cell's (the bulk SIP's), not the species'
+ * cut-cell length scale of the reference. */
+enum bosss_iface_mode { BOSSS_IFACE_SWIP = 0, BOSSS_IFACE_SIP = 1 };
+int bosss_b200_xdg_interface_setup(bosss_xdg* X, double mu_A, double mu_B, double penalty_base, int32_t mode,
+                                   int32_t nodes_1d);
+/* counts[2] = {cut cells with surface nodes, nodes}; then (any may be NULL) the cells, node
+ * offsets (cells + 1), nodes in reference coordinates of the cell (3 per node), weights (physical
+ * surface measure) and unit normals grad(phi)/|grad(phi)| (3 per node, from A into B) */
+int bosss_b200_xdg_interface_get_rules(const bosss_xdg* X, int64_t* counts, int64_t* cells, int64_t* node_offsets,
+                                       double* nodes, double* weights, double* normals);
+/* out_A += alpha * (interface term tested with species A), out_B likewise; U_A, U_B and the
+ * outputs are the species' coefficient vectors of bosss_b200_xdg_evaluate (cell-major, all cells) */
+int bosss_b200_xdg_interface_evaluate(bosss_xdg* X, double alpha, const double* U_A, const double* U_B,
+                                      double* out_A, double* out_B);
+int bosss_b200_xdg_interface_evaluate_device(bosss_xdg* X, double alpha, const double* U_A_dev,
+                                             const double* U_B_dev, double* out_A_dev, double* out_B_dev,
+                                             void* stream);
+
 /* ---- explicit Runge-Kutta time stepping ----
  * RungeKutta.Perform / PerformStage (TimeStepping/RungeKutta.cs:240-330) with the change rate
  * of ExplicitEuler.ComputeChangeRate (ExplicitEuler.cs:223-229): for s = 0..stages-1

@@ -193,3 +193,53 @@ def rk_steps(opd, gd, U, a, b, c, dt, nsteps=1):
                 upd += -b[s] * dt * k[s]
         y = y + upd
     return y
+
+
+def xdg_interface(nodes_xyz, periodic, k, rules, UA, UB, muA, muB, penalty_base, mode, alpha=1.0):
+    """Level-set interface term, restated from XLaplace_Interface.InnerEdgeForm
+    (XNSECommon/XLaplace.cs:229-297, GetPenalty :261-297, ComputeScaling :302-322,
+    CoefficientUpdate :331-341) and the two-species scatter of
+    NECQuadratureLevelSet.SaveIntegrationResults (NECQuadratureLevelSet.cs:622-661): for every
+    cut cell and surface node, Ret(vA, vB) with (vA, vB) = (phi_n, 0) is added to species A's
+    row n and with (0, phi_n) to species B's. Basis values come from the oracle's own basis
+    (monomial representation); the surface rule is given. The penalty length scale is the
+    uncut cell's (Vol / (surface / 2), boundary faces counted twice). Returns (outA, outB)."""
+    from math import comb
+    h = [float(x[1] - x[0]) for x in nodes_xyz]
+    n = [len(x) - 1 for x in nodes_xyz]
+    Np = comb(k + 3, 3)
+    detJ = np.prod([0.5 * hh for hh in h])
+    sc = 1.0 / np.sqrt(detJ)
+    if mode == 0:   # SWIP
+        omA, omB = muB / (muA + muB), muA / (muA + muB)
+        pen_mu = 2.0 * muA * muB / (muA + muB)
+    else:           # SIP
+        omA = omB = 0.5
+        pen_mu = max(abs(muA), abs(muB)) * np.sign(muA)
+    pdeg = max((k + 1.0) * (k + 3.0) / 3.0, (k + 1.0) ** 2)
+    outA = np.zeros_like(np.asarray(UA, dtype=np.float64))
+    outB = np.zeros_like(outA)
+    cells, offs = rules["cells"], rules["offsets"]
+    for r, cell in enumerate(cells):
+        ijk = (cell // (n[1] * n[2]), (cell // n[2]) % n[1], cell % n[2])
+        cj = 0.0
+        for d in range(3):
+            nb = 0 if periodic[d] else int(ijk[d] == 0) + int(ijk[d] == n[d] - 1)
+            cj += (2.0 + nb) / h[d]
+        pen = penalty_base * pdeg * pen_mu * 0.5 * cj
+        sl = slice(offs[r], offs[r + 1])
+        phi, dphi = basis_eval(3, k, rules["nodes"][sl])          # (Np, q), (Np, q, 3)
+        N = rules["normals"][sl]
+        w = rules["weights"][sl]
+        phi = phi * sc
+        gn = np.einsum("nqd,qd->nq", dphi * (sc * 2.0 / np.array(h)), N)   # grad(phi_n) . N
+        cA, cB = UA[cell * Np:(cell + 1) * Np], UB[cell * Np:(cell + 1) * Np]
+        uA, uB = cA @ phi, cB @ phi
+        gA, gB = cA @ gn, cB @ gn
+        jump = uA - uB
+        flux = muA * omA * gA + muB * omB * gB
+        retA = (flux - pen * jump) * phi + muA * omA * gn * jump      # vA = phi_n, vB = 0
+        retB = -(flux - pen * jump) * phi + muB * omB * gn * jump     # vA = 0, vB = phi_n
+        outA[cell * Np:(cell + 1) * Np] += alpha * (retA @ w)
+        outB[cell * Np:(cell + 1) * Np] += alpha * (retB @ w)
+    return outA, outB
