@@ -307,8 +307,9 @@ def run_newton(args):
 
 
 def run_xdg(args):
-    """XDG two-phase Poisson, bulk part, 128^3, k=2: rule construction (moments + weights on
-    the device) and per-species evaluation of both species."""
+    """XDG two-phase Poisson, 128^3, k=2: rule construction (moments + weights on the device,
+    surface rules on the host) and one step = the per-species bulk evaluation of both species
+    followed by the level-set interface term (XLaplace_Interface, SIP, mu 1 / 10)."""
     import torch
     from bosss_b200 import operator as O
     from bosss_b200 import problems as P
@@ -317,6 +318,10 @@ def run_xdg(args):
     X = O.XdgEvaluator(opA, opB, g, 2, c, 0.4)
     torch.cuda.synchronize()
     t_rules = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    X.SetInterface(1.0, 10.0, 4.0, X.SIP, 6)
+    t_surface = time.perf_counter() - t0
+    if_rules = X.interface_rules()
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
@@ -325,22 +330,32 @@ def run_xdg(args):
     for _ in range(max(args.warmup, 3)):
         for s in (0, 1):
             X.Evaluate(s, 1.0, 0.0, out[s], U[s])
+        X.EvaluateInterface(1.0, U[0], U[1], out[0], out[1])
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    t_bulk, t_if = 0.0, 0.0
     for _ in range(args.steps):
+        e0.record(stream)
         for s in (0, 1):
             X.Evaluate(s, 1.0, 0.0, out[s], U[s])
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+        e1.record(stream)
+        X.EvaluateInterface(1.0, U[0], U[1], out[0], out[1])
+        e2.record(stream)
+        torch.cuda.synchronize()
+        t_bulk += e0.elapsed_time(e1)
+        t_if += e1.elapsed_time(e2)
+    ms = (t_bulk + t_if) / args.steps
     infos = [X.info(0), X.info(1)]
     dofs = sum(i["cells"] for i in infos) * 10
-    line = {"metric": "xdg_bulk_dof_updates_per_s", "value": dofs / (ms * 1e-3), "unit": "DOF/s", "n_gpus": 1,
+    line = {"metric": "xdg_dof_updates_per_s", "value": dofs / (ms * 1e-3), "unit": "DOF/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": "xdg_poisson_128^3_k2_both_species", "species_dofs": dofs,
-                                            "rule_construction_s": t_rules, "species_A": infos[0],
-                                            "species_B": infos[1]}}
+            "data": "synthetic", "config": {"workload": "xdg_poisson_128^3_k2_both_species_bulk+interface",
+                                            "species_dofs": dofs, "rule_construction_s": t_rules,
+                                            "surface_rule_construction_s": t_surface,
+                                            "surface_cells": int(len(if_rules["cells"])),
+                                            "surface_nodes": int(if_rules["weights"].size),
+                                            "species_A": infos[0], "species_B": infos[1]},
+            "ms_bulk": t_bulk / args.steps, "ms_interface": t_if / args.steps}
     print(json.dumps(line), flush=True)
     X.Dispose()
 

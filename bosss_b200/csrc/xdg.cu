@@ -188,62 +188,87 @@ __global__ void k_moments(const CutItem* __restrict__ items, int nitems, LevelSe
     }
     const int S1 = sub.S1, S2 = sub.S2;
     const long long ncoarse = (dims == 3) ? (long long)S1 * S1 * S1 : (long long)S1 * S1;
-    // every thread takes coarse boxes; cut coarse boxes are refined S2-fold
-    for (long long cb = threadIdx.x; cb < ncoarse; cb += blockDim.x) {
-        int ci[3] = {(int)(cb % S1), (int)((cb / S1) % S1), (int)(cb / ((long long)S1 * S1))};
-        // reference coordinates of the coarse box
-        double rlo[3], rhi[3];
+    const long long nfine = (dims == 3) ? (long long)S2 * S2 * S2 : (long long)S2 * S2;
+    auto to_phys = [&](const double* rr, double* x) {
+        for (int d = 0; d < 3; ++d) x[d] = it.center[d];
+        for (int k = 0; k < dims; ++k) x[t[k]] = it.center[t[k]] + 0.5 * it.h[t[k]] * rr[k];
+    };
+    auto classify = [&](const double* a, const double* b) {
+        double plo[3], phi_[3];
+        to_phys(a, plo);
+        to_phys(b, phi_);
+        int mask = 0;
+        for (int k = 0; k < dims; ++k) mask |= 1 << t[k];
+        return ls_box(L, plo, phi_, mask);
+    };
+    auto coarse_box = [&](long long cb, double* rlo, double* rhi) {
+        const int ci[3] = {(int)(cb % S1), (int)((cb / S1) % S1), (int)(cb / ((long long)S1 * S1))};
         for (int k = 0; k < dims; ++k) {
             rlo[k] = -1.0 + 2.0 * ci[k] / S1;
             rhi[k] = rlo[k] + 2.0 / S1;
         }
-        auto to_phys = [&](const double* rr, double* x) {
-            for (int d = 0; d < 3; ++d) x[d] = it.center[d];
-            for (int k = 0; k < dims; ++k) x[t[k]] = it.center[t[k]] + 0.5 * it.h[t[k]] * rr[k];
-        };
-        auto classify = [&](const double* a, const double* b) {
-            double plo[3], phi_[3];
-            to_phys(a, plo);
-            to_phys(b, phi_);
-            int mask = 0;
-            for (int k = 0; k < dims; ++k) mask |= 1 << t[k];
-            return ls_box(L, plo, phi_, mask);
-        };
-        const int cls = classify(rlo, rhi);
-        if (cls == -it.sp) continue;   // fully in the other species
-        const int nsub = (cls == 0) ? S2 : 1;
-        const int nfine = (dims == 3) ? nsub * nsub * nsub : nsub * nsub;
-        for (int fb = 0; fb < nfine; ++fb) {
-            int fi[3] = {fb % nsub, (fb / nsub) % nsub, fb / (nsub * nsub)};
-            double flo[3], fhi[3];
+    };
+    // 3-point Gauss rule per direction on the box; on a cut box, the species indicator at the node
+    auto integrate = [&](const double* lo, const double* hi, bool cut) {
+        const int nq = (dims == 3) ? 27 : 9;
+        for (int q = 0; q < nq; ++q) {
+            const int qi[3] = {q % 3, (q / 3) % 3, q / 9};
+            double rr[3], wq = 1.0;
             for (int k = 0; k < dims; ++k) {
-                const double hh = (rhi[k] - rlo[k]) / nsub;
+                const double hh = hi[k] - lo[k];
+                rr[k] = lo[k] + 0.5 * hh * (sub.gx[qi[k]] + 1.0);
+                wq *= 0.5 * hh * sub.gw[qi[k]];
+            }
+            if (cut) {
+                double x[3];
+                to_phys(rr, x);
+                const double ph = ls_phi(L, x);
+                if ((it.sp < 0) ? !(ph < 0.0) : (ph < 0.0)) continue;
+            }
+            double v[XDG_MAXM];
+            if (dims == 3) basis3(it.p, rr, v);
+            else basis2(it.p, rr, v);
+            for (int m = 0; m < M; ++m) acc[m] += wq * v[m];
+        }
+    };
+    // Coarse boxes in chunks: (1) every thread classifies coarse boxes, integrates the uncut
+    // ones of the species and lists the cut ones; (2) the (cut coarse box, fine box) pairs are
+    // spread evenly over the block's threads, so the refinement work is balanced.
+    constexpr int CHUNK = 1024;
+    __shared__ int cutlist[CHUNK];
+    __shared__ int ncut;
+    for (long long base = 0; base < ncoarse; base += CHUNK) {
+        const int nb = (int)((ncoarse - base) < CHUNK ? (ncoarse - base) : CHUNK);
+        if (threadIdx.x == 0) ncut = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+            double rlo[3], rhi[3];
+            coarse_box(base + i, rlo, rhi);
+            const int cls = classify(rlo, rhi);
+            if (cls == -it.sp) continue;   // fully in the other species
+            if (cls == 0) {
+                cutlist[atomicAdd(&ncut, 1)] = i;
+                continue;
+            }
+            integrate(rlo, rhi, false);
+        }
+        __syncthreads();
+        const long long work = (long long)ncut * nfine;
+        for (long long wi = threadIdx.x; wi < work; wi += blockDim.x) {
+            double rlo[3], rhi[3], flo[3], fhi[3];
+            coarse_box(base + cutlist[wi / nfine], rlo, rhi);
+            const long long fb = wi % nfine;
+            const int fi[3] = {(int)(fb % S2), (int)((fb / S2) % S2), (int)(fb / ((long long)S2 * S2))};
+            for (int k = 0; k < dims; ++k) {
+                const double hh = (rhi[k] - rlo[k]) / S2;
                 flo[k] = rlo[k] + fi[k] * hh;
                 fhi[k] = flo[k] + hh;
             }
-            const int fcls = (nsub > 1) ? classify(flo, fhi) : cls;
+            const int fcls = classify(flo, fhi);
             if (fcls == -it.sp) continue;
-            const int nq = (dims == 3) ? 27 : 9;
-            for (int q = 0; q < nq; ++q) {
-                int qi[3] = {q % 3, (q / 3) % 3, q / 9};
-                double rr[3], wq = 1.0;
-                for (int k = 0; k < dims; ++k) {
-                    const double hh = fhi[k] - flo[k];
-                    rr[k] = flo[k] + 0.5 * hh * (sub.gx[qi[k]] + 1.0);
-                    wq *= 0.5 * hh * sub.gw[qi[k]];
-                }
-                if (fcls == 0) {   // cut leaf: indicator of the species at the node
-                    double x[3];
-                    to_phys(rr, x);
-                    const double ph = ls_phi(L, x);
-                    if ((it.sp < 0) ? !(ph < 0.0) : (ph < 0.0)) continue;
-                }
-                double v[XDG_MAXM];
-                if (dims == 3) basis3(it.p, rr, v);
-                else basis2(it.p, rr, v);
-                for (int m = 0; m < M; ++m) acc[m] += wq * v[m];
-            }
+            integrate(flo, fhi, fcls == 0);
         }
+        __syncthreads();
     }
     // block reduction
     __shared__ double red[XDG_MAXM][33];
@@ -722,6 +747,14 @@ static void sphere_surface_box(const double* lo, const double* hi, const double*
 
 }  // namespace bosss
 
+namespace bosss {
+// out[i] *= beta on [0, n): the cells outside a species' band take no contribution
+__global__ void k_scale(double* __restrict__ out, long long n, double beta) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] *= beta;
+}
+}  // namespace bosss
+
 using namespace bosss;
 
 struct bosss_xdg {
@@ -742,6 +775,9 @@ struct bosss_xdg {
     std::vector<double> fit_resid[2];
     std::vector<double> moments[2];   // XDG_MAXM per item
     long long n_cells[2] = {0, 0};
+    // per species: the cells [rng[s][0], rng[s][1]) hold every cell with species content (cells
+    // are in generator order, so a species inside a sphere spans a band of x-planes)
+    long long rng[2][2] = {{0, 0}, {0, 0}};
     // level-set interface term (set by bosss_b200_xdg_interface_setup)
     bool iface = false;
     IfaceArgs ifa{};
@@ -973,6 +1009,14 @@ int bosss_b200_xdg_create(const bosss_op_desc* opA, const bosss_op_desc* opB, co
             bosss_b200_xdg_destroy(X);
             return rc;
         }
+        long long j0 = -1, j1 = 0;
+        for (long long j = 0; j < (long long)X->vol[s].size(); ++j)
+            if (X->vol[s][j] != 0) {
+                if (j0 < 0) j0 = j;
+                j1 = j + 1;
+            }
+        X->rng[s][0] = j0 < 0 ? 0 : j0;
+        X->rng[s][1] = j1;
     }
     *out = X;
     return BOSSS_OK;
@@ -1063,11 +1107,30 @@ int bosss_b200_xdg_evaluate_device(bosss_xdg* X, int32_t species, double alpha, 
     CUDA_TRY(cudaSetDevice(X->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
     // uncut cells and faces of the species: tensor kernel with masks
-    EvalArgs keep = h->base;
-    h->base.vol_flag = X->d_vol[s];
-    h->base.face_flag = X->d_face[s];
-    int rc = run_mode(h, MODE_RES, alpha, beta, U_dev, nullptr, out_dev, time, st);
-    h->base = keep;
+    // only the band of cells holding the species is launched; the others get out = beta * out
+    const long long c0 = X->rng[s][0], c1 = X->rng[s][1], NP = np_of(3, X->K), J = h->base.g.J;
+    if (beta != 1.0) {
+        for (int part = 0; part < 2; ++part) {
+            const long long a0 = part ? c1 * NP : 0, a1 = part ? J * NP : c0 * NP;
+            if (a1 <= a0) continue;
+            if (beta == 0.0) {
+                CUDA_TRY(cudaMemsetAsync(out_dev + a0, 0, sizeof(double) * (a1 - a0), st));
+            } else {
+                k_scale<<<592, 256, 0, st>>>(out_dev + a0, a1 - a0, beta);
+                CUDA_TRY(cudaGetLastError());
+            }
+        }
+    }
+    int rc = 0;
+    if (c1 > c0) {
+        EvalArgs keep = h->base;
+        h->base.vol_flag = X->d_vol[s];
+        h->base.face_flag = X->d_face[s];
+        h->base.cbeg = c0;
+        h->base.cend = c1;
+        rc = run_mode(h, MODE_RES, alpha, beta, U_dev, nullptr, out_dev, time, st);
+        h->base = keep;
+    }
     if (rc) return rc;
     // cut cells and faces: explicit rules, added atomically
     const int n = (int)X->items[s].size();

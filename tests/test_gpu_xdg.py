@@ -87,12 +87,18 @@ def test_xdg_evaluate_matches_oracle(xdg_small):
     for s, (op, U) in enumerate([(opA, UA), (opB, UB)]):
         R = X.rules(s)
         ref = orc.xdg_evaluate(op.descriptor([2], [2], 3), g.desc(), R, U)
-        out = np.zeros_like(U)
+        out = np.full_like(U, 3.0)     # beta = 0 overwrites every cell
         X.Evaluate(s, 1.0, 0.0, out, U)
         assert rel(out, ref) <= 1e-12, (s, rel(out, ref))
         # cells without the species return 0
         absent = np.repeat(R["vol_flags"] == 0, 10)
         assert np.all(out[absent] == 0.0)
+        # out = beta * out + alpha * Op(U) on every cell, inside and outside the species' band
+        prev = np.random.default_rng(5 + s).uniform(-1, 1, U.size)
+        out = prev.copy()
+        X.Evaluate(s, 0.5, 0.25, out, U)
+        assert rel(out, 0.25 * prev + 0.5 * ref) <= 1e-12
+        assert np.array_equal(out[absent], 0.25 * prev[absent])
 
 
 def test_xdg_full_size():
