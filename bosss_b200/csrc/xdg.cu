@@ -412,6 +412,44 @@ __global__ void k_weight_solve(const CutItem* __restrict__ items, int nitems, co
 // Residual contributions of the cut items of one species, added with atomics:
 // volume items: int_{K cap s} (fV v + fG . grad v) with the item's rule;
 // face items: the SIP edge form on the cut face part (both cells, or boundary).
+// Exponents (a, b, c) of basis function n in the reference order (degree-major, then a, then b):
+// phi_n = L_a(x) L_b(y) L_c(z). With n a compile-time constant (unrolled loops) this folds away,
+// so the per-node basis values and gradients live in registers instead of per-thread arrays.
+template <int K>
+__device__ __forceinline__ void mode3(int n, int& a, int& b, int& c) {
+    int m = 0;
+    a = b = c = 0;
+#pragma unroll
+    for (int deg = 0; deg <= K; ++deg)
+#pragma unroll
+        for (int aa = 0; aa <= deg; ++aa)
+#pragma unroll
+            for (int bb = 0; bb <= deg - aa; ++bb) {
+                if (m == n) {
+                    a = aa;
+                    b = bb;
+                    c = deg - aa - bb;
+                }
+                ++m;
+            }
+}
+
+template <int K>
+__device__ __forceinline__ double bphi(const double (&L)[3][K + 1], int n) {
+    int a, b, c;
+    mode3<K>(n, a, b, c);
+    return L[0][a] * L[1][b] * L[2][c];
+}
+
+template <int K>
+__device__ __forceinline__ double bgrad(const double (&L)[3][K + 1], const double (&dL)[3][K + 1], int n, int d) {
+    int a, b, c;
+    mode3<K>(n, a, b, c);
+    if (d == 0) return dL[0][a] * L[1][b] * L[2][c];
+    if (d == 1) return L[0][a] * dL[1][b] * L[2][c];
+    return L[0][a] * L[1][b] * dL[2][c];
+}
+
 template <int K>
 __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const double* __restrict__ nodes,
                            const double* __restrict__ weights, EvalArgs a) {
@@ -460,30 +498,12 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
             legendre_vals(K, xiA[d], LA[d], dLA[d]);
             if (it.dim == 2) legendre_vals(K, xiB[d], LB[d], dLB[d]);
         }
-        double phA[NP], gA_[NP][3], phB[NP], gB_[NP][3];
-        {
-            int nn = 0;
-            for (int deg = 0; deg <= K; ++deg)
-                for (int aa = 0; aa <= deg; ++aa)
-                    for (int bb = 0; bb <= deg - aa; ++bb) {
-                        const int cc = deg - aa - bb;
-                        phA[nn] = LA[0][aa] * LA[1][bb] * LA[2][cc];
-                        gA_[nn][0] = dLA[0][aa] * LA[1][bb] * LA[2][cc];
-                        gA_[nn][1] = LA[0][aa] * dLA[1][bb] * LA[2][cc];
-                        gA_[nn][2] = LA[0][aa] * LA[1][bb] * dLA[2][cc];
-                        if (it.dim == 2) {
-                            phB[nn] = LB[0][aa] * LB[1][bb] * LB[2][cc];
-                            gB_[nn][0] = dLB[0][aa] * LB[1][bb] * LB[2][cc];
-                            gB_[nn][1] = LB[0][aa] * dLB[1][bb] * LB[2][cc];
-                            gB_[nn][2] = LB[0][aa] * LB[1][bb] * dLB[2][cc];
-                        }
-                        ++nn;
-                    }
-        }
         double uA = 0.0, GA[1][3] = {{0.0, 0.0, 0.0}};
+#pragma unroll
+        #pragma unroll
         for (int n = 0; n < NP; ++n) {
-            uA += cA[n] * phA[n];
-            for (int d = 0; d < 3; ++d) GA[0][d] += cA[n] * gA_[n][d];
+            uA += cA[n] * bphi<K>(LA, n);
+            for (int d = 0; d < 3; ++d) GA[0][d] += cA[n] * bgrad<K>(LA, dLA, n, d);
         }
         uA *= sc;
         for (int d = 0; d < 3; ++d) GA[0][d] *= sc * g.twoh[d];
@@ -493,9 +513,10 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
             double U1[1] = {uA}, fV[1] = {0.0}, fG[1][3] = {{0.0, 0.0, 0.0}};
             Phys::volume(a.ph, U1, GA, x, fV, fG);
             const double fac = wq * g.detJ * sc;
+            #pragma unroll
             for (int n = 0; n < NP; ++n) {
-                double acc = fV[0] * phA[n];
-                for (int d = 0; d < 3; ++d) acc += fG[0][d] * gA_[n][d] * g.twoh[d];
+                double acc = fV[0] * bphi<K>(LA, n);
+                for (int d = 0; d < 3; ++d) acc += fG[0][d] * bgrad<K>(LA, dLA, n, d) * g.twoh[d];
                 rA[n] += fac * acc;
             }
         } else {
@@ -503,9 +524,10 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
             double nrm[3] = {0.0, 0.0, 0.0};
             if (other >= 0) {
                 double uB = 0.0, GB[1][3] = {{0.0, 0.0, 0.0}};
+                #pragma unroll
                 for (int n = 0; n < NP; ++n) {
-                    uB += cB[n] * phB[n];
-                    for (int d = 0; d < 3; ++d) GB[0][d] += cB[n] * gB_[n][d];
+                    uB += cB[n] * bphi<K>(LB, n);
+                    for (int d = 0; d < 3; ++d) GB[0][d] += cB[n] * bgrad<K>(LB, dLB, n, d);
                 }
                 uB *= sc;
                 for (int d = 0; d < 3; ++d) GB[0][d] *= sc * g.twoh[d];
@@ -528,11 +550,12 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
                 const double gsA = selfLower ? gi[0] : go[0], gsB = selfLower ? go[0] : gi[0];
                 const double* GsA = selfLower ? Gi[0] : Go[0];
                 const double* GsB = selfLower ? Go[0] : Gi[0];
+                #pragma unroll
                 for (int n = 0; n < NP; ++n) {
-                    double accA = gsA * phA[n], accB = gsB * phB[n];
+                    double accA = gsA * bphi<K>(LA, n), accB = gsB * bphi<K>(LB, n);
                     for (int d = 0; d < 3; ++d) {
-                        accA += GsA[d] * gA_[n][d] * g.twoh[d];
-                        accB += GsB[d] * gB_[n][d] * g.twoh[d];
+                        accA += GsA[d] * bgrad<K>(LA, dLA, n, d) * g.twoh[d];
+                        accB += GsB[d] * bgrad<K>(LB, dLB, n, d) * g.twoh[d];
                     }
                     rA[n] += fac * accA;
                     rB[n] += fac * accB;
@@ -542,14 +565,16 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
                 const double pnlty = 2.0 * a.ph.pen * cell_cj(g, ijk);
                 double U1[1] = {uA}, gi[1] = {0.0}, Gi[1][3] = {{0, 0, 0}};
                 Phys::boundary(a.ph, pnlty, U1, GA, nrm, x, gi, Gi);
+                #pragma unroll
                 for (int n = 0; n < NP; ++n) {
-                    double acc = gi[0] * phA[n];
-                    for (int d = 0; d < 3; ++d) acc += Gi[0][d] * gA_[n][d] * g.twoh[d];
+                    double acc = gi[0] * bphi<K>(LA, n);
+                    for (int d = 0; d < 3; ++d) acc += Gi[0][d] * bgrad<K>(LA, dLA, n, d) * g.twoh[d];
                     rA[n] += fac * acc;
                 }
             }
         }
     }
+    #pragma unroll
     for (int n = 0; n < NP; ++n) {
         atomicAdd(&RA[n], rA[n]);
         if (it.dim == 2 && other >= 0) atomicAdd(&RB[n], rB[n]);
