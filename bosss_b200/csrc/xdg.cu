@@ -803,6 +803,10 @@ struct bosss_xdg {
     // per species: the cells [rng[s][0], rng[s][1]) hold every cell with species content (cells
     // are in generator order, so a species inside a sphere spans a band of x-planes)
     long long rng[2][2] = {{0, 0}, {0, 0}};
+    // species B on the unmasked slab kernel outside [sb[0], sb[1]): whole x-planes whose cells
+    // are all uncut species-B cells with standard faces (null: the slab kernel is not available)
+    bosss_handle* hs = nullptr;
+    long long sb[2] = {0, 0};
     // level-set interface term (set by bosss_b200_xdg_interface_setup)
     bool iface = false;
     IfaceArgs ifa{};
@@ -1042,6 +1046,25 @@ int bosss_b200_xdg_create(const bosss_op_desc* opA, const bosss_op_desc* opB, co
             }
         X->rng[s][0] = j0 < 0 ? 0 : j0;
         X->rng[s][1] = j1;
+        if (s == 1) {
+            // planes of species B holding a cell that is not plain species B
+            const long long J = (long long)X->vol[1].size(), P = X->h[1]->base.g.stride[0];
+            long long b0 = J, b1 = 0;
+            for (long long j = 0; j < J; ++j) {
+                bool plain = X->vol[1][j] == 1;
+                for (int f = 0; f < 6 && plain; ++f) plain = X->face[1][j * 6 + f] == 1;
+                if (!plain) {
+                    b0 = std::min(b0, j);
+                    b1 = j + 1;
+                }
+            }
+            if (b1 <= b0) b0 = b1 = 0;
+            X->sb[0] = (b0 / P) * P;
+            X->sb[1] = std::min(J, ((b1 + P - 1) / P) * P);
+            bosss_options sopt = hopt;
+            sopt.kernel = 2;
+            if (X->sb[1] - X->sb[0] < J && bosss_b200_create(opB, grid, &sopt, &X->hs) != BOSSS_OK) X->hs = nullptr;
+        }
     }
     *out = X;
     return BOSSS_OK;
@@ -1058,6 +1081,7 @@ int bosss_b200_xdg_destroy(bosss_xdg* X) {
         cudaFree(X->d_weights[s]);
         bosss_b200_destroy(X->h[s]);
     }
+    bosss_b200_destroy(X->hs);
     cudaFree(X->d_if_cells);
     cudaFree(X->d_if_off);
     cudaFree(X->d_if_nodes);
@@ -1147,16 +1171,28 @@ int bosss_b200_xdg_evaluate_device(bosss_xdg* X, int32_t species, double alpha, 
         }
     }
     int rc = 0;
-    if (c1 > c0) {
+    // species B: the planes of plain species-B cells go to the unmasked slab kernel
+    const bool split = (s == 1 && X->hs != nullptr);
+    const long long m0 = split ? std::max(c0, X->sb[0]) : c0, m1 = split ? std::min(c1, X->sb[1]) : c1;
+    if (m1 > m0) {
         EvalArgs keep = h->base;
         h->base.vol_flag = X->d_vol[s];
         h->base.face_flag = X->d_face[s];
-        h->base.cbeg = c0;
-        h->base.cend = c1;
+        h->base.cbeg = m0;
+        h->base.cend = m1;
         rc = run_mode(h, MODE_RES, alpha, beta, U_dev, nullptr, out_dev, time, st);
         h->base = keep;
     }
     if (rc) return rc;
+    if (split) {
+        const long long parts[2][2] = {{c0, std::min(c1, X->sb[0])}, {std::max(c0, X->sb[1]), c1}};
+        for (int part = 0; part < 2; ++part) {
+            if (parts[part][1] <= parts[part][0]) continue;
+            rc = bosss_b200_apply_device(X->hs, MODE_RES, alpha, beta, U_dev, nullptr, out_dev, time,
+                                         parts[part][0], parts[part][1], st);
+            if (rc) return rc;
+        }
+    }
     // cut cells and faces: explicit rules, added atomically
     const int n = (int)X->items[s].size();
     if (n > 0) {
