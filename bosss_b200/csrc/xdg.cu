@@ -168,15 +168,17 @@ struct Sub {
     double gx[3], gw[3];   // 3-point Gauss rule on [-1,1]
 };
 
-// moments of one item accumulated by one CTA; out[m], m < nmodes(dim, p)
-__global__ void k_moments(const CutItem* __restrict__ items, int nitems, LevelSetDev L, Sub sub, double* __restrict__ mom) {
-    const int r = blockIdx.x;
-    if (r >= nitems) return;
-    const CutItem it = items[r];
-    const int M = (it.dim == 3) ? nmodes3(it.p) : nmodes2(it.p);
-    double acc[XDG_MAXM];
-    for (int m = 0; m < XDG_MAXM; ++m) acc[m] = 0.0;
-    const int dims = it.dim;
+// The moment degree and the dimension are template parameters, so the accumulators and the
+// basis values at a node stay in registers.
+template <int PD, int DIMS>
+__device__ __forceinline__ void moments_item(const CutItem& it, long long r, const LevelSetDev& L, const Sub& sub,
+                                             double* __restrict__ mom, int* cutlist, int& ncut,
+                                             double (*red)[33]) {
+    constexpr int M = (DIMS == 3) ? (PD + 1) * (PD + 2) * (PD + 3) / 6 : (PD + 1) * (PD + 2) / 2;
+    double acc[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) acc[m] = 0.0;
+    constexpr int dims = DIMS;
     int t[3];   // reference directions integrated
     if (dims == 3) {
         t[0] = 0;
@@ -225,9 +227,10 @@ __global__ void k_moments(const CutItem* __restrict__ items, int nitems, LevelSe
                 const double ph = ls_phi(L, x);
                 if ((it.sp < 0) ? !(ph < 0.0) : (ph < 0.0)) continue;
             }
-            double v[XDG_MAXM];
-            if (dims == 3) basis3(it.p, rr, v);
-            else basis2(it.p, rr, v);
+            double v[M];
+            if (DIMS == 3) basis3(PD, rr, v);
+            else basis2(PD, rr, v);
+#pragma unroll
             for (int m = 0; m < M; ++m) acc[m] += wq * v[m];
         }
     };
@@ -235,8 +238,6 @@ __global__ void k_moments(const CutItem* __restrict__ items, int nitems, LevelSe
     // ones of the species and lists the cut ones; (2) the (cut coarse box, fine box) pairs are
     // spread evenly over the block's threads, so the refinement work is balanced.
     constexpr int CHUNK = 1024;
-    __shared__ int cutlist[CHUNK];
-    __shared__ int ncut;
     for (long long base = 0; base < ncoarse; base += CHUNK) {
         const int nb = (int)((ncoarse - base) < CHUNK ? (ncoarse - base) : CHUNK);
         if (threadIdx.x == 0) ncut = 0;
@@ -271,8 +272,8 @@ __global__ void k_moments(const CutItem* __restrict__ items, int nitems, LevelSe
         __syncthreads();
     }
     // block reduction
-    __shared__ double red[XDG_MAXM][33];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
     for (int m = 0; m < M; ++m) {
         double v = acc[m];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -283,6 +284,25 @@ __global__ void k_moments(const CutItem* __restrict__ items, int nitems, LevelSe
         double s = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
         mom[(long long)r * XDG_MAXM + threadIdx.x] = s;
+    }
+}
+
+// moments of one item accumulated by one CTA; out[m], m < nmodes(dim, p)
+__global__ void __launch_bounds__(256, 2) k_moments(const CutItem* __restrict__ items, int nitems, LevelSetDev L, Sub sub,
+                                                 double* __restrict__ mom) {
+    const int r = blockIdx.x;
+    if (r >= nitems) return;
+    const CutItem it = items[r];
+    __shared__ int cutlist[1024];
+    __shared__ int ncut;
+    __shared__ double red[XDG_MAXM][33];
+    switch (it.dim * 8 + it.p) {
+#define BOSSS_MOM_CASE(DD, PP) \
+    case DD * 8 + PP: moments_item<PP, DD>(it, r, L, sub, mom, cutlist, ncut, red); break;
+        BOSSS_MOM_CASE(3, 0) BOSSS_MOM_CASE(3, 1) BOSSS_MOM_CASE(3, 2) BOSSS_MOM_CASE(3, 3) BOSSS_MOM_CASE(3, 4)
+        BOSSS_MOM_CASE(2, 0) BOSSS_MOM_CASE(2, 1) BOSSS_MOM_CASE(2, 2) BOSSS_MOM_CASE(2, 3) BOSSS_MOM_CASE(2, 4)
+#undef BOSSS_MOM_CASE
+        default: break;
     }
 }
 
