@@ -907,6 +907,12 @@ extern "C" int bosss_b200_batch_evaluate_noalloc(int32_t n, bosss_handle* const*
         const bosss_handle* h = instances[i];
         if (!h || h->phys != phys || h->D != D || h->device != dev)
             return fail(BOSSS_ERR_BAD_ARG, "instances must share physics family, dimension and device");
+        // the batched kernel evaluates every cell of an instance: a part of a partitioned grid
+        // (ghost planes, global box) would have its ghost cells evaluated too
+        bool part = h->base.cbeg != 0 || h->base.cend != h->base.g.J;
+        for (int d = 0; d < 3; ++d) part = part || h->base.g.gn[d] != h->base.g.n[d] || h->base.g.goff[d] != 0;
+        if (part) return fail(BOSSS_ERR_BAD_ARG, "allocation-free batch: instance " + std::to_string(i) +
+                                                     " is a part of a partitioned grid; whole grids only");
         for (int m = 0; m < 3; ++m)
             if (!batch_ok(phys, m, h->K, h->Q, false))
                 return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "no batched kernel for degree " + std::to_string(h->K) +
@@ -942,7 +948,8 @@ extern "C" int bosss_b200_batch_evaluate_noalloc(int32_t n, bosss_handle* const*
                                : launch_noalloc<PhysScalar<3, false>, MODE_VJP>(scratch, n, U_dev, V_dev, out_dev, alpha, beta, time, poff, s);
     }
     if (e != cudaSuccess) return fail(BOSSS_ERR_CUDA, std::string("allocation-free batch launch: ") + cudaGetErrorString(e));
-    // the host staging area is reused by the next call: wait until the copies have read it
-    CUDA_TRY(cudaStreamSynchronize(s));
+    // no synchronisation: the staging arrays are pageable host memory, and a host-to-device
+    // cudaMemcpyAsync from pageable memory returns only after the runtime has copied the source
+    // into its own staging buffer, so the next call may overwrite them at once
     return BOSSS_OK;
 }

@@ -23,9 +23,10 @@ struct RkCoef {
     double c[RK_MAX_STAGES];
 };
 
-// out = y0 + sum_r coef.c[r] * k_r   (k stored stage-major, stride n)
-__global__ void k_rk_combine(long long n, const double* __restrict__ y0, const double* __restrict__ k, RkCoef coef,
-                             double* __restrict__ out) {
+// out = y0 + sum_r coef.c[r] * k_r   (k stored stage-major, stride n). The final update of a
+// step passes the state as both y0 and out (in place): each element is read before it is
+// written by the same thread, so y0 and out are not declared __restrict__.
+__global__ void k_rk_combine(long long n, const double* y0, const double* __restrict__ k, RkCoef coef, double* out) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         double v = y0[i];
         for (int r = 0; r < coef.ns; ++r) v += coef.c[r] * k[(long long)r * n + i];

@@ -420,11 +420,14 @@ int bosss_b200_apply_device(bosss_handle* h, int32_t mode, double alpha, double 
  * batches are rejected with BOSSS_ERR_BAD_ARG. `instances`: n handles from
  * bosss_b200_create (which allocates no device memory), same physics family (3D scalar
  * transport / advection-diffusion); vectors are the caller's device buffers, the
- * concatenation of the instances' vectors in the given order; modes as above. The first
- * call on a device looks up the array's device address; make that first call before any
- * stream capture. Every call overwrites the shared array (the queue counter is cleared
- * by each call), so calls whose kernels overlap on the GPU race; the call returns after
- * its launch has been enqueued and its staging copies have completed. */
+ * concatenation of the instances' vectors in the given order; modes as above. Whole grids
+ * only: a part of a partitioned grid is rejected with BOSSS_ERR_BAD_ARG. The first call on
+ * a device looks up the array's device address; make that first call before any stream
+ * capture. Every call overwrites the shared array (the queue counter is cleared by each
+ * call): calls on one stream are ordered by the stream, but calls whose kernels overlap on
+ * the GPU (other streams, other threads) race. The call does not wait for its kernel: it
+ * returns once the launch is enqueued. Its small instance table is copied from pageable
+ * host memory, which the CUDA runtime stages before the copy call returns. */
 int bosss_b200_batch_evaluate_noalloc(int32_t n, bosss_handle* const* instances, int32_t mode, double alpha,
                                       double beta, const double* U_dev, const double* V_dev, double* out_dev,
                                       double time, void* stream);

@@ -22,11 +22,20 @@
 //   SIPLaplace                                     NSECommon/ipLaplace.cs:30-269
 //   OptimizedHLLC{Density,Momentum,Energy}Flux     CompressibleFlowCommon/Convection/OptimizedHLLC*.cs
 //   constant source (INonlinearSource)             NECQuadratureVolume.cs:465-489
+//   OptimizedSIPG{Density,Momentum,Energy}Flux     CNS/Diffusion/OptimizedSIPG*Flux.cs (viscous
+//     compressible Navier-Stokes terms, Hartmann's G tensors, Sutherland viscosity
+//     MaterialProperty/SutherlandLaw.cs:25-75), with the outer boundary state prescribed per
+//     boundary node (SupersonicInlet.GetBoundaryState, Boundary/SupersonicInlet.cs:45-66)
 //
 // The oracle is templated on the scalar type so that a forward-mode dual
 // number gives the exact directional derivative (JVP) and, column by column
 // over a distance-2 cell colouring, the assembled Jacobian (the analogue of
 // FDJacobianBuilder, DifferentialOperator.cs:2558-2858, without the FD error).
+// The adjoint product J^T W is the gradient of the functional W . Op(U): per volume
+// node and per edge node the local form values are differentiated (multi-slot dual
+// numbers) with respect to the node states of the cells that enter them, and chained
+// back to those cells' coefficients -- the transpose of the assembled Jacobian applied
+// to W, without assembling it.
 //
 // Pinning: the basis and Gauss-rule tables are checked against the reference's
 // own tables (tests/golden/ref_*.json); the evaluator is checked against the
@@ -75,6 +84,67 @@ inline double val(Dual a) { return a.v; }
 using std::sqrt;
 template <class T> inline T tmax(T a, T b) { return (a > b) ? a : b; }  // Math.Max semantics for finite values
 template <class T> inline T tabs(T a) { return (a < T(0.0)) ? -a : a; }
+
+// Multi-slot forward dual number: value and the derivatives with respect to N inputs. The
+// operators are in-class friends (not templates), so doubles convert implicitly as for Dual.
+template <int N>
+struct DualV {
+    double v;
+    double d[N];
+    DualV() : v(0) { std::memset(d, 0, sizeof(d)); }
+    DualV(double a) : v(a) { std::memset(d, 0, sizeof(d)); }
+    friend DualV operator+(const DualV& a, const DualV& b) {
+        DualV r; r.v = a.v + b.v;
+        for (int i = 0; i < N; ++i) r.d[i] = a.d[i] + b.d[i];
+        return r;
+    }
+    friend DualV operator-(const DualV& a, const DualV& b) {
+        DualV r; r.v = a.v - b.v;
+        for (int i = 0; i < N; ++i) r.d[i] = a.d[i] - b.d[i];
+        return r;
+    }
+    friend DualV operator-(const DualV& a) {
+        DualV r; r.v = -a.v;
+        for (int i = 0; i < N; ++i) r.d[i] = -a.d[i];
+        return r;
+    }
+    friend DualV operator*(const DualV& a, const DualV& b) {
+        DualV r; r.v = a.v * b.v;
+        for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+        return r;
+    }
+    friend DualV operator/(const DualV& a, const DualV& b) {
+        DualV r; r.v = a.v / b.v;
+        const double ib2 = 1.0 / (b.v * b.v);
+        for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] * b.v - a.v * b.d[i]) * ib2;
+        return r;
+    }
+    friend DualV& operator+=(DualV& a, const DualV& b) { a = a + b; return a; }
+    friend DualV& operator-=(DualV& a, const DualV& b) { a = a - b; return a; }
+    friend DualV& operator*=(DualV& a, const DualV& b) { a = a * b; return a; }
+    friend DualV& operator/=(DualV& a, const DualV& b) { a = a / b; return a; }
+    friend bool operator>(const DualV& a, const DualV& b) { return a.v > b.v; }
+    friend bool operator<(const DualV& a, const DualV& b) { return a.v < b.v; }
+    friend bool operator>=(const DualV& a, const DualV& b) { return a.v >= b.v; }
+    friend bool operator<=(const DualV& a, const DualV& b) { return a.v <= b.v; }
+    friend DualV sqrt(const DualV& a) {
+        DualV r; r.v = std::sqrt(a.v);
+        const double f = 0.5 / r.v;
+        for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * f;
+        return r;
+    }
+    friend double val(const DualV& a) { return a.v; }
+};
+
+// Component types restated by the oracle beyond the C-ABI's device functors (same
+// descriptor struct; the library rejects them with BOSSS_ERR_UNSUPPORTED_COMPONENT).
+//   ORC_COMP_CNS_SIPG_{DENSITY,MOMENTUM,ENERGY}: OptimizedSIPG{Density,Momentum,Energy}Flux,
+//   arguments = the D+2 conservative variables (rho, m_0..m_{D-1}, rhoE);
+//   params[0] gamma, [1] Mach, [2] Reynolds, [3] Prandtl, [4] viscosity ratio (bulk/shear),
+//   [5] viscosity law (0: mu = 1, 1: Sutherland), [6] Sutherland S/T0, [7] SIPG penalty
+//   scaling, [8] momentum component (0-based). Boundary faces take the outer state from the
+//   boundary-state table (one value per domain variable and boundary face node).
+enum { ORC_COMP_CNS_SIPG_DENSITY = 20, ORC_COMP_CNS_SIPG_MOMENTUM = 21, ORC_COMP_CNS_SIPG_ENERGY = 22 };
 
 // ------------------------------------------------------------------ basis
 // Orthonormal polynomials on [-1,1]^D: products of normalised Legendre polynomials,
@@ -279,6 +349,13 @@ struct Problem {
     // face tables per degree (BasisData caches values at face nodes per face index):
     // fphi[k][((2d+s)*Qf + q)*Np + n], fdphi[k][(((2d+s)*Qf + q)*Np + n)*D + dd], s = 0 lower / 1 upper face
     std::vector<std::vector<double>> fphi, fdphi;
+    // boundary-state table (nullable): outer values of every domain variable at every boundary
+    // face node, bnd[node * n_domain + f]. Nodes are numbered cell by cell (storage order), then
+    // face direction d, then side s (0 lower, 1 upper), then face node q; bnd_off[j*2D + 2d + s]
+    // is the first node of that boundary face (-1: interior face).
+    const double* bnd = nullptr;
+    std::vector<long long> bnd_off;
+    long long n_bnd_nodes = 0;
 };
 
 static int np_of(int D, int k) {
@@ -449,6 +526,16 @@ static std::string setup(Problem& P, const bosss_op_desc* op, const bosss_grid_d
         }
         P.cj[j] = (surf + bnd) * 0.5 / vol;
     }
+    // boundary face node numbering of the boundary-state table
+    P.bnd_off.assign((size_t)P.J * 2 * P.D, -1);
+    P.n_bnd_nodes = 0;
+    for (int j = 0; j < P.J; ++j)
+        for (int d = 0; d < P.D; ++d)
+            for (int s = 0; s < 2; ++s)
+                if (neighbour(P, j, d, s) < 0) {
+                    P.bnd_off[(size_t)j * 2 * P.D + 2 * d + s] = P.n_bnd_nodes;
+                    P.n_bnd_nodes += P.nQf;
+                }
     // component checks
     for (int c = 0; c < op->n_components; ++c) {
         const auto& cp = op->components[c];
@@ -468,10 +555,100 @@ static std::string setup(Problem& P, const bosss_op_desc* op, const bosss_grid_d
                 for (int d = 0; d < P.D; ++d)
                     if (!(part ? g->global_periodic[d] : g->periodic[d])) return "HLLC: only periodic grids";
                 break;
+            case ORC_COMP_CNS_SIPG_DENSITY:
+            case ORC_COMP_CNS_SIPG_MOMENTUM:
+            case ORC_COMP_CNS_SIPG_ENERGY:
+                if (cp.n_args != P.D + 2) return "CNS SIPG needs D+2 arguments";
+                if (cp.type == ORC_COMP_CNS_SIPG_MOMENTUM && (cp.params[8] < 0 || cp.params[8] >= P.D))
+                    return "CNS SIPG momentum: bad component";
+                break;
             default: return "unsupported component";
         }
     }
     return "";
+}
+
+// ------------------------------------------------------------------ CNS viscous terms
+// Hartmann's G tensor of the viscous flux of one conservation equation, F_k = sum_{l,j}
+// G[k][l][j] dU_j/dx_l, as OptimizedSIPG{Momentum,Energy}Flux.UpdateTensorComponent and
+// UpdateBoundaryTensorComponent set it (CNS/Diffusion/OptimizedSIPGMomentumFlux.cs:592-1000,
+// OptimizedSIPGEnergyFlux.cs:630-956). U = conservative state (rho, m_0..m_{D-1}, rhoE).
+// Velocity v = m / rho, temperature T = (gamma-1) (rhoE/rho - MachScaling |v|^2 / 2),
+// mu_hat = mu(T) / (Re rho), MachScaling = gamma Mach^2, alpha = bulk viscosity ratio.
+// Momentum equation c: the coefficients of tau_ck = mu (d_k v_c + d_c v_k) + (alpha - 2/3) mu
+// delta_ck div v written on the conservative gradients (d_l v_i = (d_l m_i - v_i d_l rho)/rho).
+// In two dimensions the y-momentum entry G[x][y][rho] of the reference is -v_y mu_hat (where
+// the formula gives -v_x mu_hat); that entry is kept as the reference has it
+// (OptimizedSIPGMomentumFlux.cs:767 and the boundary variant, SIPGMomentumFlux.cs:63).
+// Energy equation: the reference's entries, in closed form (k flux direction, l gradient):
+//   G[k][k][rho] = -(MS (alpha+1/3) v_k^2 + MS |v|^2 + gPr (e - MS |v|^2)) mu_hat
+//   G[k][k][m_i] = MS (alpha+4/3 - gPr) v_k mu_hat (i = k),  MS (1 - gPr) v_i mu_hat (i != k)
+//   G[k][k][rhoE] = gPr mu_hat,  gPr = gamma / Pr
+//   G[k][l][rho] = -MS (alpha+1/3) v_k v_l mu_hat, G[k][l][m_k] = MS v_l mu_hat,
+//   G[k][l][m_l] = MS (alpha-2/3) v_k mu_hat                                   (l != k)
+template <class T>
+static void cns_gtensor(const bosss_component& cp, int D, const T* U, T G[3][3][5]) {
+    const double gamma = cp.params[0], Mach = cp.params[1], Re = cp.params[2], Pr = cp.params[3];
+    const double alpha = cp.params[4];
+    const double MS = gamma * Mach * Mach, gPr = gamma / Pr;
+    const double a43 = alpha + 4.0 / 3.0, a23 = alpha - 2.0 / 3.0, a13 = alpha + 1.0 / 3.0;
+    for (int k = 0; k < 3; ++k)
+        for (int l = 0; l < 3; ++l)
+            for (int j = 0; j < 5; ++j) G[k][l][j] = T(0.0);
+    const T rho = U[cp.args[0]];
+    T v[3];
+    T q = T(0.0);
+    for (int i = 0; i < D; ++i) {
+        v[i] = U[cp.args[1 + i]] / rho;
+        q += v[i] * v[i];
+    }
+    const T e = U[cp.args[D + 1]] / rho;
+    const T temp = T(gamma - 1.0) * (e - T(0.5 * MS) * q);
+    T mu = T(1.0);
+    if (cp.params[5] == 1.0) {
+        // SutherlandLaw.GetViscosity: T^{3/2} (1 + c) / (T + c)
+        const double c = cp.params[6];
+        mu = temp * sqrt(temp) * T(1.0 + c) / (temp + T(c));
+    }
+    const T mh = mu / T(Re) / rho;
+    if (cp.type == ORC_COMP_CNS_SIPG_MOMENTUM) {
+        const int c = (int)cp.params[8];
+        for (int k = 0; k < D; ++k)
+            for (int l = 0; l < D; ++l) {
+                // coefficient of d_l v_i in tau_ck, for every i
+                for (int i = 0; i < D; ++i) {
+                    double coef = 0.0;
+                    if (l == k && i == c) coef += 1.0;
+                    if (l == c && i == k) coef += 1.0;
+                    if (c == k && i == l) coef += a23;
+                    if (coef == 0.0) continue;
+                    G[k][l][0] -= T(coef) * v[i] * mh;
+                    G[k][l][1 + i] += T(coef) * mh;
+                }
+            }
+        if (D == 2 && c == 1) G[0][1][0] = -v[1] * mh;
+    } else if (cp.type == ORC_COMP_CNS_SIPG_ENERGY) {
+        for (int k = 0; k < D; ++k)
+            for (int l = 0; l < D; ++l) {
+                if (k == l) {
+                    G[k][k][0] = -(T(MS) * (T(a13) * v[k] * v[k] + q) + T(gPr) * (e - T(MS) * q)) * mh;
+                    for (int i = 0; i < D; ++i)
+                        G[k][k][1 + i] = (i == k) ? T(MS * (a43 - gPr)) * v[k] * mh : T(MS * (1.0 - gPr)) * v[i] * mh;
+                    G[k][k][D + 1] = T(gPr) * mh;
+                } else {
+                    G[k][l][0] = -T(MS * a13) * v[k] * v[l] * mh;
+                    G[k][l][1 + k] = T(MS) * v[l] * mh;
+                    G[k][l][1 + l] = T(MS * a23) * v[k] * mh;
+                }
+            }
+    }
+    // density: no viscous flux (OptimizedSIPGDensityFlux does nothing)
+}
+
+// SIPG penalty factor SIPGPenaltyScaling * p^2, p = the largest domain degree
+// (OptimizedSIPGMomentumFlux.cs:118-119)
+static double cns_penalty_factor(const Problem& P, const bosss_component& cp) {
+    return cp.params[7] * (double)P.pmax * (double)P.pmax;
 }
 
 // ------------------------------------------------------------------ pointwise forms
@@ -524,6 +701,17 @@ static void volume_terms(const Problem& P, const bosss_component& cp, const T* U
             for (int d = 0; d < D; ++d) msq += U[cp.args[d + 1]] * U[cp.args[d + 1]];
             T p = T(gamma - 1.0) * (E - T(gMs * 0.5) * msq / rho);
             for (int d = 0; d < D; ++d) fG[d] -= U[cp.args[d + 1]] / rho * (E + p);
+            break;
+        }
+        case ORC_COMP_CNS_SIPG_DENSITY: break;
+        case ORC_COMP_CNS_SIPG_MOMENTUM:
+        case ORC_COMP_CNS_SIPG_ENERGY: {
+            // INonlinVolumeForm_GradV.Form: f[k] += sum_{l,j} G[k][l][j] dU_j/dx_l
+            T Gt[3][3][5];
+            cns_gtensor(cp, D, U, Gt);
+            for (int k = 0; k < D; ++k)
+                for (int l = 0; l < D; ++l)
+                    for (int j = 0; j < D + 2; ++j) fG[k] += Gt[k][l][j] * G[cp.args[j]][l];
             break;
         }
     }
@@ -619,6 +807,33 @@ static void inner_edge_terms(const Problem& P, const bosss_component& cp, int jI
             gB += pen;
             break;
         }
+        case ORC_COMP_CNS_SIPG_DENSITY: break;
+        case ORC_COMP_CNS_SIPG_MOMENTUM:
+        case ORC_COMP_CNS_SIPG_ENERGY: {
+            // NonlinInternalEdge_V and _GradV (OptimizedSIPGMomentumFlux.cs:187-265, 343-449)
+            const double pen = cns_penalty_factor(P, cp) * std::max(P.cj[jIn], P.cj[jOut]);
+            T Gi[3][3][5], Go[3][3][5];
+            cns_gtensor(cp, D, UA, Gi);
+            cns_gtensor(cp, D, UB, Go);
+            T flux = T(0.0);
+            for (int k = 0; k < D; ++k) {
+                T accIn = T(0.0), accOut = T(0.0);
+                for (int l = 0; l < D; ++l)
+                    for (int j = 0; j < D + 2; ++j) {
+                        const int a = cp.args[j];
+                        const T jump = UA[a] - UB[a];
+                        flux -= T(0.5) * (Gi[k][l][j] * GA[a][l] + Go[k][l][j] * GB[a][l]) * T(n[k]);
+                        flux += T(0.5) * (Gi[k][l][j] + Go[k][l][j]) * jump * T(n[l] * pen * n[k]);
+                        accIn -= T(0.5) * Gi[k][l][j] * jump * T(n[l]);
+                        accOut -= T(0.5) * Go[k][l][j] * jump * T(n[l]);
+                    }
+                GAv[k] += accIn;
+                GBv[k] += accOut;
+            }
+            gA += flux;
+            gB -= flux;
+            break;
+        }
         case BOSSS_COMP_CONSTANT_SOURCE: break;
         case BOSSS_COMP_HLLC_DENSITY_FLUX:
         case BOSSS_COMP_HLLC_MOMENTUM_FLUX:
@@ -684,9 +899,12 @@ static void inner_edge_terms(const Problem& P, const bosss_component& cp, int jI
 }
 
 // Boundary edge (outward normal n): (gA, GA[d]).
+// Ubnd: the boundary-state table's outer values of the domain variables at this node (null if
+// the problem has no table).
 template <class T>
 static void boundary_edge_terms(const Problem& P, const bosss_component& cp, int jIn, const T* UA,
-                                const T (*GA)[3], const double* n, const double* x, T& gA, T* GAv) {
+                                const T (*GA)[3], const double* n, const double* x, const double* Ubnd, T& gA,
+                                T* GAv) {
     const int D = P.D;
     switch (cp.type) {
         case BOSSS_COMP_SCALAR_TRANSPORT_FLUX: {
@@ -721,11 +939,41 @@ static void boundary_edge_terms(const Problem& P, const bosss_component& cp, int
             // Neumann with g_N = 0 contributes nothing
             break;
         }
+        case ORC_COMP_CNS_SIPG_MOMENTUM:
+        case ORC_COMP_CNS_SIPG_ENERGY: {
+            // NonlinBoundaryEdge_V and _GradV (OptimizedSIPGMomentumFlux.cs:267-336, 451-540): the
+            // G tensor of the outer state (SupersonicInlet.GetBoundaryState), penalty p^2 cj(in)
+            if (!Ubnd) break;   // rejected by the entry points
+            const double pen = cns_penalty_factor(P, cp) * P.cj[jIn];
+            T Ub[BOSSS_MAX_VARS];
+            for (int f = 0; f < P.op.n_domain; ++f) Ub[f] = T(Ubnd[f]);
+            T Go[3][3][5];
+            cns_gtensor(cp, D, Ub, Go);
+            T flux = T(0.0);
+            for (int k = 0; k < D; ++k)
+                for (int l = 0; l < D; ++l)
+                    for (int j = 0; j < D + 2; ++j) {
+                        const int a = cp.args[j];
+                        const T jump = UA[a] - Ub[a];
+                        flux -= Go[k][l][j] * GA[a][l] * T(n[k]);
+                        flux += Go[k][l][j] * jump * T(n[l] * pen * n[k]);
+                        GAv[k] -= Go[k][l][j] * jump * T(n[l]);
+                    }
+            gA += flux;
+            break;
+        }
         default: break;
     }
 }
 
 // ------------------------------------------------------------------ evaluation
+// outer values of the boundary-state table at node q of boundary face (j, d, s), or null
+static const double* bnd_node(const Problem& P, int j, int d, int s, int q) {
+    if (!P.bnd) return nullptr;
+    const long long o = P.bnd_off[(size_t)j * 2 * P.D + 2 * d + s];
+    return o < 0 ? nullptr : P.bnd + (size_t)(o + q) * P.op.n_domain;
+}
+
 template <class T>
 static void evaluate(const Problem& P, double alpha, double beta, const T* U, T* out) {
     const int D = P.D, J = P.J, Q = (int)P.vw.size(), nd = P.op.n_domain, nc = P.op.n_codomain;
@@ -833,7 +1081,7 @@ static void evaluate(const Problem& P, double alpha, double beta, const T* U, T*
                     const auto& cp = P.op.components[ci];
                     if (cp.codomain != e) continue;
                     if (ed.out >= 0) inner_edge_terms(P, cp, ed.in, ed.out, UA, GA, UB, GB, nrm, gA, GAv, gB, GBv);
-                    else boundary_edge_terms(P, cp, ed.in, UA, GA, nrm, x, gA, GAv);
+                    else boundary_edge_terms(P, cp, ed.in, UA, GA, nrm, x, bnd_node(P, ed.in, d, fIn % 2, q), gA, GAv);
                 }
                 int k = P.op.codomain_degree[e], Np = P.cod_np[e];
                 const double* ip = &P.fphi[k][((size_t)fIn * Qf + q) * Np];
@@ -859,6 +1107,177 @@ static void evaluate(const Problem& P, double alpha, double beta, const T* U, T*
         for (int i = 0; i < Nc; ++i) out[(long)ed.in * Nc + i] += T(alpha) * Rin[(size_t)ei * Nc + i];
         if (ed.out >= 0)
             for (int i = 0; i < Nc; ++i) out[(long)ed.out * Nc + i] += T(alpha) * Rout[(size_t)ei * Nc + i];
+    }
+}
+
+// ------------------------------------------------------------------ adjoint product
+// out = J(U)^T W: the gradient of Phi(U) = W . Op(U) (alpha = 1, beta = 0). Volume node q of
+// cell j contributes w_q detJ Scaling sum_e (fV_e lam_e + fG_e . grad lam_e), lam_e = W of
+// codomain field e interpolated with its test functions; an edge node contributes the same
+// with both cells' test functions (IN and OUT sides as in the evaluation). Each contribution
+// is differentiated with respect to the node states (values and gradients of the domain
+// fields) of the cells it reads, with N dual slots (own cell first, then the OUT cell), and
+// the node-state derivatives are chained to the coefficients through the basis tables.
+template <int N>
+static void vjp(const Problem& P, const double* U, const double* W, double* out) {
+    using T = DualV<N>;
+    const int D = P.D, J = P.J, Q = (int)P.vw.size(), nd = P.op.n_domain, nc = P.op.n_codomain;
+    const int Nd = P.dom_per_cell, Nc = P.cod_per_cell, S1 = nd * (1 + D);
+    for (long i = 0; i < (long)J * Nd; ++i) out[i] = 0.0;
+
+    // ---- volume (each cell writes its own entries)
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < J; ++j) {
+        double c[3];
+        cell_center(P, j, c);
+        for (int q = 0; q < Q; ++q) {
+            T Uq[BOSSS_MAX_VARS], Gq[BOSSS_MAX_VARS][3];
+            for (int f = 0; f < nd; ++f) {
+                int k = P.op.domain_degree[f], Np = P.dom_np[f];
+                double v = 0, gr[3] = {0, 0, 0};
+                for (int n = 0; n < Np; ++n) {
+                    double cf = U[(long)j * Nd + P.dom_off[f] + n];
+                    v += cf * P.vphi[k][q * Np + n];
+                    for (int d = 0; d < D; ++d) gr[d] += cf * P.vdphi[k][(q * Np + n) * D + d];
+                }
+                Uq[f] = T(v * P.scaling);
+                Uq[f].d[f * (1 + D)] = 1.0;
+                for (int d = 0; d < D; ++d) {
+                    Gq[f][d] = T(gr[d] * P.scaling * 2.0 / P.h[d]);
+                    Gq[f][d].d[f * (1 + D) + 1 + d] = 1.0;
+                }
+            }
+            double x[3];
+            for (int d = 0; d < D; ++d) x[d] = c[d] + 0.5 * P.h[d] * P.vn[q * D + d];
+            T phi = T(0.0);
+            for (int e = 0; e < nc; ++e) {
+                T fV = T(0.0), fG[3] = {T(0.0), T(0.0), T(0.0)};
+                for (int ci = 0; ci < P.op.n_components; ++ci)
+                    if (P.op.components[ci].codomain == e) volume_terms(P, P.op.components[ci], Uq, Gq, x, fV, fG);
+                int k = P.op.codomain_degree[e], Np = P.cod_np[e];
+                double lam = 0, glam[3] = {0, 0, 0};
+                for (int m = 0; m < Np; ++m) {
+                    const double wv = W[(long)j * Nc + P.cod_off[e] + m];
+                    lam += wv * P.vphi[k][q * Np + m];
+                    for (int d = 0; d < D; ++d) glam[d] += wv * P.vdphi[k][(q * Np + m) * D + d] * 2.0 / P.h[d];
+                }
+                phi += fV * T(lam);
+                for (int d = 0; d < D; ++d) phi += fG[d] * T(glam[d]);
+            }
+            const double wq = P.vw[q] * P.detJ * P.scaling;
+            for (int f = 0; f < nd; ++f) {
+                int k = P.op.domain_degree[f], Np = P.dom_np[f];
+                for (int n = 0; n < Np; ++n) {
+                    double acc = phi.d[f * (1 + D)] * P.vphi[k][q * Np + n];
+                    for (int d = 0; d < D; ++d)
+                        acc += phi.d[f * (1 + D) + 1 + d] * P.vdphi[k][(q * Np + n) * D + d] * 2.0 / P.h[d];
+                    out[(long)j * Nd + P.dom_off[f] + n] += wq * P.scaling * acc;
+                }
+            }
+        }
+    }
+
+    // ---- edges: per-edge contributions to both cells, scattered afterwards
+    struct Edge { int in, out, d; double sgn; };
+    std::vector<Edge> edges;
+    for (int d = 0; d < D; ++d)
+        for (int j = 0; j < J; ++j) {
+            int up = neighbour(P, j, d, 1);
+            edges.push_back({j, up >= 0 ? up : -1, d, 1.0});
+            if (neighbour(P, j, d, 0) < 0) edges.push_back({j, -1, d, -1.0});
+        }
+    const int E = (int)edges.size(), Qf = P.nQf;
+    std::vector<double> Gin((size_t)E * Nd, 0.0), Gout((size_t)E * Nd, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int ei = 0; ei < E; ++ei) {
+        const Edge& ed = edges[ei];
+        const int d = ed.d;
+        double nrm[3] = {0, 0, 0};
+        nrm[d] = ed.sgn;
+        int oth[2], no = 0;
+        for (int d2 = 0; d2 < D; ++d2)
+            if (d2 != d) oth[no++] = d2;
+        double cIn[3];
+        cell_center(P, ed.in, cIn);
+        const int fIn = 2 * d + (ed.sgn > 0 ? 1 : 0), fOut = 2 * d + (ed.sgn > 0 ? 0 : 1);
+        for (int q = 0; q < Qf; ++q) {
+            double xiIn[3], x[3];
+            xiIn[d] = ed.sgn;
+            for (int t = 0; t < D - 1; ++t) xiIn[oth[t]] = P.fn[q * (D - 1) + t];
+            for (int d2 = 0; d2 < D; ++d2) x[d2] = cIn[d2] + 0.5 * P.h[d2] * xiIn[d2];
+            T UA[BOSSS_MAX_VARS], GA[BOSSS_MAX_VARS][3], UB[BOSSS_MAX_VARS], GB[BOSSS_MAX_VARS][3];
+            for (int side = 0; side < 2; ++side) {
+                if (side == 1 && ed.out < 0) break;
+                const int jc = side ? ed.out : ed.in, fi = side ? fOut : fIn, s0 = side * S1;
+                for (int f = 0; f < nd; ++f) {
+                    int k = P.op.domain_degree[f], Np = P.dom_np[f];
+                    const double* tp = &P.fphi[k][((size_t)fi * Qf + q) * Np];
+                    const double* tg = &P.fdphi[k][((size_t)fi * Qf + q) * Np * D];
+                    double v = 0, gr[3] = {0, 0, 0};
+                    for (int n = 0; n < Np; ++n) {
+                        double cf = U[(long)jc * Nd + P.dom_off[f] + n];
+                        v += cf * tp[n];
+                        for (int dd = 0; dd < D; ++dd) gr[dd] += cf * tg[n * D + dd];
+                    }
+                    T* Uo = side ? UB : UA;
+                    T(*Go)[3] = side ? GB : GA;
+                    Uo[f] = T(v * P.scaling);
+                    Uo[f].d[s0 + f * (1 + D)] = 1.0;
+                    for (int dd = 0; dd < D; ++dd) {
+                        Go[f][dd] = T(gr[dd] * P.scaling * 2.0 / P.h[dd]);
+                        Go[f][dd].d[s0 + f * (1 + D) + 1 + dd] = 1.0;
+                    }
+                }
+            }
+            T phi = T(0.0);
+            for (int e = 0; e < nc; ++e) {
+                T gA = T(0.0), gB = T(0.0), GAv[3] = {T(0.0), T(0.0), T(0.0)}, GBv[3] = {T(0.0), T(0.0), T(0.0)};
+                for (int ci = 0; ci < P.op.n_components; ++ci) {
+                    const auto& cp = P.op.components[ci];
+                    if (cp.codomain != e) continue;
+                    if (ed.out >= 0) inner_edge_terms(P, cp, ed.in, ed.out, UA, GA, UB, GB, nrm, gA, GAv, gB, GBv);
+                    else boundary_edge_terms(P, cp, ed.in, UA, GA, nrm, x, bnd_node(P, ed.in, d, fIn % 2, q), gA, GAv);
+                }
+                int k = P.op.codomain_degree[e], Np = P.cod_np[e];
+                for (int side = 0; side < 2; ++side) {
+                    if (side == 1 && ed.out < 0) break;
+                    const int jc = side ? ed.out : ed.in, fi = side ? fOut : fIn;
+                    const double* tp = &P.fphi[k][((size_t)fi * Qf + q) * Np];
+                    const double* tg = &P.fdphi[k][((size_t)fi * Qf + q) * Np * D];
+                    double lam = 0, glam[3] = {0, 0, 0};
+                    for (int m = 0; m < Np; ++m) {
+                        const double wv = W[(long)jc * Nc + P.cod_off[e] + m];
+                        lam += wv * tp[m];
+                        for (int dd = 0; dd < D; ++dd) glam[dd] += wv * tg[m * D + dd] * 2.0 / P.h[dd];
+                    }
+                    phi += (side ? gB : gA) * T(lam);
+                    for (int dd = 0; dd < D; ++dd) phi += (side ? GBv[dd] : GAv[dd]) * T(glam[dd]);
+                }
+            }
+            const double wq = P.fw[q] * P.faceSG[d] * P.scaling;
+            for (int side = 0; side < 2; ++side) {
+                if (side == 1 && ed.out < 0) break;
+                const int fi = side ? fOut : fIn, s0 = side * S1;
+                double* Gb = side ? &Gout[(size_t)ei * Nd] : &Gin[(size_t)ei * Nd];
+                for (int f = 0; f < nd; ++f) {
+                    int k = P.op.domain_degree[f], Np = P.dom_np[f];
+                    const double* tp = &P.fphi[k][((size_t)fi * Qf + q) * Np];
+                    const double* tg = &P.fdphi[k][((size_t)fi * Qf + q) * Np * D];
+                    for (int n = 0; n < Np; ++n) {
+                        double acc = phi.d[s0 + f * (1 + D)] * tp[n];
+                        for (int dd = 0; dd < D; ++dd)
+                            acc += phi.d[s0 + f * (1 + D) + 1 + dd] * tg[n * D + dd] * 2.0 / P.h[dd];
+                        Gb[P.dom_off[f] + n] += wq * P.scaling * acc;
+                    }
+                }
+            }
+        }
+    }
+    for (int ei = 0; ei < E; ++ei) {
+        const Edge& ed = edges[ei];
+        for (int i = 0; i < Nd; ++i) out[(long)ed.in * Nd + i] += Gin[(size_t)ei * Nd + i];
+        if (ed.out >= 0)
+            for (int i = 0; i < Nd; ++i) out[(long)ed.out * Nd + i] += Gout[(size_t)ei * Nd + i];
     }
 }
 
@@ -953,7 +1372,7 @@ static void face_integral(const Problem& P, int jin, int jout, int d, double sgn
                 const auto& cp = P.op.components[ci];
                 if (cp.codomain != e) continue;
                 if (jout >= 0) inner_edge_terms<double>(P, cp, jin, jout, UA, GA, UB, GB, nrm, gA, GAv, gB, GBv);
-                else boundary_edge_terms<double>(P, cp, jin, UA, GA, nrm, x, gA, GAv);
+                else boundary_edge_terms<double>(P, cp, jin, UA, GA, nrm, x, nullptr, gA, GAv);
             }
             int k = P.op.codomain_degree[e], Np = P.cod_np[e];
             for (int m = 0; m < Np; ++m) {
@@ -1094,20 +1513,55 @@ int orc_basis_eval(int D, int k, int npts, const double* pts, double* phi, doubl
     return (int)B.size();
 }
 
-int orc_evaluate(const bosss_op_desc* op, const bosss_grid_desc* g, double alpha, double beta, const double* U,
-                 double* out) {
+// setup plus the boundary-state table (bnd may be null unless a component needs it)
+static int setup_bnd(Problem& P, const bosss_op_desc* op, const bosss_grid_desc* g, const double* bnd) {
+    g_err = setup(P, op, g);
+    if (!g_err.empty()) return BOSSS_ERR_BAD_ARG;
+    P.bnd = bnd;
+    if (!bnd && P.n_bnd_nodes > 0)
+        for (int c = 0; c < op->n_components; ++c)
+            if (op->components[c].type == ORC_COMP_CNS_SIPG_MOMENTUM || op->components[c].type == ORC_COMP_CNS_SIPG_ENERGY) {
+                g_err = "CNS SIPG on a grid with boundary faces needs the boundary-state table";
+                return BOSSS_ERR_BAD_ARG;
+            }
+    return 0;
+}
+
+// number of boundary face nodes (rows of the boundary-state table)
+int orc_boundary_nodes(const bosss_op_desc* op, const bosss_grid_desc* g, int64_t* n) {
     Problem P;
     g_err = setup(P, op, g);
     if (!g_err.empty()) return BOSSS_ERR_BAD_ARG;
+    *n = P.n_bnd_nodes;
+    return 0;
+}
+
+int orc_evaluate(const bosss_op_desc* op, const bosss_grid_desc* g, const double* bnd, double alpha, double beta,
+                 const double* U, double* out) {
+    Problem P;
+    if (int rc = setup_bnd(P, op, g, bnd)) return rc;
     evaluate<double>(P, alpha, beta, U, out);
     return 0;
 }
 
-// exact directional derivative J(U) V
-int orc_jvp(const bosss_op_desc* op, const bosss_grid_desc* g, const double* U, const double* V, double* JV) {
+// exact adjoint product J(U)^T W
+int orc_vjp(const bosss_op_desc* op, const bosss_grid_desc* g, const double* bnd, const double* U, const double* W,
+            double* JTW) {
     Problem P;
-    g_err = setup(P, op, g);
-    if (!g_err.empty()) return BOSSS_ERR_BAD_ARG;
+    if (int rc = setup_bnd(P, op, g, bnd)) return rc;
+    const int need = 2 * P.op.n_domain * (1 + P.D);
+    if (need <= 8) vjp<8>(P, U, W, JTW);
+    else if (need <= 24) vjp<24>(P, U, W, JTW);
+    else if (need <= 40) vjp<40>(P, U, W, JTW);
+    else vjp<2 * BOSSS_MAX_VARS * 4>(P, U, W, JTW);
+    return 0;
+}
+
+// exact directional derivative J(U) V
+int orc_jvp(const bosss_op_desc* op, const bosss_grid_desc* g, const double* bnd, const double* U, const double* V,
+            double* JV) {
+    Problem P;
+    if (int rc = setup_bnd(P, op, g, bnd)) return rc;
     long nd = (long)P.J * P.dom_per_cell, nc = (long)P.J * P.cod_per_cell;
     std::vector<Dual> Ud(nd), od(nc);
     for (long i = 0; i < nd; ++i) Ud[i] = Dual(U[i], V[i]);
@@ -1120,11 +1574,10 @@ int orc_jvp(const bosss_op_desc* op, const bosss_grid_desc* g, const double* U, 
 // distance-2 cell colouring. Output: for each cell row j, blocks in the order
 // [self, (d=0,lower), (d=0,upper), (d=1,lower), ...]; missing neighbours get zero blocks.
 // blocks[((j*(1+2D) + b)*Nc + row)*Nd + col]; nbr[j*(1+2D)+b] = column cell or -1.
-int orc_jacobian_blocks(const bosss_op_desc* op, const bosss_grid_desc* g, const double* U, double* blocks,
-                        int32_t* nbr) {
+int orc_jacobian_blocks(const bosss_op_desc* op, const bosss_grid_desc* g, const double* bnd, const double* U,
+                        double* blocks, int32_t* nbr) {
     Problem P;
-    g_err = setup(P, op, g);
-    if (!g_err.empty()) return BOSSS_ERR_BAD_ARG;
+    if (int rc = setup_bnd(P, op, g, bnd)) return rc;
     const int D = P.D, J = P.J, Nd = P.dom_per_cell, Nc = P.cod_per_cell, NB = 1 + 2 * D;
     int m[3] = {1, 1, 1};
     for (int d = 0; d < D; ++d) {

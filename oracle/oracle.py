@@ -27,9 +27,11 @@ def lib():
             build()
         L = ctypes.CDLL(LIB)
         P = ctypes.c_void_p
-        L.orc_evaluate.argtypes = [P, P, ctypes.c_double, ctypes.c_double, P, P]
-        L.orc_jvp.argtypes = [P, P, P, P, P]
-        L.orc_jacobian_blocks.argtypes = [P, P, P, P, P]
+        L.orc_evaluate.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, P, P]
+        L.orc_jvp.argtypes = [P, P, P, P, P, P]
+        L.orc_vjp.argtypes = [P, P, P, P, P, P]
+        L.orc_jacobian_blocks.argtypes = [P, P, P, P, P, P]
+        L.orc_boundary_nodes.argtypes = [P, P, P]
         L.orc_sizes.argtypes = [P, P, P, P, P]
         L.orc_gauss_rule.argtypes = [ctypes.c_int, P, P]
         L.orc_basis_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P]
@@ -64,21 +66,51 @@ def sizes(opd, gd):
     return nd.value, nc.value, nq.value
 
 
-def evaluate(opd, gd, U, alpha=1.0, beta=0.0, out=None):
+def _bnd(opd, gd, bnd):
+    """Boundary-state table argument: None, or the outer values of every domain variable at
+    every boundary face node (``boundary_nodes`` order), shape (nodes, n_domain)."""
+    if bnd is None:
+        return None, None
+    b = np.ascontiguousarray(bnd, dtype=np.float64)
+    assert b.shape == (n_boundary_nodes(opd, gd), opd.n_domain), b.shape
+    return b, _p(b)
+
+
+def n_boundary_nodes(opd, gd):
+    n = ctypes.c_int64()
+    _check(lib().orc_boundary_nodes(ctypes.byref(opd), ctypes.byref(gd), ctypes.byref(n)))
+    return n.value
+
+
+def evaluate(opd, gd, U, alpha=1.0, beta=0.0, out=None, bnd=None):
     nd, nc, _ = sizes(opd, gd)
     U = np.ascontiguousarray(U, dtype=np.float64)
     assert U.shape == (nd,)
     out = np.zeros(nc) if out is None else np.array(out, dtype=np.float64, copy=True)
-    _check(lib().orc_evaluate(ctypes.byref(opd), ctypes.byref(gd), alpha, beta, _p(U), _p(out)))
+    keep, bp = _bnd(opd, gd, bnd)
+    _check(lib().orc_evaluate(ctypes.byref(opd), ctypes.byref(gd), bp, alpha, beta, _p(U), _p(out)))
     return out
 
 
-def jvp(opd, gd, U, V):
+def jvp(opd, gd, U, V, bnd=None):
     nd, nc, _ = sizes(opd, gd)
     U = np.ascontiguousarray(U, dtype=np.float64)
     V = np.ascontiguousarray(V, dtype=np.float64)
     out = np.zeros(nc)
-    _check(lib().orc_jvp(ctypes.byref(opd), ctypes.byref(gd), _p(U), _p(V), _p(out)))
+    keep, bp = _bnd(opd, gd, bnd)
+    _check(lib().orc_jvp(ctypes.byref(opd), ctypes.byref(gd), bp, _p(U), _p(V), _p(out)))
+    return out
+
+
+def vjp(opd, gd, U, W, bnd=None):
+    """Exact adjoint product J(U)^T W (gradient of W . Op(U), differentiated node by node)."""
+    nd, nc, _ = sizes(opd, gd)
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    W = np.ascontiguousarray(W, dtype=np.float64)
+    assert U.shape == (nd,) and W.shape == (nc,)
+    out = np.zeros(nd)
+    keep, bp = _bnd(opd, gd, bnd)
+    _check(lib().orc_vjp(ctypes.byref(opd), ctypes.byref(gd), bp, _p(U), _p(W), _p(out)))
     return out
 
 
@@ -93,7 +125,7 @@ def jacobian_dense(opd, gd, U):
     blocks = np.zeros(J * NB * Nc * Nd)
     nbr = np.zeros(J * NB, dtype=np.int32)
     U = np.ascontiguousarray(U, dtype=np.float64)
-    _check(lib().orc_jacobian_blocks(ctypes.byref(opd), ctypes.byref(gd), _p(U), _p(blocks), _p(nbr)))
+    _check(lib().orc_jacobian_blocks(ctypes.byref(opd), ctypes.byref(gd), None, _p(U), _p(blocks), _p(nbr)))
     blocks = blocks.reshape(J, NB, Nc, Nd)
     nbr = nbr.reshape(J, NB)
     A = np.zeros((nc, nd))
@@ -118,7 +150,7 @@ def jacobian_blocks(opd, gd, U):
     blocks = np.zeros(J * NB * Nc * Nd)
     nbr = np.zeros(J * NB, dtype=np.int32)
     U = np.ascontiguousarray(U, dtype=np.float64)
-    _check(lib().orc_jacobian_blocks(ctypes.byref(opd), ctypes.byref(gd), _p(U), _p(blocks), _p(nbr)))
+    _check(lib().orc_jacobian_blocks(ctypes.byref(opd), ctypes.byref(gd), None, _p(U), _p(blocks), _p(nbr)))
     return blocks.reshape(J, NB, Nc, Nd), nbr.reshape(J, NB)
 
 

@@ -1,7 +1,7 @@
 """Extract golden reference data from the BoSSS sources into small JSON fixtures.
 
-This script is test infrastructure. It runs only in a container where the
-reference tree is mounted (default ``/root/reference``); the fixtures it writes
+This script is test infrastructure. It runs only where the reference tree is
+available (its root is the required ``--ref`` argument); the fixtures it writes
 are committed so that the tests never read the reference tree at run time.
 
 What it extracts (all *data*, no code):
@@ -15,10 +15,14 @@ What it extracts (all *data*, no code):
   use, decoded from the base64/BSON resource ``LineQuadRules_bin.txt``
   (decoder: ``QuadRuleResource.cs:66-77``; tensor construction
   ``Square.cs:110-127`` and ``Cube.cs:155-200``), first 12 rules.
+* ``sipg_consistency_p{1,2,3}.json`` -- the reference's stored operator outputs of the
+  CNS SIPG consistency test, ``src/L4-application/CNS/Tests/DiffusiveFlux/
+  SIPGConsistencyRefSolution_p{1,2,3}.txt`` (one value per DOF, checked there to 1e-11
+  by ``SIPGConsistency.cs:87-160``), copied value by value.
 
 Usage::
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <root of the BoSSS tree>
 """
 import argparse
 import base64
@@ -28,6 +32,7 @@ import re
 import struct
 
 FOUNDATION = "src/L2-foundation/BoSSS.Foundation"
+SIPG_DIR = "src/L4-application/CNS/Tests/DiffusiveFlux"
 
 
 def parse_polys(path, dim, max_degree):
@@ -118,7 +123,7 @@ def parse_line_rules(path, count):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the BoSSS source tree")
     args = ap.parse_args()
     here = os.path.dirname(os.path.abspath(__file__))
     base = os.path.join(args.ref, FOUNDATION)
@@ -136,6 +141,15 @@ def main():
     with open(os.path.join(here, "ref_gauss_rules.json"), "w") as f:
         json.dump({"source": src + "/LineQuadRules_bin.txt", "rules": rules}, f, indent=0)
     print("2d polys:", len(sq), "3d polys:", len(cu), "rules:", [r["order"] for r in rules])
+
+    sipg = os.path.join(args.ref, SIPG_DIR)
+    for p in (1, 2, 3):
+        name = "SIPGConsistencyRefSolution_p%d.txt" % p
+        with open(os.path.join(sipg, name), encoding="utf-8-sig") as f:
+            vals = [float(line) for line in f if line.strip()]
+        with open(os.path.join(here, "sipg_consistency_p%d.json" % p), "w") as f:
+            json.dump({"source": "BoSSS " + SIPG_DIR + "/" + name, "degree": p, "values": vals}, f, indent=0)
+        print(name, len(vals), "values")
 
 
 if __name__ == "__main__":

@@ -1,5 +1,9 @@
 """Pins of the CPU oracle against the reference's own data and known answers.
 
+* operator output: the oracle reproduces the reference's stored ``Evaluate`` results of
+  the CNS SIPG consistency test (``CNS/Tests/DiffusiveFlux/SIPGConsistencyRefSolution_p{1,2,3}.txt``,
+  fixtures ``tests/golden/sipg_consistency_p*.json``) DOF by DOF within the reference's
+  own threshold 1e-11 (``SIPGConsistency.cs:87-160``); perturbed physics misses them;
 * basis tables: the oracle's orthonormal polynomials equal the reference's
   ``Square.cs`` / ``Cube_polynomials.cs`` tables (fixtures extracted by
   ``tests/golden/make_golden.py``), coefficient by coefficient and in the same order;
@@ -8,8 +12,9 @@
   orthonormality (mass matrix = I), consistency of the upwind transport operator
   and of the SIP Laplacian (constant and nonlinear viscosity) on polynomial
   fields, free-stream preservation of the HLLC Euler operator;
-* exact JVP against central finite differences (eps = 1e-6) and the assembled
-  Jacobian against the JVP.
+* exact JVP against central finite differences (eps = 1e-6), the assembled
+  Jacobian against the JVP, and the adjoint product (VJP) against the transposed
+  assembled Jacobian.
 """
 import json
 import os
@@ -23,6 +28,45 @@ from bosss_b200 import problems as P
 from oracle import oracle as orc
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_oracle_reproduces_reference_sipg_consistency_output(p):
+    import cns_sipg_case as S
+    opd, gd, U, bnd = S.case(p)
+    R = orc.evaluate(opd, gd, U, bnd=bnd)
+    ref = S.reference_values(p)
+    assert R.shape == ref.shape == (9 * 4 * (p + 1) * (p + 2) // 2,)
+    # the reference's check: |refSol[i] - output[i]| < 1e-11 for every DOF
+    assert np.abs(R - ref).max() < 1e-11
+    # the density rows are zero (OptimizedSIPGDensityFlux has no terms)
+    Np = (p + 1) * (p + 2) // 2
+    assert np.all(R.reshape(9, 4, Np)[:, 0, :] == 0.0)
+
+
+@pytest.mark.parametrize("i,value", [(6, 0.3), (7, 1.001), (4, 0.01)])
+def test_reference_sipg_output_pins_the_physics(i, value):
+    """Perturbing the Sutherland ratio, the penalty scaling or the bulk viscosity ratio
+    moves the oracle off the reference's stored values: the pin is not vacuous."""
+    import cns_sipg_case as S
+    p = 2
+    params = [S.GAMMA, S.MACH, 1.0, 1.0, 0.0, 1.0, S.SUTHERLAND, 1.0]
+    params[i] = value
+    opd, gd, U, bnd = S.case(p)
+    opd2 = S.op_desc(p, params)
+    R = orc.evaluate(opd2, gd, U, bnd=bnd)
+    assert np.abs(R - S.reference_values(p)).max() > 1e-6
+
+
+def test_oracle_sipg_vjp_is_transposed_jacobian():
+    import cns_sipg_case as S
+    opd, gd, U, bnd = S.case(2)
+    W = np.random.default_rng(4).uniform(-1, 1, U.size)
+    nd = U.size
+    # Jacobian columns by exact JVPs (small case)
+    A = np.stack([orc.jvp(opd, gd, U, np.eye(nd)[i], bnd=bnd) for i in range(nd)], axis=1)
+    g = orc.vjp(opd, gd, U, W, bnd=bnd)
+    assert np.linalg.norm(g - A.T @ W) <= 1e-12 * np.linalg.norm(A.T @ W)
 
 
 def _load(name):
@@ -173,3 +217,18 @@ def test_oracle_jacobian_matches_jvp(name, make):
     V = np.random.default_rng(6).uniform(-1, 1, pr.n_dofs)
     jv = orc.jvp(opd, gd, pr.U, V)
     assert np.linalg.norm(A @ V - jv) <= 1e-13 * np.linalg.norm(jv)
+
+
+@pytest.mark.parametrize("name,make", [
+    ("transport2d_bnd", lambda: P.transport2d(n=4, k=2, seed=7, periodic=False)),
+    ("euler3d", lambda: P.euler3d(n=3, k=1, seed=5)),
+    ("sip3d", lambda: P.nonlinear_diffusion3d(n=3, k=2, seed=6)),
+    ("advdiff3d", lambda: P.advection_diffusion3d(n=3, k=2, seed=8)),
+])
+def test_oracle_vjp_matches_transposed_jacobian(name, make):
+    pr = make()
+    opd, gd = pr.descs()
+    nd, nc, _ = orc.sizes(opd, gd)
+    W = np.random.default_rng(1).uniform(-1, 1, nc)
+    ref = orc.jacobian_dense(opd, gd, pr.U).T @ W
+    assert np.linalg.norm(orc.vjp(opd, gd, pr.U, W) - ref) <= 1e-13 * np.linalg.norm(ref)

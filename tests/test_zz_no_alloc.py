@@ -10,7 +10,10 @@ Checked through the C-ABI: two calls in a row give the same results as the alloc
 batch entry point (relative L2 <= 1e-12, the tolerance of the parity tests), device free
 memory is the same after the first and after the second call (the first call is where the
 driver loads the library's module with the array, when no other test did before), and
-oversize batches are rejected.
+oversize batches and parts of partitioned grids are rejected. Each round enqueues the
+residual and the VJP call on one stream with no synchronisation between them: the call
+does not wait for its kernel, and the stream orders the second call's use of the shared
+array after the first kernel.
 """
 import ctypes
 
@@ -64,6 +67,18 @@ def test_noalloc_batch_matches_allocating_batch():
         rc = L.bosss_b200_batch_evaluate_noalloc(513, many, C.MODE_RESIDUAL, 1.0, 0.0, C.ptr(U), None, C.ptr(R), 0.0,
                                                  legacy)
         assert rc == C.ERR_BAD_ARG and "512" in C.last_error()
+        # a part of a partitioned grid (ghost planes, global box) is rejected, nothing launched
+        from bosss_b200 import distributed as Dd
+        pr = P.advection_diffusion3d(n=6, k=1, seed=1)
+        part = Dd.SlabPartition(pr.grid, 2, 0, pr.dom[0].Np)
+        pe = Dd.PartEvaluator(pr.op, pr.grid, [1], [1], part)
+        try:
+            one = (ctypes.c_void_p * 1)(pe.handle.value)
+            rc = L.bosss_b200_batch_evaluate_noalloc(1, one, C.MODE_RESIDUAL, 1.0, 0.0, C.ptr(U), None, C.ptr(R), 0.0,
+                                                     legacy)
+            assert rc == C.ERR_BAD_ARG and "partitioned" in C.last_error()
+        finally:
+            pe.Dispose()
     finally:
         for e in evs:
             e.Dispose()
