@@ -31,6 +31,9 @@ COMP_CONSTANT_SOURCE = 3
 COMP_HLLC_DENSITY_FLUX = 10
 COMP_HLLC_MOMENTUM_FLUX = 11
 COMP_HLLC_ENERGY_FLUX = 12
+COMP_CNS_SIPG_DENSITY_FLUX = 20
+COMP_CNS_SIPG_MOMENTUM_FLUX = 21
+COMP_CNS_SIPG_ENERGY_FLUX = 22
 
 # quadrature-order kinds
 QUAD_FIXED = 0
@@ -191,6 +194,10 @@ SIGNATURES = {
     "bosss_b200_xdg_info": (ctypes.c_int, [_P, ctypes.c_int32, _I64, _I64, _I64, _I32, _I32, _I32, _D]),
     "bosss_b200_xdg_get_rules": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P]),
     "bosss_b200_xdg_get_moments": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
+    "bosss_b200_xdg_get_length_scales": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
+    "bosss_b200_boundary_nodes": (ctypes.c_int, [_P, _I64, _P]),
+    "bosss_b200_set_boundary_state": (ctypes.c_int, [_P, _P]),
+    "bosss_b200_xdg_set_length_scales": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
     "bosss_b200_xdg_evaluate": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_double, _P, _P,
                                                ctypes.c_double]),
     "bosss_b200_xdg_evaluate_device": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_double, _P, _P,

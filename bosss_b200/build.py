@@ -3,16 +3,19 @@
 Every CUDA translation unit is compiled by nvcc for ``sm_100a`` only
 (``-gencode arch=compute_100a,code=sm_100a``); the objects are linked into one
 shared library exporting the C-ABI of ``include/bosss_b200.h``. Translation units
-are compiled in parallel and skipped when their object is newer than every source.
+are compiled in parallel and skipped when their object is newer than the unit and every
+local header it includes.
 
 Usage: ``python -m bosss_b200.build [--force] [-j N]``
 """
 import argparse
 import glob
 import os
+import re
 import shutil
 import subprocess
 import sys
+import time
 from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -25,6 +28,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
     "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
     "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include"),
+    # optimise the kernels of one translation unit on several threads (the batched and XDG
+    # units instantiate dozens of kernels)
+    "--split-compile=0",
 ]
 
 
@@ -39,9 +45,23 @@ def _sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
-def _deps():
-    return (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
-            + [os.path.join(ROOT, "include", "bosss_b200.h")])
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(src, seen=None):
+    """Local headers a translation unit includes, transitively (quoted includes only)."""
+    seen = set() if seen is None else seen
+    try:
+        with open(src) as f:
+            text = f.read()
+    except OSError:
+        return seen
+    for inc in _INCLUDE.findall(text):
+        path = os.path.normpath(os.path.join(os.path.dirname(src), inc))
+        if path not in seen and os.path.exists(path):
+            seen.add(path)
+            _deps(path, seen)
+    return seen
 
 
 def _stale(target, inputs):
@@ -55,12 +75,11 @@ def build(force=False, jobs=None, verbose=False):
     """Compile every CUDA translation unit and link the shared library; returns its path."""
     os.makedirs(OBJDIR, exist_ok=True)
     cc = nvcc()
-    deps = _deps()
     objs, todo = [], []
     for src in _sources():
         obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
-        if force or _stale(obj, [src] + deps):
+        if force or _stale(obj, [src] + sorted(_deps(src))):
             todo.append((src, obj))
 
     def compile_one(item):
@@ -68,9 +87,13 @@ def build(force=False, jobs=None, verbose=False):
         cmd = [cc] + NVCC_FLAGS + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
+        t0 = time.time()
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("nvcc failed for %s:\n%s%s" % (src, r.stdout, r.stderr))
+        # the object reflects the sources as they were when the compile started: a header
+        # edited during a long compile leaves it stale
+        os.utime(obj, (t0, t0))
         return src
 
     if todo:

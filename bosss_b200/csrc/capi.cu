@@ -21,6 +21,7 @@
 #include "dg_kernel.cuh"
 #include "dg_registry.h"
 #include "handle.h"
+#include "tc_volume.h"
 
 namespace bosss {
 
@@ -37,6 +38,7 @@ static void ensure_registered() {
         register_scalar3_slab();
         register_euler2();
         register_euler3();
+        register_cns();
     });
 }
 
@@ -158,14 +160,62 @@ static int classify(const bosss_op_desc& op, int D, int& phys, PhysParams& ph) {
     std::memset(&ph, 0, sizeof(ph));
     if (op.n_components < 1 || op.n_components > BOSSS_MAX_COMPONENTS)
         return fail(BOSSS_ERR_BAD_ARG, "operator has no equation components");
-    bool euler = false;
+    bool euler = false, cns = false;
     for (int c = 0; c < op.n_components; ++c) {
         int t = op.components[c].type;
         if (t == BOSSS_COMP_HLLC_DENSITY_FLUX || t == BOSSS_COMP_HLLC_MOMENTUM_FLUX || t == BOSSS_COMP_HLLC_ENERGY_FLUX)
             euler = true;
+        else if (t == BOSSS_COMP_CNS_SIPG_DENSITY_FLUX || t == BOSSS_COMP_CNS_SIPG_MOMENTUM_FLUX ||
+                 t == BOSSS_COMP_CNS_SIPG_ENERGY_FLUX)
+            cns = true;
         else if (t != BOSSS_COMP_SCALAR_TRANSPORT_FLUX && t != BOSSS_COMP_SIP_LAPLACE && t != BOSSS_COMP_CONSTANT_SOURCE)
             return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT,
                         "equation component type " + std::to_string(t) + " has no device functor");
+    }
+    if (cns) {
+        // the complete OptimizedSIPG set: density, D momentum components, energy, one material
+        const int NV = D + 2;
+        if (euler) return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "CNS viscous terms cannot be mixed with HLLC fluxes");
+        if (op.n_domain != NV || op.n_codomain != NV)
+            return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "CNS viscous operator needs D+2 domain and codomain variables");
+        std::vector<int> seen(NV, 0);
+        for (int c = 0; c < op.n_components; ++c) {
+            const auto& cp = op.components[c];
+            if (cp.type != BOSSS_COMP_CNS_SIPG_DENSITY_FLUX && cp.type != BOSSS_COMP_CNS_SIPG_MOMENTUM_FLUX &&
+                cp.type != BOSSS_COMP_CNS_SIPG_ENERGY_FLUX)
+                return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "CNS viscous terms cannot be mixed with other components");
+            if (cp.n_args != NV) return fail(BOSSS_ERR_BAD_ARG, "CNS viscous flux needs D+2 arguments");
+            for (int a = 0; a < NV; ++a)
+                if (cp.args[a] != a)
+                    return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "CNS arguments must be (rho, m_0..m_{D-1}, rhoE)");
+            if (cp.type == BOSSS_COMP_CNS_SIPG_MOMENTUM_FLUX && (cp.params[8] < 0 || cp.params[8] >= D))
+                return fail(BOSSS_ERR_BAD_ARG, "CNS momentum component out of range");
+            const int cod = (cp.type == BOSSS_COMP_CNS_SIPG_DENSITY_FLUX) ? 0
+                            : (cp.type == BOSSS_COMP_CNS_SIPG_ENERGY_FLUX) ? D + 1
+                                                                          : (int)cp.params[8] + 1;
+            if (cp.codomain != cod)
+                return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "CNS flux registered on an unexpected codomain variable");
+            if (seen[cod]++) return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "duplicate CNS viscous flux");
+            for (int i = 0; i < 8; ++i)
+                if (cp.params[i] != op.components[0].params[i])
+                    return fail(BOSSS_ERR_BAD_ARG, "CNS viscous fluxes with different material parameters");
+        }
+        for (int v = 0; v < NV; ++v)
+            if (!seen[v]) return fail(BOSSS_ERR_UNSUPPORTED_COMPONENT, "incomplete CNS viscous flux set");
+        const double* pp = op.components[0].params;
+        if (!(pp[0] > 1.0) || !(pp[1] > 0.0) || !(pp[2] > 0.0) || !(pp[3] > 0.0))
+            return fail(BOSSS_ERR_BAD_ARG, "bad gamma / Mach / Reynolds / Prandtl");
+        if (pp[5] != 0.0 && pp[5] != 1.0) return fail(BOSSS_ERR_BAD_ARG, "viscosity law: 0 (constant) or 1 (Sutherland)");
+        ph.gamma = pp[0];
+        ph.mach = pp[1];
+        ph.re = pp[2];
+        ph.pr = pp[3];
+        ph.visc_ratio = pp[4];
+        ph.visc_law = (int)pp[5];
+        ph.suth = pp[6];
+        ph.pen = pp[7];   // times p^2 in create()
+        phys = PHYS_CNS;
+        return 0;
     }
     if (euler) {
         const int NV = D + 2;
@@ -260,6 +310,25 @@ __global__ void nan_scan_kernel(const double* x, long long n, int* flag) {
         }
 }
 
+// One evaluation launch of `mode` on the cells [a.cbeg, a.cend). A split-precision residual
+// (BOSSS_PRECISION_SPLIT_FP32, whole grids only) runs the tensor-core volume kernel
+// (out = beta*out + alpha*volume terms), then the slab kernel adds the face terms.
+static int launch_eval(bosss_handle* h, int mode, EvalArgs a, cudaStream_t s) {
+    if (h->n_bnd_nodes > 0 && !a.bnd_state)
+        return fail(BOSSS_ERR_BAD_ARG, "the operator's boundary terms need the boundary-state table "
+                                       "(bosss_b200_set_boundary_state)");
+    if (mode == MODE_RES && h->precision == BOSSS_PRECISION_SPLIT_FP32) {
+        if (a.cbeg != 0 || a.cend != h->base.g.J)
+            return fail(BOSSS_ERR_BAD_ARG, "split-precision residuals evaluate whole grids only");
+        int rc = tc_volume_launch(h, a.U, a.out, a.alpha, a.beta, s);
+        if (rc) return rc;
+        a.faces_only = 1;
+        a.beta = 1.0;
+    }
+    CUDA_TRY(h->kern[mode].launch(a, s));
+    return 0;
+}
+
 int run_mode(bosss_handle* h, int mode, double alpha, double beta, const double* U, const double* V,
                     double* out, double time, cudaStream_t s) {
     EvalArgs a = h->base;
@@ -272,7 +341,7 @@ int run_mode(bosss_handle* h, int mode, double alpha, double beta, const double*
     CUDA_TRY(cudaSetDevice(h->device));
     if ((a.vol_flag || a.face_flag) && h->variant != VARIANT_GENERIC)
         return fail(BOSSS_ERR_BAD_ARG, "species masks need the generic kernel");
-    if (h->base.g.J > 0) CUDA_TRY(h->kern[mode].launch(a, s));
+    if (h->base.g.J > 0) return launch_eval(h, mode, a, s);
     return 0;
 }
 
@@ -385,8 +454,9 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     const int Q = std::max(1, (order + 2) / 2);   // smallest Gauss rule with 2Q-1 >= order
     ensure_registered();
     auto& reg = kernel_registry();
-    if (opt && opt->precision != BOSSS_PRECISION_FP64)
-        return fail(BOSSS_ERR_BAD_ARG, "only BOSSS_PRECISION_FP64 is built (no split-FP32 contractions)");
+    const int prec = opt ? opt->precision : BOSSS_PRECISION_FP64;
+    if (prec != BOSSS_PRECISION_FP64 && prec != BOSSS_PRECISION_SPLIT_FP32)
+        return fail(BOSSS_ERR_BAD_ARG, "unknown precision");
     const int want = opt ? opt->kernel : 0;
     if (want < 0 || want > 2) return fail(BOSSS_ERR_BAD_ARG, "bad kernel selector");
     bool have_slab = true, have_generic = true;
@@ -403,6 +473,12 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     for (int m = 0; m < 3; ++m) {
         const bool slab_pays = phys == PHYS_EULER || m == MODE_RES || Q <= 5;
         mode_variant[m] = (want == 2 || (want == 0 && have_slab && slab_pays)) ? VARIANT_SLAB : VARIANT_GENERIC;
+    }
+    if (prec == BOSSS_PRECISION_SPLIT_FP32) {
+        // the face terms of a split-precision residual come from the slab kernel's faces-only pass
+        if (!have_slab || want == 1)
+            return fail(BOSSS_ERR_BAD_ARG, "split precision needs the slab kernel for the face terms");
+        mode_variant[MODE_RES] = VARIANT_SLAB;
     }
     bool need_generic = false;
     for (int m = 0; m < 3; ++m) need_generic = need_generic || mode_variant[m] == VARIANT_GENERIC;
@@ -466,13 +542,14 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
             if (d2 != d) sg *= 0.5 * g.h[d2];
         g.faceSG[d] = sg;
     }
+    if (phys == PHYS_CNS) ph.pen *= (double)K * (double)K;   // SIPGPenaltyScaling * p^2
     if (ph.has_sip) {
         // ipLaplace.cs CoefficientUpdate: max(triangle formula, (p+1)^2)
         const double p = K;
         ph.pen *= std::max((p + 1.0) * (p + D) / D, (p + 1.0) * (p + 1.0));
     }
     h->base.ph = ph;
-    const int NV = (phys == PHYS_EULER) ? D + 2 : 1;
+    const int NV = (phys == PHYS_EULER || phys == PHYS_CNS) ? D + 2 : 1;
     h->ndom = (int64_t)J * NV * np_of(D, K);
     h->ncod = h->ndom;
     h->variant = VARIANT_GENERIC;   // generic unless some mode runs on the slab kernel
@@ -485,6 +562,47 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     if (e != cudaSuccess) {
         delete h;
         return fail(BOSSS_ERR_CUDA, std::string("stream creation: ") + cudaGetErrorString(e));
+    }
+    if (phys == PHYS_CNS) {
+        // boundary faces numbered cell by cell, direction, side; Q^(D-1) nodes each
+        std::vector<long long> off((size_t)J * 2 * D, -1);
+        long long nb = 0;
+        const long long QF = (D == 3) ? (long long)Q * Q : Q;
+        for (long long j = 0; j < J; ++j) {
+            int ijk[3];
+            for (int d = 0; d < 3; ++d) ijk[d] = d < D ? (int)((j / g.stride[d]) % g.n[d]) : 0;
+            for (int d = 0; d < D; ++d)
+                for (int sd = 0; sd < 2; ++sd) {
+                    const int gi = ijk[d] + g.goff[d];
+                    const bool bnd = !g.gper[d] && (sd == 0 ? gi == 0 : gi == g.gn[d] - 1);
+                    if (bnd) {
+                        off[(size_t)j * 2 * D + 2 * d + sd] = nb;
+                        nb += QF;
+                    }
+                }
+        }
+        h->n_bnd_nodes = nb;
+        if (nb > 0) {
+            e = cudaMalloc(&h->d_bnd_off, sizeof(long long) * off.size());
+            if (e == cudaSuccess) e = cudaMemcpy(h->d_bnd_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                bosss_b200_destroy(h);
+                return fail(BOSSS_ERR_CUDA, std::string("boundary table: ") + cudaGetErrorString(e));
+            }
+        }
+    }
+    if (prec == BOSSS_PRECISION_SPLIT_FP32) {
+        h->precision = prec;
+        if (part) {
+            bosss_b200_destroy(h);
+            return fail(BOSSS_ERR_BAD_ARG, "split precision evaluates whole grids (no parts of partitioned grids)");
+        }
+        const int rc = tc_volume_setup(h);
+        if (rc) {
+            const std::string msg = g_last_error;
+            bosss_b200_destroy(h);
+            return fail(rc, msg);
+        }
     }
     *out = h;
     return BOSSS_OK;
@@ -506,7 +624,58 @@ int bosss_b200_destroy(bosss_handle* h) {
     if (h->s_in) cudaStreamDestroy(h->s_in);
     if (h->s_out) cudaStreamDestroy(h->s_out);
     if (h->stream) cudaStreamDestroy(h->stream);
+    cudaFree(h->d_bnd_off);
+    cudaFree(h->d_bnd_state);
+    tc_volume_destroy(h);
     delete h;
+    return BOSSS_OK;
+}
+
+int bosss_b200_boundary_nodes(const bosss_handle* h, int64_t* n_nodes, double* xyz) {
+    if (!h || !n_nodes) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    *n_nodes = h->n_bnd_nodes;
+    if (!xyz || h->n_bnd_nodes == 0) return BOSSS_OK;
+    const GridConst& g = h->base.g;
+    const Tables1D& T = h->base.tab;
+    const int D = h->D, Q = h->Q, QF = (D == 3) ? Q * Q : Q;
+    long long k = 0;
+    for (long long j = 0; j < g.J; ++j) {
+        int ijk[3];
+        for (int d = 0; d < 3; ++d) ijk[d] = d < D ? (int)((j / g.stride[d]) % g.n[d]) : 0;
+        for (int d = 0; d < D; ++d) {
+            const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
+            for (int sd = 0; sd < 2; ++sd) {
+                const int gi = ijk[d] + g.goff[d];
+                if (g.gper[d] || !(sd == 0 ? gi == 0 : gi == g.gn[d] - 1)) continue;
+                for (int qf = 0; qf < QF; ++qf) {
+                    const int q1 = qf % Q, q2 = qf / Q;
+                    double x[3];
+                    for (int dd = 0; dd < D; ++dd) x[dd] = g.lo[dd] + (ijk[dd] + g.goff[dd] + 0.5) * g.h[dd];
+                    x[d] += (sd ? 0.5 : -0.5) * g.h[d];
+                    x[t1] += 0.5 * g.h[t1] * T.xq[q1];
+                    if (D == 3) x[t2] += 0.5 * g.h[t2] * T.xq[q2];
+                    for (int dd = 0; dd < D; ++dd) xyz[k * D + dd] = x[dd];
+                    ++k;
+                }
+            }
+        }
+    }
+    return BOSSS_OK;
+}
+
+int bosss_b200_set_boundary_state(bosss_handle* h, const double* state) {
+    if (!h || !state) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    if (h->n_bnd_nodes == 0) return fail(BOSSS_ERR_BAD_ARG, "the operator takes no boundary-state table");
+    const int NV = (int)(h->ndom / h->base.g.J / np_of(h->D, h->K));
+    const size_t n = (size_t)h->n_bnd_nodes * NV;
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(state[i])) return fail(BOSSS_ERR_BAD_ARG, "non-finite boundary state");
+    CUDA_TRY(cudaSetDevice(h->device));
+    if (!h->d_bnd_state) CUDA_TRY(cudaMalloc(&h->d_bnd_state, sizeof(double) * n));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    CUDA_TRY(cudaMemcpy(h->d_bnd_state, state, sizeof(double) * n, cudaMemcpyHostToDevice));
+    h->base.bnd_off = h->d_bnd_off;
+    h->base.bnd_state = h->d_bnd_state;
     return BOSSS_OK;
 }
 
@@ -548,8 +717,7 @@ int bosss_b200_apply_device(bosss_handle* h, int32_t mode, double alpha, double 
     a.cbeg = cell_begin;
     a.cend = cell_end;
     CUDA_TRY(cudaSetDevice(h->device));
-    CUDA_TRY(h->kern[mode].launch(a, s));
-    return BOSSS_OK;
+    return launch_eval(h, mode, a, s);
 }
 
 // Host-buffer evaluation pipelined over chunks of planes of the slowest-varying grid direction
@@ -586,6 +754,8 @@ static int host_pipelined(bosss_handle* h, const HostJob* jobs, int njobs, const
     for (int k = 0; k < njobs; ++k) bytes += sizeof(double) * (size_t)J * nY(jobs[k]);
     int nch = (int)std::min<long long>(bosss_handle::MAX_CHUNKS / 2, planes / 2);
     if (bytes < (size_t)16 << 20 || h->check_nan) nch = 1;
+    for (int k = 0; k < njobs; ++k)   // split-precision residuals evaluate the whole grid at once
+        if (jobs[k].mode == MODE_RES && h->precision == BOSSS_PRECISION_SPLIT_FP32) nch = 1;
     if (nch < 1) nch = 1;
     if (!h->s_in) CUDA_TRY(cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking));
     if (!h->s_out) CUDA_TRY(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking));
@@ -641,7 +811,8 @@ static int host_pipelined(bosss_handle* h, const HostJob* jobs, int njobs, const
             a.time = time;
             a.cbeg = first_plane(c) * pc;
             a.cend = first_plane(c + 1) * pc;
-            e = h->kern[jobs[k].mode].launch(a, s);
+            rc = launch_eval(h, jobs[k].mode, a, s);
+            if (rc) return finish(rc);
         }
         if (e == cudaSuccess) e = cudaEventRecord(h->ev_done[c], s);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(so, h->ev_done[c], 0);
@@ -660,7 +831,7 @@ static int host_pipelined(bosss_handle* h, const HostJob* jobs, int njobs, const
     e = cudaStreamSynchronize(so);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return finish(fail(BOSSS_ERR_CUDA, cudaGetErrorString(e)));
-    return BOSSS_OK;
+    return tc_volume_check(h);
 }
 
 int bosss_b200_evaluate(bosss_handle* h, double alpha, double beta, const double* U, double* out, double time) {
@@ -715,7 +886,7 @@ int bosss_b200_synchronize(bosss_handle* h) {
     if (!h) return fail(BOSSS_ERR_BAD_ARG, "null handle");
     CUDA_TRY(cudaSetDevice(h->device));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
-    return BOSSS_OK;
+    return tc_volume_check(h);
 }
 
 // ---------------------------------------------------------------- block-sparse matrix

@@ -50,6 +50,19 @@ struct EvalArgs {
     const unsigned char* face_flag;
     // the launch evaluates the cells [cbeg, cend) (the whole grid: 0, J)
     long long cbeg, cend;
+    // 1: face terms only (the slab kernel skips its volume pass; the split-precision path
+    // evaluates the volume terms on the tensor cores first and the faces add with beta = 1)
+    int faces_only;
+    // optional per-cell penalty size factor (1 / cell length scale) of the SIP penalty, in the
+    // local cell order; null: the grid's 1 / CellLengthScale. The XDG bulk sets the species'
+    // cut-cell length scales here (CoefficientSet.CellLengthScales, XLaplace.cs:104-113).
+    const double* cell_pf;
+    // optional boundary-state table: outer values of the NV domain variables at every boundary
+    // face node, bnd_state[(bnd_off[j*2D + 2d + s] + q) * NV + f] for boundary face (d, s) of
+    // cell j and face node q (bnd_off -1: interior face); read by functors whose boundary
+    // terms take a prescribed outer state (CNS viscous terms)
+    const long long* bnd_off;
+    const double* bnd_state;
 };
 
 template <class Phys, int K, int Q, int MODE>
@@ -120,6 +133,20 @@ __device__ __forceinline__ long long neighbour(const GridConst& g, const int* ij
 }
 
 // cj = 1/CellLengthScale = (surface + boundary surface) * 0.5 / volume  (GridData_CellData.cs:683-684)
+__device__ __forceinline__ double cell_cj(const GridConst& g, const int* ijk);
+
+// penalty size factor of a cell: the per-cell array when given (whole grids), else cj
+__device__ __forceinline__ double penalty_size(const double* pf, const GridConst& g, const int* ijk) {
+    if (pf) {
+        long long j = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (d < g.D) j += (long long)ijk[d] * g.stride[d];
+        return pf[j];
+    }
+    return cell_cj(g, ijk);
+}
+
 __device__ __forceinline__ double cell_cj(const GridConst& g, const int* ijk) {
     double cj = 0.0;
 #pragma unroll
@@ -680,9 +707,14 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
             if (inner) {
                 int ijk2[3] = {ijk[0], ijk[1], ijk[2]};
                 ijk2[d] = (int)((nb / g.stride[d]) % g.n[d]);
-                pnlty = args.ph.pen * fmax(cell_cj(g, ijk), cell_cj(g, ijk2));
+                pnlty = args.ph.pen * fmax(penalty_size(args.cell_pf, g, ijk), penalty_size(args.cell_pf, g, ijk2));
             } else {
-                pnlty = 2.0 * args.ph.pen * cell_cj(g, ijk);
+                pnlty = Phys::BND_PEN * args.ph.pen * penalty_size(args.cell_pf, g, ijk);
+            }
+            const double* ub = nullptr;   // outer state of the boundary-state table at this node
+            if (!inner && args.bnd_state) {
+                const long long o = args.bnd_off[(c0 + cl) * (2 * D) + 2 * d + s];
+                if (o >= 0) ub = args.bnd_state + (o + qf) * NV;
             }
             const bool selfA = !inner || s == 1;   // own cell is IN (lower) unless it is the upper cell
             const double* trOwn = TR(cl) + ((s * 2 + 0) * NFI) * NCI * QF;
@@ -711,7 +743,7 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
                     for (int dd = 0; dd < D; ++dd) GAv[e][dd] = GBv[e][dd] = 0.0;
                 }
                 if (inner) Phys::inner(args.ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, gA, GAv);
+                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, ub, gA, GAv);
 #pragma unroll
                 for (int e = 0; e < NC; ++e) {
                     const double gv = selfA ? gA[e] : gB[e];
@@ -739,7 +771,7 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
                     }
                 }
                 if (inner) Phys::inner(args.ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, gA, GAv);
+                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, ub, gA, GAv);
 #pragma unroll
                 for (int e = 0; e < NC; ++e) {
                     const double gv = selfA ? gA[e].d[0] : gB[e].d[0];
@@ -770,7 +802,7 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
                         for (int dd = 0; dd < D; ++dd) (selfA ? GA : GB)[i][dd].d[i * (1 + D) + 1 + dd] = 1.0;
                 }
                 if (inner) Phys::inner(args.ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, gA, GAv);
+                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, ub, gA, GAv);
                 T phi(0.0);
 #pragma unroll
                 for (int e = 0; e < NC; ++e) {

@@ -27,8 +27,12 @@ struct PhysParams {
     double g0, g1[3], g2[3];  // g_D(x) = g0 + sum g1_d x_d + g2_d x_d^2
     int has_source;
     double src;           // constant source value
-    double gamma, mach;   // HLLC
+    double gamma, mach;   // HLLC, CNS viscous terms
     double ims, imach;    // HLLC: 1/(gamma Ma^2), 1/Ma
+    // CNS viscous terms (OptimizedSIPG fluxes): Reynolds and Prandtl numbers, bulk / shear
+    // viscosity ratio, viscosity law (0: mu = 1, 1: Sutherland with ratio suth = S/T0)
+    double re, pr, visc_ratio, suth;
+    int visc_law;
 };
 
 template <class T> __host__ __device__ __forceinline__ T tconst(double a) { return T(a); }
@@ -46,6 +50,7 @@ struct PhysScalar {
     static constexpr bool FACE_V = true;
     static constexpr bool FACE_G = SIP;     // symmetry term of SIP
     static constexpr bool ADJOINT = false;  // VJP by forward mode over the node's state
+    static constexpr double BND_PEN = 2.0;  // boundary penalty = 2 * GetPenalty (ipLaplace.cs:224)
 
     template <class T>
     __device__ static void volume(const PhysParams& p, const T* U, const T (*G)[D], const double* x, T* fV,
@@ -100,9 +105,11 @@ struct PhysScalar {
         }
     }
 
+    // ub: the boundary-state table's outer values at this node (null without a table; unused here)
     template <class T>
     __device__ static void boundary(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
-                                    const double* n, const double* x, T* gA, T (*GAv)[D]) {
+                                    const double* n, const double* x, const double* ub, T* gA, T (*GAv)[D]) {
+        (void)ub;
         if (p.has_transport) {
             double an = 0.0;
 #pragma unroll
@@ -132,6 +139,160 @@ struct PhysScalar {
     }
 };
 
+// --------------------------------------------------------------- compressible Navier-Stokes, viscous SIPG
+// OptimizedSIPG{Density,Momentum,Energy}Flux of the CNS solver (CNS/Diffusion/OptimizedSIPG*Flux.cs):
+// the viscous flux of the D+2 conservative equations F_k = sum_{l,j} G[k][l][j] dU_j/dx_l with
+// Hartmann's G tensors (UpdateTensorComponent / UpdateBoundaryTensorComponent, entries in
+// closed form below), symmetric interior penalty edge terms with the penalty
+// SIPGPenaltyScaling * p^2 * max(cj_in, cj_out) (p.pen = SIPGPenaltyScaling * p^2) inside and
+// p^2 cj_in on boundary faces, where the outer state is the boundary-state table's value at
+// the node (SupersonicInlet.GetBoundaryState). Every edge term applies the same linear map
+// G(U) . X to X = grad U or X = jump (x) normal, so the functor evaluates that map directly.
+template <int D_>
+struct PhysCNSVisc {
+    static constexpr int D = D_;
+    static constexpr int NV = D + 2, NC = D + 2;
+    static constexpr bool GRAD_U = true;
+    static constexpr bool VOL_V = false;
+    static constexpr bool VOL_G = true;
+    static constexpr bool FACE_V = true;
+    static constexpr bool FACE_G = true;
+    static constexpr bool ADJOINT = false;
+    static constexpr double BND_PEN = 1.0;   // NonlinBoundaryEdge_V: p^2 cj_in, not doubled
+
+    // F_k = sum_{l,j} G_e[k][l][j] X[j][l] for equation e (1..D momentum, D+1 energy; 0 density
+    // has no viscous flux) at the state U
+    template <class T>
+    __host__ __device__ static void vflux(const PhysParams& p, int e, const T* U, const T (*X)[D], T* F) {
+        const double MS = p.gamma * p.mach * p.mach, gPr = p.gamma / p.pr;
+        const double a43 = p.visc_ratio + 4.0 / 3.0, a23 = p.visc_ratio - 2.0 / 3.0, a13 = p.visc_ratio + 1.0 / 3.0;
+        const T irho = 1.0 / U[0];
+        T v[D];
+        T q = U[1] * (U[1] * irho) * irho;
+        v[0] = U[1] * irho;
+#pragma unroll
+        for (int i = 1; i < D; ++i) {
+            v[i] = U[1 + i] * irho;
+            q += v[i] * v[i];
+        }
+        const T en = U[D + 1] * irho;
+        const T temp = (en - q * (0.5 * MS)) * (p.gamma - 1.0);
+        T mu = T(1.0);
+        if (p.visc_law == 1) mu = temp * dsqrt(temp) * (1.0 + p.suth) / (temp + p.suth);   // SutherlandLaw
+        const T mh = mu * irho * (1.0 / p.re);
+#pragma unroll
+        for (int k = 0; k < D; ++k) F[k] = T(0.0);
+        if (e >= 1 && e <= D) {
+            const int c = e - 1;
+            // tau_ck on the conservative gradients: d_l v_i = (X[1+i][l] - v_i X[0][l]) / rho
+#pragma unroll
+            for (int k = 0; k < D; ++k)
+#pragma unroll
+                for (int l = 0; l < D; ++l)
+#pragma unroll
+                    for (int i = 0; i < D; ++i) {
+                        double coef = 0.0;
+                        if (l == k && i == c) coef += 1.0;
+                        if (l == c && i == k) coef += 1.0;
+                        if (c == k && i == l) coef += a23;
+                        if (coef != 0.0) F[k] += (X[1 + i][l] - v[i] * X[0][l]) * (coef * mh);
+                    }
+            // two dimensions, y-momentum: the reference's G[x][y][rho] is -v_y mu_hat
+            // (OptimizedSIPGMomentumFlux.cs:767, SIPGMomentumFlux.cs:63)
+            if (D == 2 && c == 1) F[0] += (v[0] - v[D - 1]) * X[0][1] * mh;
+        } else if (e == D + 1) {
+#pragma unroll
+            for (int k = 0; k < D; ++k)
+#pragma unroll
+                for (int l = 0; l < D; ++l) {
+                    if (k == l) {
+                        T g0 = -((v[k] * v[k] * a13 + q) * MS + (en - q * MS) * gPr);
+                        T acc = g0 * X[0][k] + X[D + 1][k] * gPr;
+#pragma unroll
+                        for (int i = 0; i < D; ++i)
+                            acc += X[1 + i][k] * v[i] * (MS * ((i == k) ? (a43 - gPr) : (1.0 - gPr)));
+                        F[k] += acc * mh;
+                    } else {
+                        T acc = -(v[k] * v[l]) * (MS * a13) * X[0][l] + v[l] * MS * X[1 + k][l] +
+                                v[k] * (MS * a23) * X[1 + l][l];
+                        F[k] += acc * mh;
+                    }
+                }
+        }
+    }
+
+    template <class T>
+    __host__ __device__ static void volume(const PhysParams& p, const T* U, const T (*G)[D], const double* x, T* fV,
+                                           T (*fG)[D]) {
+        (void)x; (void)fV;
+#pragma unroll
+        for (int e = 1; e < NC; ++e) {
+            T F[D];
+            vflux(p, e, U, G, F);
+#pragma unroll
+            for (int k = 0; k < D; ++k) fG[e][k] += F[k];   // INonlinVolumeForm_GradV: f[k] += G . grad U
+        }
+    }
+
+    template <class T>
+    __host__ __device__ static void inner(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
+                                          const T* UB, const T (*GB)[D], const double* n, const double* x, T* gA,
+                                          T (*GAv)[D], T* gB, T (*GBv)[D]) {
+        (void)x;
+        T J[NV][D];
+#pragma unroll
+        for (int j = 0; j < NV; ++j)
+#pragma unroll
+            for (int l = 0; l < D; ++l) J[j][l] = (UA[j] - UB[j]) * n[l];
+#pragma unroll
+        for (int e = 1; e < NC; ++e) {
+            T FA[D], FB[D], PA[D], PB[D];
+            vflux(p, e, UA, GA, FA);
+            vflux(p, e, UB, GB, FB);
+            vflux(p, e, UA, J, PA);
+            vflux(p, e, UB, J, PB);
+            T flux = T(0.0);
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                flux += (FA[k] + FB[k]) * (-0.5 * n[k]);            // consistency
+                flux += (PA[k] + PB[k]) * (0.5 * pnlty * n[k]);     // penalty
+                GAv[e][k] -= PA[k] * 0.5;                           // NonlinInternalEdge_GradV
+                GBv[e][k] -= PB[k] * 0.5;
+            }
+            gA[e] += flux;
+            gB[e] -= flux;
+        }
+    }
+
+    template <class T>
+    __host__ __device__ static void boundary(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
+                                             const double* n, const double* x, const double* ub, T* gA,
+                                             T (*GAv)[D]) {
+        (void)x;
+        if (!ub) return;   // create() requires the boundary-state table when the grid has boundary faces
+        T Uo[NV], J[NV][D];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            Uo[j] = T(ub[j]);
+#pragma unroll
+            for (int l = 0; l < D; ++l) J[j][l] = (UA[j] - ub[j]) * n[l];
+        }
+#pragma unroll
+        for (int e = 1; e < NC; ++e) {
+            T F[D], P[D];
+            vflux(p, e, Uo, GA, F);      // G of the outer state applied to grad U_in
+            vflux(p, e, Uo, J, P);
+            T flux = T(0.0);
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                flux += F[k] * (-n[k]) + P[k] * (pnlty * n[k]);
+                GAv[e][k] -= P[k];
+            }
+            gA[e] += flux;
+        }
+    }
+};
+
 // --------------------------------------------------------------- compressible Euler, HLLC
 // OptimizedHLLC{Density,Momentum,Energy}Flux, CompressibleFlowCommon/Convection/*.cs.
 // The three reference components share the same wave-speed estimate; the functor
@@ -145,6 +306,7 @@ struct PhysEuler {
     static constexpr bool VOL_G = true;
     static constexpr bool FACE_V = true;
     static constexpr bool FACE_G = false;
+    static constexpr double BND_PEN = 2.0;   // (no penalty terms)
 
     // FP64 divisions are costly on the GPU (a reciprocal estimate plus Newton steps): every
     // quotient by a state-dependent value below is a product with one reciprocal, and the
@@ -259,9 +421,10 @@ struct PhysEuler {
 
     template <class T>
     __host__ __device__ static void boundary(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
-                                             const double* n, const double* x, T* gA, T (*GAv)[D]) {
+                                             const double* n, const double* x, const double* ub, T* gA,
+                                             T (*GAv)[D]) {
         // no boundary-condition map on the device: create() rejects non-periodic Euler grids
-        (void)p; (void)pnlty; (void)UA; (void)GA; (void)n; (void)x; (void)gA; (void)GAv;
+        (void)p; (void)pnlty; (void)UA; (void)GA; (void)n; (void)x; (void)ub; (void)gA; (void)GAv;
     }
 
     // ---- reverse-mode adjoints (VJP): one primal sweep plus one reverse sweep per node in

@@ -7,7 +7,7 @@
 namespace bosss {
 struct EvalArgs;
 
-enum PhysId { PHYS_TRANSPORT = 0, PHYS_SIP = 1, PHYS_EULER = 2 };
+enum PhysId { PHYS_TRANSPORT = 0, PHYS_SIP = 1, PHYS_EULER = 2, PHYS_CNS = 3 };
 
 // returns the CUDA error of the launch; smem_bytes/cells_per_block describe the tile
 struct KernelEntry {
@@ -25,4 +25,5 @@ void register_scalar3();
 void register_scalar3_slab();
 void register_euler2();
 void register_euler3();
+void register_cns();
 }  // namespace bosss

@@ -238,7 +238,7 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
             for (int d = 0; d < D; ++d) GAv[e][d] = GBv[e][d] = 0.0;
         }
         if (inner) Phys::inner(ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, gA, GAv);
+        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, nullptr, gA, GAv);
 #pragma unroll
         for (int e = 0; e < NC; ++e) {
             if (OV) out(e, 0, (selfA ? gA[e] : gB[e]) * fac);
@@ -264,7 +264,7 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
             }
         }
         if (inner) Phys::inner(ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, gA, GAv);
+        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, nullptr, gA, GAv);
 #pragma unroll
         for (int e = 0; e < NC; ++e) {
             if (OV) out(e, 0, (selfA ? gA[e].d[0] : gB[e].d[0]) * fac);
@@ -311,7 +311,7 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
                 for (int d = 0; d < D; ++d) (selfA ? GA[i][d] : GB[i][d]).d[i * (1 + D) + 1 + d] = 1.0;
         }
         if (inner) Phys::inner(ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, gA, GAv);
+        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, nullptr, gA, GAv);
         T phi(0.0);
 #pragma unroll
         for (int e = 0; e < NC; ++e) {
@@ -626,6 +626,7 @@ __device__ __forceinline__ void slab_tile(const EvalArgs& args, const Tables1D& 
 
     // ---------------------------------------------------------- volume
     constexpr int OUT0 = 0;
+    if (!args.faces_only) {   // uniform over the CTA
     if (active) {
         if (part == 0) slab_volume_interp<Phys, K, Q, MODE, 0>(args, T, CIN(cl), WK(cl), o, q, Aq, dAq);
         else if constexpr (SPLIT > 1) slab_volume_interp<Phys, K, Q, MODE, 1>(args, T, CIN(cl), WK(cl), o, q, Aq, dAq);
@@ -662,6 +663,7 @@ __device__ __forceinline__ void slab_tile(const EvalArgs& args, const Tables1D& 
             slab_project<K, Q, C::VOL_OV, C::VOL_OG, 1, SPLIT, NO * FV>(T, ob, Aq, dAq, q, R);
     }
     __syncthreads();
+    }
 
     // ---------------------------------------------------------- faces
     auto face_pass = [&](auto dirc) {
@@ -699,9 +701,9 @@ __device__ __forceinline__ void slab_tile(const EvalArgs& args, const Tables1D& 
             if (inner) {
                 int ijk2[3] = {cijk[0], cijk[1], cijk[2]};
                 ijk2[DIR] = (int)((nbc / g.stride[DIR]) % g.n[DIR]);
-                pnlty = args.ph.pen * fmax(cell_cj(g, cijk), cell_cj(g, ijk2));
+                pnlty = args.ph.pen * fmax(penalty_size(args.cell_pf, g, cijk), penalty_size(args.cell_pf, g, ijk2));
             } else {
-                pnlty = 2.0 * args.ph.pen * cell_cj(g, cijk);
+                pnlty = Phys::BND_PEN * args.ph.pen * penalty_size(args.cell_pf, g, cijk);
             }
             const bool selfA = !inner || s == 1;
             const double* trOwn = WK(c) + (s * 2 + 0) * C::TRB;

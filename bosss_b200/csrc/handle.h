@@ -9,8 +9,18 @@
 #include "dg_kernel.cuh"
 #include "dg_registry.h"
 
+namespace bosss {
+struct TcVolume;
+}
+
 struct bosss_handle {
     int device = 0;
+    int precision = 0;                  // enum bosss_precision
+    bosss::TcVolume* tcv = nullptr;     // split-precision volume tables (BOSSS_PRECISION_SPLIT_FP32)
+    // boundary-state table of operators with prescribed outer states (CNS viscous terms)
+    int64_t n_bnd_nodes = 0;
+    long long* d_bnd_off = nullptr;
+    double* d_bnd_state = nullptr;
     cudaStream_t stream = nullptr;
     int phys = 0, D = 0, K = 0, Q = 0, variant = 0;
     bosss::EvalArgs base{};

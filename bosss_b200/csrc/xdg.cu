@@ -556,7 +556,7 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
                 nrm[it.dir] = 1.0;
                 int ijk2[3] = {ijk[0], ijk[1], ijk[2]};
                 ijk2[it.dir] = (int)((other / g.stride[it.dir]) % g.n[it.dir]);
-                const double pnlty = a.ph.pen * fmax(cell_cj(g, ijk), cell_cj(g, ijk2));
+                const double pnlty = a.ph.pen * fmax(penalty_size(a.cell_pf, g, ijk), penalty_size(a.cell_pf, g, ijk2));
                 double U_in[1], U_out[1], G_in[1][3], G_out[1][3];
                 U_in[0] = selfLower ? uA : uB;
                 U_out[0] = selfLower ? uB : uA;
@@ -582,9 +582,9 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
                 }
             } else {
                 nrm[it.dir] = it.side ? 1.0 : -1.0;
-                const double pnlty = 2.0 * a.ph.pen * cell_cj(g, ijk);
+                const double pnlty = 2.0 * a.ph.pen * penalty_size(a.cell_pf, g, ijk);
                 double U1[1] = {uA}, gi[1] = {0.0}, Gi[1][3] = {{0, 0, 0}};
-                Phys::boundary(a.ph, pnlty, U1, GA, nrm, x, gi, Gi);
+                Phys::boundary(a.ph, pnlty, U1, GA, nrm, x, nullptr, gi, Gi);
                 #pragma unroll
                 for (int n = 0; n < NP; ++n) {
                     double acc = gi[0] * bphi<K>(LA, n);
@@ -616,8 +616,12 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
 struct IfaceArgs {
     double muA, muB;     // species diffusivities
     double omA, omB;     // flux weights (SIP 1/2, 1/2; SWIP muB/(muA+muB), muA/(muA+muB))
-    double pen;          // penalty_base * penalty_deg * penalty_muFactor (times 1/length scale per cell)
+    double pen;          // penalty_base * penalty_deg * penalty_muFactor (times the size factor per cell)
     double alpha;
+    // the species' penalty size factors (1 / cell length scale, per cell): the interface penalty
+    // takes max(pfA[j], pfB[j]) of the cut cell (XLaplace_Interface.GetPenalty, XLaplace.cs:261-297)
+    const double* pfA;
+    const double* pfB;
 };
 
 template <int K>
@@ -638,9 +642,7 @@ __global__ void k_interface_eval(const long long* __restrict__ cells, const long
         RB[n] = 0.0;
     }
     __syncthreads();
-    int ijk[3];
-    cell_ijk(g, cell, ijk);
-    const double pen = f.pen * cell_cj(g, ijk);
+    const double pen = f.pen * fmax(f.pfA[cell], f.pfB[cell]);
     const double sc = g.scaling;
     double rA[NP], rB[NP];
     for (int n = 0; n < NP; ++n) rA[n] = rB[n] = 0.0;
@@ -827,6 +829,10 @@ struct bosss_xdg {
     // are all uncut species-B cells with standard faces (null: the slab kernel is not available)
     bosss_handle* hs = nullptr;
     long long sb[2] = {0, 0};
+    // per species: cell length scales of the SIP penalty (computed defaults, and the ones in
+    // use: the defaults or the caller's), penalty size factors 1/len on the device
+    std::vector<double> len_default[2], len[2];
+    double* d_pf[2] = {nullptr, nullptr};
     // level-set interface term (set by bosss_b200_xdg_interface_setup)
     bool iface = false;
     IfaceArgs ifa{};
@@ -995,6 +1001,128 @@ static int upload_and_fit(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
     return BOSSS_OK;
 }
 
+// Surface rules of the sphere in every cut cell (height-function quadrature, sphere_surface_box):
+// cells, node offsets (cells + 1), nodes in reference coordinates of the cell (3 per node),
+// weights (physical surface measure) and unit normals (3 per node).
+static void surface_rules(const bosss_xdg* X, int nodes_1d, std::vector<long long>& cells, std::vector<long long>& off,
+                          std::vector<double>& xi, std::vector<double>& w, std::vector<double>& nr) {
+    std::vector<double> gx, gw, tmp;
+    gauss(nodes_1d, gx, gw);
+    const GridConst& g = X->h[0]->base.g;
+    cells.clear();
+    off.assign(1, 0);
+    xi.clear();
+    w.clear();
+    nr.clear();
+    const double c[3] = {X->ls.c[0], X->ls.c[1], X->ls.c[2]};
+    for (int i = 0; i < g.n[0]; ++i)
+        for (int j = 0; j < g.n[1]; ++j)
+            for (int k = 0; k < g.n[2]; ++k) {
+                const int ijk[3] = {i, j, k};
+                double lo[3], hi[3];
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = g.lo[d] + ijk[d] * g.h[d];
+                    hi[d] = lo[d] + g.h[d];
+                }
+                if (ls_box(X->ls, lo, hi, 7) != 0) continue;
+                tmp.clear();
+                sphere_surface_box(lo, hi, c, X->ls.r, gx, gw, 0, tmp);
+                if (tmp.empty()) continue;
+                const size_t nn = tmp.size() / 7;
+                for (size_t q = 0; q < nn; ++q) {
+                    for (int d = 0; d < 3; ++d) xi.push_back(2.0 * (tmp[7 * q + d] - lo[d]) / g.h[d] - 1.0);
+                    w.push_back(tmp[7 * q + 3]);
+                    for (int d = 0; d < 3; ++d) nr.push_back(tmp[7 * q + 4 + d]);
+                }
+                cells.push_back((long long)i * g.stride[0] + (long long)j * g.stride[1] + (long long)k * g.stride[2]);
+                off.push_back(off.back() + (long long)nn);
+            }
+}
+
+// The species' cell length scales without agglomeration, as MultiphaseAgglomerator.LengthScaleAgg
+// computes them from the cut-cell metrics (MultiphaseAgglomerator.cs:744-944): for each cell of the
+// species, len = V / S with V = the species volume in the cell and S = the interface area in the
+// cell plus the species' part of every face of the cell (boundary faces included); len >=
+// machine epsilon * h_min; with no agglomeration, cells whose volume fraction is <= 1e-10 get
+// 1e10 times the uncut cell length scale. V and the face parts come from the fitted rules (the
+// uncut ones are the whole cell / face), the interface area from the surface rules. Cells
+// without the species get NaN (no term reads them).
+static void default_length_scales(const bosss_xdg* X, int s, const std::vector<double>& iface_area,
+                                  std::vector<double>& len) {
+    const GridConst& g = X->h[s]->base.g;
+    const long long J = g.J;
+    const double vol_cell = g.h[0] * g.h[1] * g.h[2];
+    double area[3];
+    for (int d = 0; d < 3; ++d) area[d] = vol_cell / g.h[d];
+    std::vector<double> V(J, 0.0), fa((size_t)J * 6, 0.0);
+    for (long long j = 0; j < J; ++j) {
+        if (X->vol[s][j] == 1) V[j] = vol_cell;
+        for (int f = 0; f < 6; ++f)
+            if (X->face[s][j * 6 + f] == 1) fa[j * 6 + f] = area[f / 2];
+    }
+    const auto& items = X->items[s];
+    const auto& w = X->weights[s];
+    for (const CutItem& it : items) {
+        double sw = 0.0;
+        for (int q = 0; q < it.nnodes; ++q) sw += w[it.node_off + q];
+        if (it.dim == 3) {
+            V[it.cell] = sw * g.detJ;
+        } else {
+            const double a = sw * g.faceSG[it.dir];
+            fa[it.cell * 6 + 2 * it.dir + it.side] = a;
+            int ijk[3];
+            for (int d = 0; d < 3; ++d) ijk[d] = (int)((it.cell / g.stride[d]) % g.n[d]);
+            const int n2 = ijk[it.dir] + (it.side ? 1 : -1);
+            if (n2 >= 0 && n2 < g.n[it.dir]) {
+                const long long nb = it.cell + (it.side ? 1 : -1) * g.stride[it.dir];
+                fa[nb * 6 + 2 * it.dir + (1 - it.side)] = a;
+            } else if (g.periodic[it.dir]) {
+                const long long nb = it.cell + (long long)(it.side ? -(g.n[it.dir] - 1) : (g.n[it.dir] - 1)) * g.stride[it.dir];
+                fa[nb * 6 + 2 * it.dir + (1 - it.side)] = a;
+            }
+        }
+    }
+    const double hmin = std::min(g.h[0], std::min(g.h[1], g.h[2]));
+    len.assign(J, std::nan(""));
+    for (long long j = 0; j < J; ++j) {
+        if (X->vol[s][j] == 0) continue;
+        double S = iface_area[j];
+        for (int f = 0; f < 6; ++f) S += fa[j * 6 + f];
+        double L = std::nan("");
+        if (std::fabs(S) >= 1e-25) L = std::max(V[j] / S, 2.220446049250313e-16 * hmin);
+        if (V[j] / vol_cell <= 1e-10) {
+            // the reference's treatment of vanishing fractions without agglomeration
+            int ijk[3];
+            double cj = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                ijk[d] = (int)((j / g.stride[d]) % g.n[d]);
+                const int nb = g.periodic[d] ? 0 : (ijk[d] == 0) + (ijk[d] == g.n[d] - 1);
+                cj += (2.0 + nb) / g.h[d];
+            }
+            L = 1e10 / (0.5 * cj);
+        }
+        len[j] = L;
+    }
+}
+
+// upload 1/len of species s and point the species' handles at it
+static int apply_length_scales(bosss_xdg* X, int s) {
+    const long long J = (long long)X->len[s].size();
+    std::vector<double> pf(J);
+    for (long long j = 0; j < J; ++j) {
+        const double L = X->len[s][j];
+        pf[j] = (std::isfinite(L) && L > 0.0) ? 1.0 / L : 0.0;
+    }
+    CUDA_TRY(cudaSetDevice(X->device));
+    if (!X->d_pf[s]) CUDA_TRY(cudaMalloc(&X->d_pf[s], sizeof(double) * std::max<long long>(J, 1)));
+    CUDA_TRY(cudaMemcpy(X->d_pf[s], pf.data(), sizeof(double) * J, cudaMemcpyHostToDevice));
+    X->h[s]->base.cell_pf = X->d_pf[s];
+    if (s == 1 && X->hs) X->hs->base.cell_pf = X->d_pf[s];
+    X->ifa.pfA = X->d_pf[0];
+    X->ifa.pfB = X->d_pf[1];
+    return BOSSS_OK;
+}
+
 }  // namespace bosss
 
 extern "C" {
@@ -1086,13 +1214,53 @@ int bosss_b200_xdg_create(const bosss_op_desc* opA, const bosss_op_desc* opB, co
             if (X->sb[1] - X->sb[0] < J && bosss_b200_create(opB, grid, &sopt, &X->hs) != BOSSS_OK) X->hs = nullptr;
         }
     }
+    {
+        // default cell length scales of both species (interface areas from the surface rules)
+        std::vector<long long> cells, off;
+        std::vector<double> xi, w, nr;
+        surface_rules(X, 6, cells, off, xi, w, nr);
+        std::vector<double> ia((size_t)X->h[0]->base.g.J, 0.0);
+        for (size_t r = 0; r < cells.size(); ++r)
+            for (long long q = off[r]; q < off[r + 1]; ++q) ia[cells[r]] += w[q];
+        for (int s = 0; s < 2; ++s) {
+            default_length_scales(X, s, ia, X->len_default[s]);
+            X->len[s] = X->len_default[s];
+            const int rc = apply_length_scales(X, s);
+            if (rc) {
+                bosss_b200_xdg_destroy(X);
+                return rc;
+            }
+        }
+    }
     *out = X;
     return BOSSS_OK;
+}
+
+int bosss_b200_xdg_get_length_scales(const bosss_xdg* X, int32_t species, double* len) {
+    if (!X || species < 0 || species > 1 || !len) return fail(BOSSS_ERR_BAD_ARG, "bad argument");
+    std::copy(X->len[species].begin(), X->len[species].end(), len);
+    return BOSSS_OK;
+}
+
+int bosss_b200_xdg_set_length_scales(bosss_xdg* X, int32_t species, const double* len) {
+    if (!X || species < 0 || species > 1) return fail(BOSSS_ERR_BAD_ARG, "bad argument");
+    const long long J = (long long)X->len_default[species].size();
+    if (len) {
+        for (long long j = 0; j < J; ++j)
+            if (X->vol[species][j] != 0 && !(std::isfinite(len[j]) && len[j] > 0.0))
+                return fail(BOSSS_ERR_BAD_ARG, "length scales of the species' cells must be finite and positive (cell " +
+                                                   std::to_string(j) + ")");
+        X->len[species].assign(len, len + J);
+    } else {
+        X->len[species] = X->len_default[species];
+    }
+    return apply_length_scales(X, species);
 }
 
 int bosss_b200_xdg_destroy(bosss_xdg* X) {
     if (!X) return BOSSS_OK;
     cudaSetDevice(X->device);
+    for (int s = 0; s < 2; ++s) cudaFree(X->d_pf[s]);
     for (int s = 0; s < 2; ++s) {
         cudaFree(X->d_vol[s]);
         cudaFree(X->d_face[s]);
@@ -1279,34 +1447,11 @@ int bosss_b200_xdg_interface_setup(bosss_xdg* X, double mu_A, double mu_B, doubl
     const double pdeg = std::max((K + 1.0) * (K + 3.0) / 3.0, (K + 1.0) * (K + 1.0));
     f.pen = penalty_base * pdeg * pen_mu;
     f.alpha = 1.0;
-    std::vector<double> gx, gw;
-    gauss(nodes_1d, gx, gw);
-    const GridConst& g = X->h[0]->base.g;
-    std::vector<long long> cells, off = {0};
-    std::vector<double> xi, w, nr, tmp;
-    const double c[3] = {X->ls.c[0], X->ls.c[1], X->ls.c[2]};
-    for (int i = 0; i < g.n[0]; ++i)
-        for (int j = 0; j < g.n[1]; ++j)
-            for (int k = 0; k < g.n[2]; ++k) {
-                const int ijk[3] = {i, j, k};
-                double lo[3], hi[3];
-                for (int d = 0; d < 3; ++d) {
-                    lo[d] = g.lo[d] + ijk[d] * g.h[d];
-                    hi[d] = lo[d] + g.h[d];
-                }
-                if (ls_box(X->ls, lo, hi, 7) != 0) continue;
-                tmp.clear();
-                sphere_surface_box(lo, hi, c, X->ls.r, gx, gw, 0, tmp);
-                if (tmp.empty()) continue;
-                const size_t nn = tmp.size() / 7;
-                for (size_t q = 0; q < nn; ++q) {
-                    for (int d = 0; d < 3; ++d) xi.push_back(2.0 * (tmp[7 * q + d] - lo[d]) / g.h[d] - 1.0);
-                    w.push_back(tmp[7 * q + 3]);
-                    for (int d = 0; d < 3; ++d) nr.push_back(tmp[7 * q + 4 + d]);
-                }
-                cells.push_back((long long)i * g.stride[0] + (long long)j * g.stride[1] + (long long)k * g.stride[2]);
-                off.push_back(off.back() + (long long)nn);
-            }
+    std::vector<long long> cells, off;
+    std::vector<double> xi, w, nr;
+    surface_rules(X, nodes_1d, cells, off, xi, w, nr);
+    f.pfA = X->d_pf[0];
+    f.pfB = X->d_pf[1];
     CUDA_TRY(cudaSetDevice(X->device));
     cudaFree(X->d_if_cells);
     cudaFree(X->d_if_off);

@@ -252,6 +252,49 @@ class OptimizedHLLCEnergyFlux(OptimizedHLLCDensityFlux):
     ctype = C.COMP_HLLC_ENERGY_FLUX
 
 
+class CNSMaterial:
+    """Material and numerics of the CNS viscous terms (CNSControl / Material.cs): ideal gas
+    gamma, Mach (default 1/sqrt(gamma): MachScaling = 1), Reynolds, Prandtl, bulk / shear
+    viscosity ratio, Sutherland's law (S/T0 = 110.4/273.15, SutherlandLaw.cs) or mu = 1, and
+    the SIPG penalty scaling."""
+
+    def __init__(self, gamma=1.4, Mach=None, Reynolds=1.0, Prandtl=1.0, ViscosityRatio=0.0, sutherland=True,
+                 sutherland_ratio=110.4 / 273.15, SIPGPenaltyScaling=1.0):
+        self.gamma = float(gamma)
+        self.Mach = float(Mach) if Mach is not None else 1.0 / np.sqrt(gamma)
+        self.Re, self.Pr, self.alpha = float(Reynolds), float(Prandtl), float(ViscosityRatio)
+        self.law = 1.0 if sutherland else 0.0
+        self.suth, self.penalty = float(sutherland_ratio), float(SIPGPenaltyScaling)
+
+
+class OptimizedSIPGDensityFlux(_Component):
+    """``CNS/Diffusion/OptimizedSIPGDensityFlux.cs`` (no viscous density flux)."""
+    ctype = C.COMP_CNS_SIPG_DENSITY_FLUX
+
+    def __init__(self, material, dim=3):
+        self.material = material
+        self.ArgumentOrdering = _euler_args(dim)
+        self.component = 0
+
+    def params(self, dim):
+        m = self.material
+        return [m.gamma, m.Mach, m.Re, m.Pr, m.alpha, m.law, m.suth, m.penalty, float(self.component)]
+
+
+class OptimizedSIPGMomentumFlux(OptimizedSIPGDensityFlux):
+    """``CNS/Diffusion/OptimizedSIPGMomentumFlux.cs``, momentum component ``component``."""
+    ctype = C.COMP_CNS_SIPG_MOMENTUM_FLUX
+
+    def __init__(self, material, component, dim=3):
+        super().__init__(material, dim)
+        self.component = int(component)
+
+
+class OptimizedSIPGEnergyFlux(OptimizedSIPGDensityFlux):
+    """``CNS/Diffusion/OptimizedSIPGEnergyFlux.cs``."""
+    ctype = C.COMP_CNS_SIPG_ENERGY_FLUX
+
+
 # ----------------------------------------------------------------------------- operator
 
 
@@ -488,6 +531,21 @@ class Evaluator:
         C.check(C.lib().bosss_b200_newton_solve(self.handle, C.ptr(U), self.time, ctypes.byref(o), ctypes.byref(r)))
         return U, _report(r)
 
+    def boundary_nodes(self):
+        """Coordinates (n, D) of the boundary face nodes of the boundary-state table."""
+        n = ctypes.c_int64()
+        C.check(C.lib().bosss_b200_boundary_nodes(self.handle, ctypes.byref(n), None))
+        xyz = np.zeros(n.value * self.grid.dim)
+        if n.value:
+            C.check(C.lib().bosss_b200_boundary_nodes(self.handle, ctypes.byref(n), C.ptr(xyz)))
+        return xyz.reshape(n.value, self.grid.dim)
+
+    def SetBoundaryState(self, state):
+        """Outer state (n_nodes, n_domain) at the boundary face nodes, what the C# side's
+        boundary-condition map returns there (e.g. SupersonicInlet.GetBoundaryState)."""
+        a = np.ascontiguousarray(state, dtype=np.float64)
+        C.check(C.lib().bosss_b200_set_boundary_state(self.handle, C.ptr(a)))
+
     def residual_vjp(self, U, W, R=None, G=None, alpha=1.0, beta=0.0):
         """Host arrays: ``R = beta*R + alpha*Op(U)`` and ``G = J(U)^T W`` in one pipelined call
         (U and W cross PCIe once). Returns (R, G)."""
@@ -655,6 +713,23 @@ class XdgEvaluator:
         C.check(C.lib().bosss_b200_xdg_get_moments(self.handle, species, C.ptr(mom)))
         return {"info": info.reshape(ni, 5), "offsets": offs, "nodes": nodes.reshape(nn, 3), "weights": w,
                 "vol_flags": vf, "face_flags": ff, "moments": mom.reshape(ni, 35)}
+
+    def length_scales(self, species):
+        """The species' cell length scales of the SIP penalty (``CoefficientSet.CellLengthScales``
+        of the species); NaN on cells without the species."""
+        out = np.zeros(self.grid.NoOfCells)
+        C.check(C.lib().bosss_b200_xdg_get_length_scales(self.handle, species, C.ptr(out)))
+        return out
+
+    def set_length_scales(self, species, length_scales=None):
+        """The caller's length scales (e.g. agglomerated ones); None restores the defaults."""
+        if length_scales is None:
+            C.check(C.lib().bosss_b200_xdg_set_length_scales(self.handle, species, None))
+            return
+        a = np.ascontiguousarray(length_scales, dtype=np.float64)
+        if a.shape != (self.grid.NoOfCells,):
+            raise C.BosssError(C.ERR_BAD_ARG, "one length scale per cell")
+        C.check(C.lib().bosss_b200_xdg_set_length_scales(self.handle, species, C.ptr(a)))
 
     def Evaluate(self, species, alpha, beta, output, U):
         if hasattr(U, "is_cuda") and U.is_cuda:

@@ -216,3 +216,36 @@ def xdg_poisson3d(n=128, k=2, seed=4000, muA=1.0, muB=10.0, radius=0.4, penalty_
     UA = r.uniform(-1, 1, g.NoOfCells * Np)
     UB = r.uniform(-1, 1, g.NoOfCells * Np)
     return ops[0], ops[1], g, c, UA, UB
+
+
+def hex_block_pattern(n, np_cell, seed=3000, periodic=False):
+    """Block-sparse pattern of a DG operator on an n^3 hex grid (generator cell order): each
+    block row (cell) holds its own block and one per face neighbour (7 blocks inside, fewer at
+    non-periodic boundaries), blocks np_cell x np_cell with seeded values U[-1, 1] -- the
+    shape of the C3 Jacobian (48^3, k = 2: 110,592 block rows x 7 blocks of 10 x 10).
+    Returns (row_ptr, col_idx, values[nnz, np_cell, np_cell])."""
+    J = n ** 3
+    idx = np.arange(J)
+    i, j, k = idx // (n * n), (idx // n) % n, idx % n
+    cols = [idx]
+    valid = [np.ones(J, dtype=bool)]
+    for d, (a, st) in enumerate(((i, n * n), (j, n), (k, 1))):
+        for s in (-1, 1):
+            a2 = a + s
+            ok = (a2 >= 0) & (a2 < n)
+            if periodic:
+                a2 = a2 % n
+                ok = np.ones(J, dtype=bool)
+            cols.append(idx + (a2 - a) * st)
+            valid.append(ok)
+    C = np.stack(cols, axis=1)
+    V = np.stack(valid, axis=1)
+    order = np.argsort(np.where(V, C, J + 1), axis=1, kind="stable")
+    C = np.take_along_axis(C, order, axis=1)
+    V = np.take_along_axis(V, order, axis=1)
+    counts = V.sum(axis=1)
+    row_ptr = np.zeros(J + 1, dtype=np.int64)
+    row_ptr[1:] = np.cumsum(counts)
+    col_idx = C[V].astype(np.int32)
+    vals = rng(seed).uniform(-1.0, 1.0, (len(col_idx), np_cell, np_cell))
+    return row_ptr, col_idx, vals

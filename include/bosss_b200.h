@@ -77,7 +77,18 @@ enum bosss_component_type {
      * momentum: params[2] = component index. Only periodic grids (no boundary-condition map). */
     BOSSS_COMP_HLLC_DENSITY_FLUX = 10,
     BOSSS_COMP_HLLC_MOMENTUM_FLUX = 11,
-    BOSSS_COMP_HLLC_ENERGY_FLUX = 12
+    BOSSS_COMP_HLLC_ENERGY_FLUX = 12,
+    /* OptimizedSIPG{Density,Momentum,Energy}Flux, CNS/Diffusion/OptimizedSIPG*Flux.cs: the
+     * viscous terms of the compressible Navier-Stokes equations (SIPG); arguments = the D+2
+     * conservative variables (rho, m_0..m_{D-1}, rhoE); params[0] gamma, [1] Mach, [2] Reynolds,
+     * [3] Prandtl, [4] bulk/shear viscosity ratio (ViscosityRatio), [5] viscosity law (0: mu = 1,
+     * 1: Sutherland), [6] Sutherland S/T0, [7] SIPGPenaltyScaling, [8] momentum component.
+     * Boundary faces take the outer state from the boundary-state table
+     * (bosss_b200_set_boundary_state), which the C# side fills from its boundary-condition
+     * map (GetBoundaryState at the nodes of bosss_b200_boundary_nodes); not adiabatic walls. */
+    BOSSS_COMP_CNS_SIPG_DENSITY_FLUX = 20,
+    BOSSS_COMP_CNS_SIPG_MOMENTUM_FLUX = 21,
+    BOSSS_COMP_CNS_SIPG_ENERGY_FLUX = 22
 };
 
 /* ---- quadrature-order functions, QuadOrderFunc.cs ---- */
@@ -139,8 +150,17 @@ typedef struct bosss_grid_desc {
 } bosss_grid_desc;
 
 enum bosss_precision {
-    BOSSS_PRECISION_FP64 = 0,        /* plain FP64 path (the only one built) */
-    BOSSS_PRECISION_SPLIT_FP32 = 1   /* reserved: split-FP32 basis contractions; create() rejects it */
+    BOSSS_PRECISION_FP64 = 0,        /* plain FP64 path */
+    /* Split precision: the residual's volume contractions (basis -> quadrature nodes, the
+     * dgemm of DGField_Evaluation.cs:100-110, and the projection onto the test-function
+     * gradients, NECQuadratureVolume.cs:689-716) run on the tensor cores. Each FP64 operand
+     * row is scaled by a power of two and split exactly into 5 signed 8-bit slices; the
+     * slice products accumulate exactly in 32-bit integers and are recombined in FP64, so
+     * results agree with the FP64 path to about 1e-13 relative. The pointwise fluxes, the
+     * face terms and JVP / VJP stay FP64. Built for 3D Euler (HLLC) with DG degree <= 3 and
+     * 4 Gauss nodes per direction, whole grids (create() rejects other operators and parts
+     * of partitioned grids with BOSSS_ERR_BAD_ARG). */
+    BOSSS_PRECISION_SPLIT_FP32 = 1
 };
 
 typedef struct bosss_options {
@@ -181,6 +201,18 @@ int bosss_b200_evaluate(bosss_handle* h, double alpha, double beta, const double
  * (cudaStream_t, NULL = the handle's stream); returns after enqueueing. */
 int bosss_b200_evaluate_device(bosss_handle* h, double alpha, double beta, const double* U_dev,
                                double* out_dev, double time, void* stream);
+
+/* Boundary-state table of an operator whose boundary terms take a prescribed outer state
+ * (the CNS viscous components): boundary_nodes returns the number of boundary face nodes
+ * and, if xyz is not NULL, their physical coordinates (D per node), numbered cell by cell
+ * (local order), then face direction d, then side (lower, upper), then the face's Gauss node
+ * (the direction after d fastest); set_boundary_state uploads n_nodes * n_domain values, the
+ * outer state of every domain variable at every node -- what the reference's
+ * boundary-condition map returns there (CompressibleBoundaryCondMap.GetBoundaryState, e.g.
+ * SupersonicInlet.cs:45-66). Evaluations of such an operator on a grid with boundary faces
+ * fail with BOSSS_ERR_BAD_ARG until the table is set. */
+int bosss_b200_boundary_nodes(const bosss_handle* h, int64_t* n_nodes, double* xyz);
+int bosss_b200_set_boundary_state(bosss_handle* h, const double* state);
 
 /* Directional derivative J(U)*V of the nonlinear operator; replaces the FD `dirder`
  * of the matrix-free Newton-GMRES (Newton.cs:1450-1495). Host buffers. */
@@ -351,6 +383,19 @@ int bosss_b200_xdg_get_rules(const bosss_xdg* X, int32_t species, int64_t* n_ite
 int bosss_b200_xdg_get_moments(const bosss_xdg* X, int32_t species, double* moments);
 int bosss_b200_xdg_evaluate(bosss_xdg* X, int32_t species, double alpha, double beta, const double* U, double* out,
                             double time);
+/* Cell length scales of a species' SIP penalty: the CoefficientSet.CellLengthScales that
+ * XLaplace_Bulk and the base SIPLaplace read (XLaplace.cs:104-113, 193-198; ipLaplace.cs:131-141;
+ * inner faces max(1/len[in], 1/len[out]), boundary faces 2/len[in]) and that the interface term
+ * reads for both species (XLaplace.cs:261-297, max(1/len_A[j], 1/len_B[j])). len: J values in the
+ * grid's cell order. Default, computed at create from the fitted rules as
+ * MultiphaseAgglomerator.LengthScaleAgg does without agglomeration (MultiphaseAgglomerator.cs:744-944):
+ * len = species volume / (interface area + the species' part of every face of the cell), at
+ * least machine epsilon * h, and 1e10 times the uncut length scale for cells whose volume
+ * fraction is <= 1e-10; NaN for cells without the species. set: the caller's scales (e.g. the
+ * agglomerated ones of its cell agglomerator, XOperatorFactoryBase.cs:93-105), finite and
+ * positive on every cell of the species; NULL restores the default. */
+int bosss_b200_xdg_get_length_scales(const bosss_xdg* X, int32_t species, double* len);
+int bosss_b200_xdg_set_length_scales(bosss_xdg* X, int32_t species, const double* len);
 int bosss_b200_xdg_evaluate_device(bosss_xdg* X, int32_t species, double alpha, double beta, const double* U_dev,
                                    double* out_dev, double time, void* stream);
 
@@ -361,8 +406,8 @@ int bosss_b200_xdg_evaluate_device(bosss_xdg* X, int32_t species, double alpha, 
  * setup: mu_A (phi < 0), mu_B (phi > 0), penalty base factor and mode as the XLaplace_Interface
  * constructor (mode BOSSS_IFACE_SWIP or BOSSS_IFACE_SIP, the reference's enum order); builds the
  * surface rules of the sphere on the host (nodes_1d Gauss nodes per interval; <= 0: 6).
- * The penalty's cell length scale is the uncut cell's (the bulk SIP's), not the species'
- * cut-cell length scale of the reference. */
+ * The penalty's size factor is max(1/len_A[j], 1/len_B[j]) of the species' cell length scales
+ * (bosss_b200_xdg_get_length_scales). */
 enum bosss_iface_mode { BOSSS_IFACE_SWIP = 0, BOSSS_IFACE_SIP = 1 };
 int bosss_b200_xdg_interface_setup(bosss_xdg* X, double mu_A, double mu_B, double penalty_base, int32_t mode,
                                    int32_t nodes_1d);

@@ -136,15 +136,16 @@ struct DualV {
     friend double val(const DualV& a) { return a.v; }
 };
 
-// Component types restated by the oracle beyond the C-ABI's device functors (same
-// descriptor struct; the library rejects them with BOSSS_ERR_UNSUPPORTED_COMPONENT).
-//   ORC_COMP_CNS_SIPG_{DENSITY,MOMENTUM,ENERGY}: OptimizedSIPG{Density,Momentum,Energy}Flux,
-//   arguments = the D+2 conservative variables (rho, m_0..m_{D-1}, rhoE);
-//   params[0] gamma, [1] Mach, [2] Reynolds, [3] Prandtl, [4] viscosity ratio (bulk/shear),
-//   [5] viscosity law (0: mu = 1, 1: Sutherland), [6] Sutherland S/T0, [7] SIPG penalty
-//   scaling, [8] momentum component (0-based). Boundary faces take the outer state from the
-//   boundary-state table (one value per domain variable and boundary face node).
-enum { ORC_COMP_CNS_SIPG_DENSITY = 20, ORC_COMP_CNS_SIPG_MOMENTUM = 21, ORC_COMP_CNS_SIPG_ENERGY = 22 };
+// CNS viscous components (BOSSS_COMP_CNS_SIPG_*_FLUX of the C-ABI): arguments = the D+2
+// conservative variables; params[0] gamma, [1] Mach, [2] Reynolds, [3] Prandtl, [4] viscosity
+// ratio (bulk/shear), [5] viscosity law (0: mu = 1, 1: Sutherland), [6] Sutherland S/T0,
+// [7] SIPG penalty scaling, [8] momentum component (0-based). Boundary faces take the outer
+// state from the boundary-state table (one value per domain variable and boundary face node).
+enum {
+    ORC_COMP_CNS_SIPG_DENSITY = BOSSS_COMP_CNS_SIPG_DENSITY_FLUX,
+    ORC_COMP_CNS_SIPG_MOMENTUM = BOSSS_COMP_CNS_SIPG_MOMENTUM_FLUX,
+    ORC_COMP_CNS_SIPG_ENERGY = BOSSS_COMP_CNS_SIPG_ENERGY_FLUX
+};
 
 // ------------------------------------------------------------------ basis
 // Orthonormal polynomials on [-1,1]^D: products of normalised Legendre polynomials,
@@ -974,8 +975,12 @@ static const double* bnd_node(const Problem& P, int j, int d, int s, int q) {
     return o < 0 ? nullptr : P.bnd + (size_t)(o + q) * P.op.n_domain;
 }
 
+// vflags / fflags (nullable): XDG species masks -- a cell's volume integral is taken only where
+// vflags[j] == 1, a face only where fflags[j*2D + 2d + s] == 1 (interior faces by their lower
+// cell's upper side, s = 1)
 template <class T>
-static void evaluate(const Problem& P, double alpha, double beta, const T* U, T* out) {
+static void evaluate(const Problem& P, double alpha, double beta, const T* U, T* out,
+                     const unsigned char* vflags = nullptr, const unsigned char* fflags = nullptr) {
     const int D = P.D, J = P.J, Q = (int)P.vw.size(), nd = P.op.n_domain, nc = P.op.n_codomain;
     const int Nd = P.dom_per_cell, Nc = P.cod_per_cell;
     // output *= beta  (DifferentialOperator.cs:1593-1594)
@@ -984,6 +989,7 @@ static void evaluate(const Problem& P, double alpha, double beta, const T* U, T*
     // ---- volume (NECQuadratureVolume.EvaluateEx)
 #pragma omp parallel for schedule(static)
     for (int j = 0; j < J; ++j) {
+        if (vflags && vflags[j] != 1) continue;
         std::vector<T> R(Nc, T(0.0));
         double c[3];
         cell_center(P, j, c);
@@ -1022,12 +1028,12 @@ static void evaluate(const Problem& P, double alpha, double beta, const T* U, T*
     // ---- edges (NECQuadratureEdge.EvaluateEx): list of (cellIn, cellOut or -1, direction, normal sign)
     struct Edge { int in, out, d; double sgn; };
     std::vector<Edge> edges;
+    auto on = [&](int j, int d, int s) { return !fflags || fflags[(size_t)j * 2 * D + 2 * d + s] == 1; };
     for (int d = 0; d < D; ++d)
         for (int j = 0; j < J; ++j) {
             int up = neighbour(P, j, d, 1);
-            if (up >= 0) edges.push_back({j, up, d, 1.0});
-            else edges.push_back({j, -1, d, 1.0});
-            if (neighbour(P, j, d, 0) < 0) edges.push_back({j, -1, d, -1.0});
+            if (on(j, d, 1)) edges.push_back({j, up >= 0 ? up : -1, d, 1.0});
+            if (neighbour(P, j, d, 0) < 0 && on(j, d, 0)) edges.push_back({j, -1, d, -1.0});
         }
     const int E = (int)edges.size();
     std::vector<T> Rin((size_t)E * Nc, T(0.0)), Rout((size_t)E * Nc, T(0.0));
@@ -1394,32 +1400,26 @@ static void face_integral(const Problem& P, int jin, int jout, int d, double sgn
 
 }  // namespace orc
 
+// len (nullable): the species' cell length scales of the SIP penalty (CoefficientSet.CellLengthScales
+// of the species, XLaplace.cs:104-113 and the base SIPLaplace.GetPenalty, ipLaplace.cs:131-141)
+// in place of the uncut grid's
 extern "C" int orc_xdg_evaluate(const bosss_op_desc* op, const bosss_grid_desc* g, const unsigned char* vol_flags,
                                 const unsigned char* face_flags, int64_t n_items, const int64_t* info,
-                                const int64_t* offs, const double* nodes, const double* weights, const double* U,
-                                double* out) {
+                                const int64_t* offs, const double* nodes, const double* weights, const double* len,
+                                const double* U, double* out) {
     using namespace orc;
     Problem P;
     g_err = setup(P, op, g);
     if (!g_err.empty()) return BOSSS_ERR_BAD_ARG;
+    if (len)
+        for (int j = 0; j < P.J; ++j) P.cj[j] = 1.0 / len[j];
     const int D = P.D, J = P.J, Nc = P.cod_per_cell;
-    std::memset(out, 0, sizeof(double) * (size_t)J * Nc);
-    std::vector<double> Rb(Nc), Ro(Nc);
-    for (int j = 0; j < J; ++j)
-        if (vol_flags[j] == 1) vol_integral(P, j, (int)P.vw.size(), P.vn.data(), P.vw.data(), U, out + (size_t)j * Nc);
-    for (int j = 0; j < J; ++j)
-        for (int d = 0; d < D; ++d)
-            for (int s = 0; s < 2; ++s) {
-                if (face_flags[(size_t)j * 2 * D + 2 * d + s] != 1) continue;
-                const int nb = neighbour(P, j, d, s);
-                if (nb >= 0 && s == 0) continue;   // interior faces from their lower cell
-                std::fill(Rb.begin(), Rb.end(), 0.0);
-                std::fill(Ro.begin(), Ro.end(), 0.0);
-                face_integral(P, j, nb, d, s ? 1.0 : -1.0, P.nQf, P.fn.data(), P.fw.data(), U, Rb.data(), Ro.data());
-                for (int i = 0; i < Nc; ++i) out[(size_t)j * Nc + i] += Rb[i];
-                if (nb >= 0)
-                    for (int i = 0; i < Nc; ++i) out[(size_t)nb * Nc + i] += Ro[i];
-            }
+    // uncut cells and faces of the species: the standard rules, masked
+    evaluate<double>(P, 1.0, 0.0, U, out, vol_flags, face_flags);
+    // cut items with their own rules, per item into buffers, then added in item order
+    std::vector<double> Rb((size_t)n_items * Nc, 0.0), Ro((size_t)n_items * Nc, 0.0);
+    std::vector<int> nbs(n_items, -1);
+#pragma omp parallel for schedule(dynamic, 16)
     for (int64_t r = 0; r < n_items; ++r) {
         const int j = (int)info[r * 5 + 0], dim = (int)info[r * 5 + 1], d = (int)info[r * 5 + 2], s = (int)info[r * 5 + 3];
         const int64_t o0 = offs[r], o1 = offs[r + 1];
@@ -1428,19 +1428,23 @@ extern "C" int orc_xdg_evaluate(const bosss_op_desc* op, const bosss_grid_desc* 
         if (dim == D) {
             for (int q = 0; q < npts; ++q)
                 for (int k = 0; k < D; ++k) xi[(size_t)q * D + k] = nodes[(o0 + q) * 3 + k];
-            vol_integral(P, j, npts, xi.data(), w.data(), U, out + (size_t)j * Nc);
+            vol_integral(P, j, npts, xi.data(), w.data(), U, &Rb[(size_t)r * Nc]);
         } else {
             for (int q = 0; q < npts; ++q)
                 for (int k = 0; k < D - 1; ++k) xi[(size_t)q * (D - 1) + k] = nodes[(o0 + q) * 3 + k];
             const int nb = neighbour(P, j, d, s);
-            std::fill(Rb.begin(), Rb.end(), 0.0);
-            std::fill(Ro.begin(), Ro.end(), 0.0);
-            face_integral(P, j, nb, d, s ? 1.0 : -1.0, npts, xi.data(), w.data(), U, Rb.data(), Ro.data());
-            for (int i = 0; i < Nc; ++i) out[(size_t)j * Nc + i] += Rb[i];
-            if (nb >= 0)
-                for (int i = 0; i < Nc; ++i) out[(size_t)nb * Nc + i] += Ro[i];
+            nbs[r] = nb;
+            face_integral(P, j, nb, d, s ? 1.0 : -1.0, npts, xi.data(), w.data(), U, &Rb[(size_t)r * Nc],
+                          &Ro[(size_t)r * Nc]);
         }
     }
+    for (int64_t r = 0; r < n_items; ++r) {
+        const int j = (int)info[r * 5 + 0];
+        for (int i = 0; i < Nc; ++i) out[(size_t)j * Nc + i] += Rb[(size_t)r * Nc + i];
+        if (nbs[r] >= 0)
+            for (int i = 0; i < Nc; ++i) out[(size_t)nbs[r] * Nc + i] += Ro[(size_t)r * Nc + i];
+    }
+    (void)J;
     return 0;
 }
 
@@ -1554,6 +1558,31 @@ int orc_vjp(const bosss_op_desc* op, const bosss_grid_desc* g, const double* bnd
     else if (need <= 24) vjp<24>(P, U, W, JTW);
     else if (need <= 40) vjp<40>(P, U, W, JTW);
     else vjp<2 * BOSSS_MAX_VARS * 4>(P, U, W, JTW);
+    return 0;
+}
+
+// BlockMsrMatrix.SpMV (BlockMsrMatrix.cs:2554-2990): y = beta*y + alpha*A*x on a block-CSR
+// matrix, blocks dense row-major (row_block x col_block), block rows in parallel.
+int orc_bsr_spmv(int64_t nbr, int32_t br, int32_t bc, const int64_t* rowptr, const int32_t* colidx,
+                 const double* vals, double alpha, const double* x, double beta, double* y) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nbr; ++i) {
+        double acc[64];
+        for (int r = 0; r < br; ++r) acc[r] = 0.0;
+        for (int64_t b = rowptr[i]; b < rowptr[i + 1]; ++b) {
+            const double* blk = vals + b * (int64_t)br * bc;
+            const double* xb = x + (int64_t)colidx[b] * bc;
+            for (int r = 0; r < br; ++r) {
+                double s = 0.0;
+                for (int c = 0; c < bc; ++c) s += blk[r * bc + c] * xb[c];
+                acc[r] += s;
+            }
+        }
+        for (int r = 0; r < br; ++r) {
+            double& yr = y[i * br + r];
+            yr = (beta == 0.0) ? alpha * acc[r] : beta * yr + alpha * acc[r];
+        }
+    }
     return 0;
 }
 

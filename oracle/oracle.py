@@ -32,12 +32,14 @@ def lib():
         L.orc_vjp.argtypes = [P, P, P, P, P, P]
         L.orc_jacobian_blocks.argtypes = [P, P, P, P, P, P]
         L.orc_boundary_nodes.argtypes = [P, P, P]
+        L.orc_bsr_spmv.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, P, P, P, ctypes.c_double, P,
+                                   ctypes.c_double, P]
         L.orc_sizes.argtypes = [P, P, P, P, P]
         L.orc_gauss_rule.argtypes = [ctypes.c_int, P, P]
         L.orc_basis_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P]
         L.orc_basis_monomials.argtypes = [ctypes.c_int, ctypes.c_int, P, P]
         L.orc_threads.argtypes = [ctypes.c_int]
-        L.orc_xdg_evaluate.argtypes = [P, P, P, P, ctypes.c_int64, P, P, P, P, P, P]
+        L.orc_xdg_evaluate.argtypes = [P, P, P, P, ctypes.c_int64, P, P, P, P, P, P, P]
         L.orc_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         _lib = L
     return _lib
@@ -187,17 +189,21 @@ def basis_monomials(D, k):
     return out
 
 
-def xdg_evaluate(opd, gd, rules, U):
-    """XDG bulk evaluation of one species with given rules (flags, cut items, nodes, weights)."""
+def xdg_evaluate(opd, gd, rules, U, length_scales=None):
+    """XDG bulk evaluation of one species with given rules (flags, cut items, nodes, weights).
+    ``length_scales``: the species' cell length scales of the SIP penalty (one per cell,
+    ``CoefficientSet.CellLengthScales`` of the species, XLaplace.cs:104-113, ipLaplace.cs:131-141);
+    None: the uncut grid's (Vol / (surface / 2))."""
     nd, nc, _ = sizes(opd, gd)
     U = np.ascontiguousarray(U, dtype=np.float64)
     out = np.zeros(nc)
     info = np.ascontiguousarray(rules["info"], dtype=np.int64)
+    ls = None if length_scales is None else np.ascontiguousarray(length_scales, dtype=np.float64)
     _check(lib().orc_xdg_evaluate(ctypes.byref(opd), ctypes.byref(gd), _p(np.ascontiguousarray(rules["vol_flags"])),
                                   _p(np.ascontiguousarray(rules["face_flags"])), len(info), _p(info),
                                   _p(np.ascontiguousarray(rules["offsets"], dtype=np.int64)),
                                   _p(np.ascontiguousarray(rules["nodes"])), _p(np.ascontiguousarray(rules["weights"])),
-                                  _p(U), _p(out)))
+                                  None if ls is None else _p(ls), _p(U), _p(out)))
     return out
 
 
@@ -227,15 +233,18 @@ def rk_steps(opd, gd, U, a, b, c, dt, nsteps=1):
     return y
 
 
-def xdg_interface(nodes_xyz, periodic, k, rules, UA, UB, muA, muB, penalty_base, mode, alpha=1.0):
+def xdg_interface(nodes_xyz, periodic, k, rules, UA, UB, muA, muB, penalty_base, mode, alpha=1.0,
+                  length_scales=None):
     """Level-set interface term, restated from XLaplace_Interface.InnerEdgeForm
     (XNSECommon/XLaplace.cs:229-297, GetPenalty :261-297, ComputeScaling :302-322,
     CoefficientUpdate :331-341) and the two-species scatter of
     NECQuadratureLevelSet.SaveIntegrationResults (NECQuadratureLevelSet.cs:622-661): for every
     cut cell and surface node, Ret(vA, vB) with (vA, vB) = (phi_n, 0) is added to species A's
     row n and with (0, phi_n) to species B's. Basis values come from the oracle's own basis
-    (monomial representation); the surface rule is given. The penalty length scale is the
-    uncut cell's (Vol / (surface / 2), boundary faces counted twice). Returns (outA, outB)."""
+    (monomial representation); the surface rule is given. ``length_scales`` = (species A,
+    species B) cell length scales: the penalty size factor is max(1 / len_A[j], 1 / len_B[j])
+    of the cut cell j (GetPenalty, XLaplace.cs:261-297); None: the uncut cell's
+    (Vol / (surface / 2), boundary faces counted twice). Returns (outA, outB)."""
     from math import comb
     h = [float(x[1] - x[0]) for x in nodes_xyz]
     n = [len(x) - 1 for x in nodes_xyz]
@@ -254,11 +263,15 @@ def xdg_interface(nodes_xyz, periodic, k, rules, UA, UB, muA, muB, penalty_base,
     cells, offs = rules["cells"], rules["offsets"]
     for r, cell in enumerate(cells):
         ijk = (cell // (n[1] * n[2]), (cell // n[2]) % n[1], cell % n[2])
-        cj = 0.0
-        for d in range(3):
-            nb = 0 if periodic[d] else int(ijk[d] == 0) + int(ijk[d] == n[d] - 1)
-            cj += (2.0 + nb) / h[d]
-        pen = penalty_base * pdeg * pen_mu * 0.5 * cj
+        if length_scales is None:
+            cj = 0.0
+            for d in range(3):
+                nb = 0 if periodic[d] else int(ijk[d] == 0) + int(ijk[d] == n[d] - 1)
+                cj += (2.0 + nb) / h[d]
+            size = 0.5 * cj
+        else:
+            size = max(1.0 / length_scales[0][cell], 1.0 / length_scales[1][cell])
+        pen = penalty_base * pdeg * pen_mu * size
         sl = slice(offs[r], offs[r + 1])
         phi, dphi = basis_eval(3, k, rules["nodes"][sl])          # (Np, q), (Np, q, 3)
         N = rules["normals"][sl]
@@ -275,3 +288,15 @@ def xdg_interface(nodes_xyz, periodic, k, rules, UA, UB, muA, muB, penalty_base,
         outA[cell * Np:(cell + 1) * Np] += alpha * (retA @ w)
         outB[cell * Np:(cell + 1) * Np] += alpha * (retB @ w)
     return outA, outB
+
+
+def bsr_spmv(row_ptr, col_idx, values, alpha, x, beta, y):
+    """BlockMsrMatrix.SpMV restated: y = beta*y + alpha*A*x; values[nnz, row_block, col_block]."""
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    ci = np.ascontiguousarray(col_idx, dtype=np.int32)
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.array(y, dtype=np.float64, copy=True)
+    assert v.ndim == 3 and y.size == (len(rp) - 1) * v.shape[1]
+    lib().orc_bsr_spmv(len(rp) - 1, v.shape[1], v.shape[2], _p(rp), _p(ci), _p(v), alpha, _p(x), beta, _p(y))
+    return y

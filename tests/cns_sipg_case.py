@@ -44,10 +44,10 @@ MACH = 1.0 / math.sqrt(GAMMA)
 SUTHERLAND = 110.4 / 273.15
 N_CELLS = 3
 
-# oracle-side component ids of the OptimizedSIPG{Density,Momentum,Energy}Flux
-COMP_CNS_SIPG_DENSITY = 20
-COMP_CNS_SIPG_MOMENTUM = 21
-COMP_CNS_SIPG_ENERGY = 22
+# component ids of the OptimizedSIPG{Density,Momentum,Energy}Flux (C-ABI and oracle)
+COMP_CNS_SIPG_DENSITY = C.COMP_CNS_SIPG_DENSITY_FLUX
+COMP_CNS_SIPG_MOMENTUM = C.COMP_CNS_SIPG_MOMENTUM_FLUX
+COMP_CNS_SIPG_ENERGY = C.COMP_CNS_SIPG_ENERGY_FLUX
 
 
 def primitive(x, y):
@@ -166,3 +166,24 @@ def case(p):
 def reference_values(p):
     with open(os.path.join(HERE, "golden", "sipg_consistency_p%d.json" % p)) as f:
         return np.array(json.load(f)["values"])
+
+
+def problem(p):
+    """The case registered through the operator mirror the way the CNS solver builds its
+    diffusive operator (OperatorFactory / Operator.ToSpatialOperator, CNS/EquationSystem/
+    Operator.cs:143-174): (op, grid, domain fields, codomain fields)."""
+    from bosss_b200 import operator as O
+    x = np.linspace(0.0, 2.0 * math.pi, N_CELLS + 1)
+    g = O.Cartesian2DGrid(x, x, False, False)
+    names = ["rho", "m0", "m1", "rhoE"]
+    op = O.DifferentialOperator(names, [], names, O.QuadOrderFunc.NonLinear(2))
+    mat = O.CNSMaterial(gamma=GAMMA, Mach=MACH, Reynolds=1.0, Prandtl=1.0, ViscosityRatio=0.0, sutherland=True,
+                        sutherland_ratio=SUTHERLAND, SIPGPenaltyScaling=1.0)
+    op.EquationComponents["rho"].Add(O.OptimizedSIPGDensityFlux(mat, 2))
+    for d in range(2):
+        op.EquationComponents["m%d" % d].Add(O.OptimizedSIPGMomentumFlux(mat, d, 2))
+    op.EquationComponents["rhoE"].Add(O.OptimizedSIPGEnergyFlux(mat, 2))
+    op.Commit()
+    dom = [O.DGField(g, p, n) for n in names]
+    cod = [O.DGField(g, p, n) for n in names]
+    return op, g, dom, cod

@@ -104,3 +104,32 @@ def test_batch_schedules_match_single_instances(tmp_path, schedule):
         assert rel(Rb[sl].cpu().numpy(), Rs.cpu().numpy()) <= 1e-13
         assert rel(JV[sl].cpu().numpy(), JVs.cpu().numpy()) <= 1e-13
         assert rel(Gb[sl].cpu().numpy(), Gs.cpu().numpy()) <= 1e-13
+
+
+def test_full_c5_mix_one_instance_per_class_matches_oracle():
+    """The full seed-5000 mix (256 instances, 16..48^3, k = 1..4, 188M DOFs): residual and
+    VJP of the whole batch in one launch per mode; the first instance of every
+    (grid size, degree) class against the oracle's residual and exact VJP."""
+    import torch
+    probs = P.batched_advection_diffusion(n_instances=256, seed=5000)
+    n = sum(p.n_dofs for p in probs)
+    U = torch.from_numpy(np.concatenate([p.U for p in probs])).cuda()
+    W = torch.from_numpy(np.random.default_rng(7).uniform(-1, 1, n)).cuda()
+    with O.BatchEvaluator(probs) as b:
+        off = b.dom_offsets
+        R = b.evaluate(C.MODE_RESIDUAL, U)
+        G = b.evaluate(C.MODE_VJP, U, W)
+        torch.cuda.synchronize()
+    seen = {}
+    for i, p in enumerate(probs):
+        key = (p.grid.n[0], p.dom[0].degree)
+        if key not in seen:
+            seen[key] = i
+    assert len(seen) == 16, sorted(seen)
+    for key, i in sorted(seen.items()):
+        p = probs[i]
+        sl = slice(int(off[i]), int(off[i + 1]))
+        opd, gd = p.descs()
+        Wi = W[sl].cpu().numpy()
+        assert rel(R[sl].cpu().numpy(), orc.evaluate(opd, gd, p.U)) <= 1e-12, key
+        assert rel(G[sl].cpu().numpy(), orc.vjp(opd, gd, p.U, Wi)) <= 1e-12, key

@@ -1,8 +1,9 @@
 """GPU parity of the sm_100a path against the CPU FP64 oracle, through the C-ABI.
 
 Tolerances (FP64 plain path): relative L2 error <= 1e-12 against the oracle for
-residuals and JVPs; the VJP is checked against the transpose of the oracle's
-assembled Jacobian (small grids) and, at full size, through the adjoint identity
+residuals, JVPs and VJPs at the small sizes and at the full config sizes (C1 64^2 k=2,
+C2 32^3 k=3, C3 48^3 k=2 / 24^3 k=3 / 16^3 k=4); the VJP also against the transpose of
+the oracle's assembled Jacobian (small grids) and through the adjoint identity
 w.(J v) = (J^T w).v.
 """
 import ctypes
@@ -231,13 +232,22 @@ def test_adjoint_identity_full_size(name, make):
     assert abs(a - b) <= 1e-11 * (np.linalg.norm(W) * np.linalg.norm(jv)), (a, b)
 
 
-def test_jvp_full_size_matches_oracle():
-    pr = P.nonlinear_diffusion3d(n=48, k=2, seed=3000)
-    V = np.random.default_rng(5).uniform(-1, 1, pr.n_dofs)
-    ref = orc.jvp(*pr.descs(), pr.U, V)
+@pytest.mark.parametrize("name,make", FULL, ids=[s[0] for s in FULL])
+def test_jvp_vjp_full_size_match_oracle(name, make):
+    """J V and J^T W at the full config sizes against the oracle's exact products (the
+    oracle's VJP differentiates W . Op(U) node by node, edge-centric, with dense tables)."""
+    pr = make()
+    opd, gd = pr.descs()
+    r = np.random.default_rng(5)
+    V = r.uniform(-1, 1, pr.n_dofs)
+    W = r.uniform(-1, 1, pr.n_dofs)
+    ref_jv = orc.jvp(opd, gd, pr.U, V)
+    ref_jtw = orc.vjp(opd, gd, pr.U, W)
     with pr.evaluator() as ev:
         jv = ev.jvp(pr.U, V)
-    assert rel(jv, ref) <= TOL, rel(jv, ref)
+        jtw = ev.vjp(pr.U, W)
+    assert rel(jv, ref_jv) <= TOL, rel(jv, ref_jv)
+    assert rel(jtw, ref_jtw) <= TOL, rel(jtw, ref_jtw)
 
 
 def test_jvp_matches_central_fd_full_size():
@@ -368,3 +378,23 @@ def test_host_pipeline_matches_device_path(case):
     for a, b in ((host_r, dev_r), (host_jv, dev_jv), (host_g, dev_g), (comb_r, dev_r), (comb_g, dev_g)):
         b = b.cpu().numpy()
         assert np.max(np.abs(a - b)) <= 1e-14 * np.max(np.abs(b))
+
+
+def test_block_sparse_spmv_full_c3_pattern():
+    """BlockMsrMatrix.SpMV at the C3 Jacobian's block pattern (48^3, k = 2: 110,592 block rows,
+    7 blocks of 10 x 10 inside) against the oracle's restatement, y = beta*y + alpha*A*x."""
+    pytest.importorskip("torch")
+    rp, ci, vals = P.hex_block_pattern(48, 10)
+    nbr = len(rp) - 1
+    r = np.random.default_rng(12)
+    x = r.uniform(-1, 1, nbr * 10)
+    y0 = r.uniform(-1, 1, nbr * 10)
+    ref = orc.bsr_spmv(rp, ci, vals, 0.5, x, -2.0, y0)
+    A = O.BlockMsrMatrix.from_blocks(nbr, nbr, rp, ci, vals)
+    try:
+        y = A.SpMV(0.5, x, -2.0, y0.copy())
+        assert rel(y, ref) <= 1e-14, rel(y, ref)
+        y = A.SpMV(1.0, x, 0.0, np.full_like(y0, np.nan))   # beta = 0 overwrites
+        assert rel(y, orc.bsr_spmv(rp, ci, vals, 1.0, x, 0.0, y0)) <= 1e-14
+    finally:
+        A.Dispose()

@@ -3,8 +3,12 @@
 * the device weight solve equals numpy's minimum-norm least squares (what DGELSY returns)
   on the same node sets and moments;
 * the species volumes integrated with the rules reproduce the sphere volume;
-* the per-species evaluation equals the oracle's restatement given the same rules;
-* the full-size case (128^3, k=2) builds its rules and evaluates both species.
+* the per-species evaluation equals the oracle's restatement given the same rules and
+  species cell length scales;
+* the default species length scales equal species volume / (interface area + the species'
+  face areas) recomputed here from the rules (MultiphaseAgglomerator.LengthScaleAgg without
+  agglomeration), and caller-supplied (e.g. agglomerated) scales take effect;
+* the full-size case (128^3, k=2): both species equal the oracle with the same rules.
 """
 import numpy as np
 import pytest
@@ -86,7 +90,7 @@ def test_xdg_evaluate_matches_oracle(xdg_small):
     opA, opB, g, c, UA, UB, X = xdg_small
     for s, (op, U) in enumerate([(opA, UA), (opB, UB)]):
         R = X.rules(s)
-        ref = orc.xdg_evaluate(op.descriptor([2], [2], 3), g.desc(), R, U)
+        ref = orc.xdg_evaluate(op.descriptor([2], [2], 3), g.desc(), R, U, length_scales=X.length_scales(s))
         out = np.full_like(U, 3.0)     # beta = 0 overwrites every cell
         X.Evaluate(s, 1.0, 0.0, out, U)
         assert rel(out, ref) <= 1e-12, (s, rel(out, ref))
@@ -101,16 +105,92 @@ def test_xdg_evaluate_matches_oracle(xdg_small):
         assert np.array_equal(out[absent], 0.25 * prev[absent])
 
 
-def test_xdg_full_size():
+def test_xdg_full_size_matches_oracle():
+    """The full 128^3, k=2 case: both species against the oracle with the same rules."""
     import torch
     opA, opB, g, c, UA, UB = P.xdg_poisson3d(n=128, k=2, seed=4000)
     with O.XdgEvaluator(opA, opB, g, 2, c, 0.4) as X:
         infA, infB = X.info(0), X.info(1)
         assert 5000 < infA["cut_cells"] < 20000
         assert infA["min_nodes"] >= 1 and infA["max_nodes"] <= 128
-        for s, U in ((0, UA), (1, UB)):
+        for s, (op, U) in enumerate([(opA, UA), (opB, UB)]):
             Ud = torch.from_numpy(U).cuda()
             out = torch.zeros_like(Ud)
             X.Evaluate(s, 1.0, 0.0, out, Ud)
             torch.cuda.synchronize()
-            assert torch.isfinite(out).all()
+            ref = orc.xdg_evaluate(op.descriptor([2], [2], 3), g.desc(), X.rules(s), U,
+                                   length_scales=X.length_scales(s))
+            assert rel(out.cpu().numpy(), ref) <= 1e-12, (s, rel(out.cpu().numpy(), ref))
+
+
+def _default_length_scales(X, s, n):
+    """Independent recomputation from the rules: V / (A_interface + sum of the species' face areas)."""
+    R = X.rules(s)
+    h = 2.0 / n
+    J = n ** 3
+    vol = h ** 3
+    V = np.where(R["vol_flags"] == 1, vol, 0.0)
+    fa = np.where(R["face_flags"].reshape(J, 6) == 1, h * h, 0.0)
+    stride = [n * n, n, 1]
+    for r, (cell, dim, d, side, deg) in enumerate(R["info"]):
+        sw = R["weights"][R["offsets"][r]:R["offsets"][r + 1]].sum()
+        if dim == 3:
+            V[cell] = sw * (h / 2) ** 3
+        else:
+            a = sw * (h / 2) ** 2
+            fa[cell, 2 * d + side] = a
+            i = (cell // stride[d]) % n
+            i2 = i + (1 if side else -1)
+            if 0 <= i2 < n:
+                fa[cell + (1 if side else -1) * stride[d], 2 * d + (1 - side)] = a
+    X.SetInterface(1.0, 10.0, 4.0, X.SIP, nodes_1d=6)
+    IR = X.interface_rules()
+    ia = np.zeros(J)
+    for r, cell in enumerate(IR["cells"]):
+        ia[cell] += IR["weights"][IR["offsets"][r]:IR["offsets"][r + 1]].sum()
+    S = ia + fa.sum(axis=1)
+    L = np.full(J, np.nan)
+    m = R["vol_flags"] != 0
+    L[m] = np.maximum(V[m] / S[m], 2.220446049250313e-16 * h)
+    return L, V, m
+
+
+def test_default_length_scales_from_rules(xdg_small):
+    opA, opB, g, c, UA, UB, X = xdg_small
+    for s in (0, 1):
+        L, V, m = _default_length_scales(X, s, 10)
+        got = X.length_scales(s)
+        assert np.array_equal(np.isnan(got), ~m)
+        assert np.allclose(got[m], L[m], rtol=1e-13, atol=0)
+        # uncut cells of the species: h^3 / (6 h^2); cut cells differ from the uncut value
+        h = 0.2
+        uncut = (X.rules(s)["vol_flags"] == 1)
+        assert np.allclose(got[uncut], h / 6, rtol=1e-14)
+        cut = X.rules(s)["vol_flags"] == 2
+        assert np.abs(got[cut] - h / 6).max() > 0.1 * h / 6
+
+
+def test_caller_length_scales_take_effect(xdg_small):
+    """Caller-supplied (e.g. agglomerated) length scales: GPU == oracle with the same scales,
+    different from the defaults' result; None restores the defaults."""
+    opA, opB, g, c, UA, UB, X = xdg_small
+    s = 0
+    R = X.rules(s)
+    base = X.length_scales(s)
+    L = np.where(np.isnan(base), np.nan, np.random.default_rng(3).uniform(0.01, 0.05, base.size))
+    try:
+        X.set_length_scales(s, L)
+        assert np.array_equal(np.nan_to_num(X.length_scales(s), nan=-1), np.nan_to_num(L, nan=-1))
+        ref = orc.xdg_evaluate(opA.descriptor([2], [2], 3), g.desc(), R, UA, length_scales=L)
+        out = np.zeros_like(UA)
+        X.Evaluate(s, 1.0, 0.0, out, UA)
+        assert rel(out, ref) <= 1e-12
+        ref0 = orc.xdg_evaluate(opA.descriptor([2], [2], 3), g.desc(), R, UA, length_scales=base)
+        assert rel(ref, ref0) > 1e-3
+        bad = L.copy()
+        bad[np.flatnonzero(~np.isnan(L))[0]] = 0.0
+        with pytest.raises(Exception):
+            X.set_length_scales(s, bad)
+    finally:
+        X.set_length_scales(s, None)
+    assert np.array_equal(np.nan_to_num(X.length_scales(s), nan=-1), np.nan_to_num(base, nan=-1))

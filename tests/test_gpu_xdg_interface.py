@@ -67,7 +67,9 @@ def test_interface_matches_oracle(mode, n):
     with O.XdgEvaluator(opA, opB, g, k, c, R0) as X:
         X.SetInterface(1.0, 10.0, 4.0, mode, 5)
         rules = X.interface_rules()
-        refA, refB = orc.xdg_interface(node_vectors(g), g.periodic, k, rules, UA, UB, 1.0, 10.0, 4.0, mode, alpha=0.7)
+        lens = (X.length_scales(0), X.length_scales(1))
+        refA, refB = orc.xdg_interface(node_vectors(g), g.periodic, k, rules, UA, UB, 1.0, 10.0, 4.0, mode, alpha=0.7,
+                                       length_scales=lens)
         # host-buffer entry point: adds to the given outputs
         oA = np.full(UA.size, 0.25)
         oB = np.full(UB.size, -0.5)
