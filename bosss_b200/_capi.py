@@ -56,6 +56,7 @@ MODE_VJP = 2
 KERNEL_AUTO = 0
 KERNEL_GENERIC = 1
 KERNEL_SLAB = 2
+KERNEL_FACES = 3
 
 PRECISION_FP64 = 0
 PRECISION_SPLIT_FP32 = 1

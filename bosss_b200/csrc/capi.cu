@@ -21,6 +21,7 @@
 #include "dg_kernel.cuh"
 #include "dg_registry.h"
 #include "handle.h"
+#include "faces_euler.h"
 #include "tc_volume.h"
 
 namespace bosss {
@@ -313,17 +314,27 @@ __global__ void nan_scan_kernel(const double* x, long long n, int* flag) {
 // One evaluation launch of `mode` on the cells [a.cbeg, a.cend). A split-precision residual
 // (BOSSS_PRECISION_SPLIT_FP32, whole grids only) runs the tensor-core volume kernel
 // (out = beta*out + alpha*volume terms), then the slab kernel adds the face terms.
+// A face-once handle (3D Euler) evaluates residual and VJP as the slab kernel's volume pass
+// (or the tensor-core volume kernel) followed by the face kernels of faces_euler.cu.
 static int launch_eval(bosss_handle* h, int mode, EvalArgs a, cudaStream_t s) {
     if (h->n_bnd_nodes > 0 && !a.bnd_state)
         return fail(BOSSS_ERR_BAD_ARG, "the operator's boundary terms need the boundary-state table "
                                        "(bosss_b200_set_boundary_state)");
-    if (mode == MODE_RES && h->precision == BOSSS_PRECISION_SPLIT_FP32) {
+    const bool split = mode == MODE_RES && h->precision == BOSSS_PRECISION_SPLIT_FP32;
+    const bool once = h->faces_once && (mode == MODE_RES || mode == MODE_VJP);
+    if (split) {
         if (a.cbeg != 0 || a.cend != h->base.g.J)
             return fail(BOSSS_ERR_BAD_ARG, "split-precision residuals evaluate whole grids only");
         int rc = tc_volume_launch(h, a.U, a.out, a.alpha, a.beta, s);
         if (rc) return rc;
+        if (once) return faces_once_launch(h, mode, a, s);
         a.faces_only = 1;
         a.beta = 1.0;
+    } else if (once) {
+        EvalArgs v = a;
+        v.volume_only = 1;
+        CUDA_TRY(h->kern[mode].launch(v, s));
+        return faces_once_launch(h, mode, a, s);
     }
     CUDA_TRY(h->kern[mode].launch(a, s));
     return 0;
@@ -458,13 +469,13 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     if (prec != BOSSS_PRECISION_FP64 && prec != BOSSS_PRECISION_SPLIT_FP32)
         return fail(BOSSS_ERR_BAD_ARG, "unknown precision");
     const int want = opt ? opt->kernel : 0;
-    if (want < 0 || want > 2) return fail(BOSSS_ERR_BAD_ARG, "bad kernel selector");
+    if (want < 0 || want > 3) return fail(BOSSS_ERR_BAD_ARG, "bad kernel selector");
     bool have_slab = true, have_generic = true;
     for (int m = 0; m < 3; ++m) {
         have_slab = have_slab && reg.count(KernelKey(phys, D, K, Q, m, VARIANT_SLAB));
         have_generic = have_generic && reg.count(KernelKey(phys, D, K, Q, m, VARIANT_GENERIC));
     }
-    if (want == 2 && !have_slab) return fail(BOSSS_ERR_BAD_ARG, "no slab kernel for this operator");
+    if ((want == 2 || want == 3) && !have_slab) return fail(BOSSS_ERR_BAD_ARG, "no slab kernel for this operator");
     // automatic choice per mode, measured on B200 (16^3-48^3 grids): the slab kernel for 3D
     // systems (Euler, 3-6x); for the scalar family (two threads per node row) the slab residual
     // at every rule (1.1-1.7x faster) and the slab JVP / VJP up to 5 nodes per direction
@@ -472,7 +483,8 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     int mode_variant[3];
     for (int m = 0; m < 3; ++m) {
         const bool slab_pays = phys == PHYS_EULER || m == MODE_RES || Q <= 5;
-        mode_variant[m] = (want == 2 || (want == 0 && have_slab && slab_pays)) ? VARIANT_SLAB : VARIANT_GENERIC;
+        mode_variant[m] = (want == 2 || want == 3 || (want == 0 && have_slab && slab_pays)) ? VARIANT_SLAB
+                                                                                           : VARIANT_GENERIC;
     }
     if (prec == BOSSS_PRECISION_SPLIT_FP32) {
         // the face terms of a split-precision residual come from the slab kernel's faces-only pass
@@ -563,6 +575,12 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
         delete h;
         return fail(BOSSS_ERR_CUDA, std::string("stream creation: ") + cudaGetErrorString(e));
     }
+    // face-once face terms (3D Euler): selected explicitly (kernel 3) or automatically
+    if ((want == 3 || want == 0) && faces_once_supported(h) && h->variant == VARIANT_SLAB) h->faces_once = true;
+    if (want == 3 && !h->faces_once) {
+        bosss_b200_destroy(h);
+        return fail(BOSSS_ERR_BAD_ARG, "the face-once path needs 3D Euler on a whole periodic grid");
+    }
     if (phys == PHYS_CNS) {
         // boundary faces numbered cell by cell, direction, side; Q^(D-1) nodes each
         std::vector<long long> off((size_t)J * 2 * D, -1);
@@ -626,6 +644,7 @@ int bosss_b200_destroy(bosss_handle* h) {
     if (h->stream) cudaStreamDestroy(h->stream);
     cudaFree(h->d_bnd_off);
     cudaFree(h->d_bnd_state);
+    cudaFree(h->dFace);
     tc_volume_destroy(h);
     delete h;
     return BOSSS_OK;

@@ -53,6 +53,9 @@ struct EvalArgs {
     // 1: face terms only (the slab kernel skips its volume pass; the split-precision path
     // evaluates the volume terms on the tensor cores first and the faces add with beta = 1)
     int faces_only;
+    // 1: volume terms only (the slab kernel skips its face passes; the face-once path adds
+    // the face terms from its face buffer afterwards)
+    int volume_only;
     // optional per-cell penalty size factor (1 / cell length scale) of the SIP penalty, in the
     // local cell order; null: the grid's 1 / CellLengthScale. The XDG bulk sets the species'
     // cut-cell length scales here (CoefficientSet.CellLengthScales, XLaplace.cs:104-113).

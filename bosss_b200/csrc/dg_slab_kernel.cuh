@@ -738,9 +738,11 @@ __device__ __forceinline__ void slab_tile(const EvalArgs& args, const Tables1D& 
         }
         __syncthreads();
     };
-    face_pass(std::integral_constant<int, 0>{});
-    face_pass(std::integral_constant<int, 1>{});
-    face_pass(std::integral_constant<int, 2>{});
+    if (!args.volume_only) {   // uniform over the CTA
+        face_pass(std::integral_constant<int, 0>{});
+        face_pass(std::integral_constant<int, 1>{});
+        face_pass(std::integral_constant<int, 2>{});
+    }
 
     // ---------------------------------------------------------- reduce partials and store
     if (active) {

@@ -21,6 +21,9 @@ struct bosss_handle {
     int64_t n_bnd_nodes = 0;
     long long* d_bnd_off = nullptr;
     double* d_bnd_state = nullptr;
+    // face-once path (3D Euler residual and VJP): enabled flag and the face buffer
+    bool faces_once = false;
+    double* dFace = nullptr;
     cudaStream_t stream = nullptr;
     int phys = 0, D = 0, K = 0, Q = 0, variant = 0;
     bosss::EvalArgs base{};

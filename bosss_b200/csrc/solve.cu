@@ -327,7 +327,7 @@ struct KrylovWork {
         if (e == cudaSuccess) e = cudaMalloc(&w, sizeof(T) * n);
         if (e == cudaSuccess) e = cudaMalloc(&z, sizeof(T) * n);
         if (e == cudaSuccess) e = cudaMalloc(&partials, sizeof(double) * RED_BLOCKS * (m + 1));
-        if (e == cudaSuccess) e = cudaMalloc(&hbuf, sizeof(double) * (m + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&hbuf, sizeof(double) * gmres_dev_doubles(m));
         return e;
     }
 };

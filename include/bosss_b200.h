@@ -167,7 +167,9 @@ typedef struct bosss_options {
     int32_t device;        /* CUDA device ordinal */
     int32_t precision;     /* enum bosss_precision */
     int32_t check_nan;     /* 1 = scan outputs for NaN/Inf, fail with BOSSS_ERR_NAN */
-    int32_t kernel;        /* 0 = automatic, 1 = generic fused kernel, 2 = slab kernel (3D systems) */
+    int32_t kernel;        /* 0 = automatic, 1 = generic fused kernel, 2 = slab kernel (3D systems),
+                              3 = slab volume pass + face-once face kernels (3D Euler, whole periodic
+                              grids; residual and VJP, each face's HLLC flux evaluated once) */
     int32_t reserved[8];
 } bosss_options;
 

@@ -72,14 +72,15 @@ def test_vjp_is_transposed_jacobian(name, make):
     assert rel(out, ref) <= TOL, rel(out, ref)
 
 
-EULER_VARIANTS = [(k, kern) for k in (1, 2, 3, 4) for kern in (C.KERNEL_GENERIC, C.KERNEL_SLAB)]
+EULER_VARIANTS = [(k, kern) for k in (1, 2, 3, 4) for kern in (C.KERNEL_GENERIC, C.KERNEL_SLAB, C.KERNEL_FACES)]
+_KNAME = {C.KERNEL_GENERIC: "generic", C.KERNEL_SLAB: "slab", C.KERNEL_FACES: "faces"}
 
 
-@pytest.mark.parametrize("k,kernel", EULER_VARIANTS, ids=["k%d_%s" % (k, "slab" if v == 2 else "generic")
-                                                         for k, v in EULER_VARIANTS])
+@pytest.mark.parametrize("k,kernel", EULER_VARIANTS, ids=["k%d_%s" % (k, _KNAME[v]) for k, v in EULER_VARIANTS])
 def test_euler_kernel_variants(k, kernel):
-    """Both 3D kernels (generic fused and register-blocked slab) against the oracle:
-    residual with alpha/beta, JVP, and VJP vs the transposed Jacobian."""
+    """The 3D kernels (generic fused, register-blocked slab, slab volume + face-once face
+    kernels) against the oracle: residual with alpha/beta, JVP, and VJP vs the transposed
+    Jacobian."""
     pr = P.euler3d(n=3, k=k, seed=50 + k)
     opd, gd = pr.descs()
     r = np.random.default_rng(8)
@@ -104,12 +105,45 @@ def test_euler_kernel_variants(k, kernel):
 def test_euler_full_size_slab_matches_generic():
     pr = P.euler3d(n=32, k=3, seed=2000)
     W = np.random.default_rng(9).uniform(-1, 1, pr.n_dofs)
-    with pr.evaluator(kernel=C.KERNEL_GENERIC) as e1, pr.evaluator(kernel=C.KERNEL_SLAB) as e2:
-        r1, r2 = np.zeros(pr.n_dofs), np.zeros(pr.n_dofs)
+    with pr.evaluator(kernel=C.KERNEL_GENERIC) as e1, pr.evaluator(kernel=C.KERNEL_SLAB) as e2, \
+            pr.evaluator(kernel=C.KERNEL_FACES) as e3:
+        r1, r2, r3 = np.zeros(pr.n_dofs), np.zeros(pr.n_dofs), np.zeros(pr.n_dofs)
         e1.Evaluate(1.0, 0.0, r1, pr.U)
         e2.Evaluate(1.0, 0.0, r2, pr.U)
-        g1, g2 = e1.vjp(pr.U, W), e2.vjp(pr.U, W)
+        e3.Evaluate(1.0, 0.0, r3, pr.U)
+        g1, g2, g3 = e1.vjp(pr.U, W), e2.vjp(pr.U, W), e3.vjp(pr.U, W)
     assert rel(r2, r1) <= TOL and rel(g2, g1) <= TOL
+    assert rel(r3, r1) <= TOL and rel(g3, g1) <= TOL
+
+
+def test_face_once_cell_ranges_match_whole_grid():
+    """Face-once evaluation on cell ranges (each range computes the faces its cells need):
+    three ranges one after the other equal the whole-grid launch, residual and VJP."""
+    import torch
+    pr = P.euler3d(n=6, k=3, seed=2301)
+    W = np.random.default_rng(10).uniform(-1, 1, pr.n_dofs)
+    with pr.evaluator(kernel=C.KERNEL_FACES) as ev:
+        U = torch.from_numpy(pr.U).cuda()
+        Wd = torch.from_numpy(W).cuda()
+        whole_r, whole_g = torch.zeros_like(U), torch.zeros_like(U)
+        part_r, part_g = torch.zeros_like(U), torch.zeros_like(U)
+        L = C.lib()
+        legacy = ctypes.c_void_p(C.CUDA_STREAM_LEGACY)
+        J = pr.grid.NoOfCells
+        C.check(L.bosss_b200_apply_device(ev.handle, C.MODE_RESIDUAL, 1.0, 0.0, C.ptr(U), None, C.ptr(whole_r), 0.0,
+                                          0, J, legacy))
+        C.check(L.bosss_b200_apply_device(ev.handle, C.MODE_VJP, 1.0, 0.0, C.ptr(U), C.ptr(Wd), C.ptr(whole_g), 0.0,
+                                          0, J, legacy))
+        for a, b in ((0, 72), (72, 150), (150, J)):
+            C.check(L.bosss_b200_apply_device(ev.handle, C.MODE_RESIDUAL, 1.0, 0.0, C.ptr(U), None, C.ptr(part_r),
+                                              0.0, a, b, legacy))
+            C.check(L.bosss_b200_apply_device(ev.handle, C.MODE_VJP, 1.0, 0.0, C.ptr(U), C.ptr(Wd), C.ptr(part_g),
+                                              0.0, a, b, legacy))
+        torch.cuda.synchronize()
+    assert torch.equal(whole_r, part_r) and torch.equal(whole_g, part_g)
+    ref = orc.evaluate(*pr.descs(), pr.U)
+    assert rel(whole_r.cpu().numpy(), ref) <= TOL
+    assert rel(whole_g.cpu().numpy(), orc.vjp(*pr.descs(), pr.U, W)) <= TOL
 
 
 def _transport3d(n, k, seed, periodic):
