@@ -34,6 +34,7 @@ ranks.
 ``--impl reference`` times the CPU oracle alone on the host cores (rank 0).
 """
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -62,6 +63,12 @@ def parse():
                          "graph; newton: matrix-free Newton-GMRES on -div((1+u^2) grad u) = 1, 48^3; rk: "
                          "classical RK4 time steps of the Euler workload, one step captured in a CUDA graph")
     ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--precond", default="multigrid", choices=["multigrid", "block-jacobi", "none"],
+                    help="preconditioner of the newton workload")
+    ap.add_argument("--precond-update", type=int, default=1,
+                    help="newton workload: rebuild the preconditioner every this many Newton steps")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "generic", "slab", "faces"],
+                    help="kernel path of the euler3d workload (auto: the library's choice)")
     ap.add_argument("--partitioned", action="store_true",
                     help="euler3d through the partitioned (x-slab, ghost-plane) evaluator even on one GPU; "
                          "always used for --gpus > 1")
@@ -394,7 +401,7 @@ def run_spmv(args):
                    "l2": "flushed between steps (512 MB write outside the timed events)"},
         "rel_err_vs_oracle": err,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None, "kernel": "bsr_spmv_kernel",
+                     "frac": achieved / hbm_peak, "traffic": None, "kernel": "k_ell_spmv (sliced ELL copy of the block-sparse matrix)",
                      "algorithmic_bytes": bytes_},
         "e2e": {"value": rows / e2e_s, "unit": "rows/s", "h2d_bytes_per_step": 8 * rows,
                 "d2h_bytes_per_step": 8 * rows},
@@ -406,20 +413,61 @@ def run_spmv(args):
 
 
 def run_newton(args):
-    """Matrix-free Newton-GMRES (exact JVP, block-Jacobi) on the nonlinear diffusion problem."""
+    """Matrix-free Newton-GMRES (exact JVP; multigrid V-cycle or block-Jacobi preconditioner) on
+    the nonlinear diffusion problem, to a 1e-10 relative residual, confirmed by the oracle.
+    Beside the solve time: the device time of one JVP, one V-cycle and one Jacobian assembly
+    at the solution, the per-iteration budget the solver's iteration rate is compared with."""
+    import torch
+    from bosss_b200 import _capi as C
     from bosss_b200 import problems as P
     from oracle import oracle as orc
     pr = P.nonlinear_diffusion3d(n=args.n, k=args.k, seed=3000, source=1.0)
+    precond = {"multigrid": 2, "block-jacobi": 1, "none": 0}[args.precond]
     with pr.evaluator() as ev:
         t0 = time.perf_counter()
-        U, rep = ev.NewtonSolve(np.zeros(pr.n_dofs), rtol=1e-10, restart=60, max_krylov=3000, inner_rtol=1e-6)
+        U, rep = ev.NewtonSolve(np.zeros(pr.n_dofs), rtol=1e-10, restart=60, max_krylov=3000, inner_rtol=1e-6,
+                                precond=precond, precond_update=args.precond_update)
         dt = time.perf_counter() - t0
+        # component times at the solution (device events, legacy stream)
+        dev = torch.device("cuda", 0)
+        Ud = torch.from_numpy(U).to(dev)
+        V = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, pr.n_dofs)).to(dev)
+        Y = torch.zeros_like(V)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def timed(fn, reps=20):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+
+        legacy = ctypes.c_void_p(C.CUDA_STREAM_LEGACY)
+        ms_jvp = timed(lambda: C.check(C.lib().bosss_b200_jvp_device(ev.handle, C.ptr(Ud), C.ptr(V), C.ptr(Y), 0.0,
+                                                                     legacy)))
+        t0a = time.perf_counter()
+        A = ev.ComputeJacobian(U)
+        s_assembly = time.perf_counter() - t0a
+        ms_vcycle = None
+        if precond == 2:
+            M = ev.Multigrid(A)
+            ms_vcycle = timed(lambda: M.apply_device(V, Y, legacy))
+            M.Dispose()
+        A.Dispose()
     R = orc.evaluate(*pr.descs(), U)
     R0 = orc.evaluate(*pr.descs(), np.zeros(pr.n_dofs))
     line = {"metric": "newton_gmres_solve_time", "value": dt, "unit": "s", "n_gpus": 1, "higher_is_better": False,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": pr.config["workload"] + "_newton_gmres", "dofs": pr.n_dofs},
-            "report": rep, "oracle_relative_residual": float(np.linalg.norm(R) / np.linalg.norm(R0))}
+            "config": {"workload": pr.config["workload"] + "_newton_gmres", "dofs": pr.n_dofs,
+                       "preconditioner": args.precond, "precond_update": args.precond_update, "restart": 60,
+                       "inner_rtol": 1e-6},
+            "report": rep, "oracle_relative_residual": float(np.linalg.norm(R) / np.linalg.norm(R0)),
+            "ms_jvp": ms_jvp, "ms_vcycle": ms_vcycle, "s_jacobian_assembly": s_assembly,
+            "krylov_iters_per_s": rep["krylov_iters"] / dt}
     print(json.dumps(line), flush=True)
 
 
@@ -673,6 +721,13 @@ def run_partitioned(args, rank, world, local):
         dist.destroy_process_group()
 
 
+# kernels of one call per kernel path (bosss_b200_kernel_info)
+PATH_KERNELS = {1: "dg_cell_kernel<PhysEuler<3>,K,Q,%s>",
+                2: "dg_slab_kernel<PhysEuler<3>,K,Q,%s>",
+                3: "dg_slab_kernel<PhysEuler<3>,K,Q,%s> volume pass + k_euler_faces + k_euler_face_project",
+                4: "tc_volume_kernel + %s face terms"}
+
+
 def main():
     args = parse()
     if args.workload == "rk" and args.impl != "reference":
@@ -703,7 +758,11 @@ def main():
     from bosss_b200 import problems as P
 
     pr = P.euler3d(n=args.n, k=args.k, seed=2000 + rank)
-    ev = pr.evaluator(device=local)
+    kern = {"auto": C.KERNEL_AUTO, "generic": C.KERNEL_GENERIC, "slab": C.KERNEL_SLAB,
+            "faces": C.KERNEL_FACES}[args.kernel]
+    ev = pr.evaluator(device=local, kernel=kern)
+    path_res, launch_res = ev.kernel_info(C.MODE_RESIDUAL)
+    path_vjp, launch_vjp = ev.kernel_info(C.MODE_VJP)
     L = C.lib()
     dev = torch.device("cuda", local)
     n = pr.n_dofs
@@ -721,7 +780,7 @@ def main():
         C.check(L.bosss_b200_evaluate_device(h, 1.0, 0.0, C.ptr(U), C.ptr(R), 0.0, sptr))
         C.check(L.bosss_b200_vjp_device(h, C.ptr(U), C.ptr(W), C.ptr(G), 0.0, sptr))
 
-    launches_per_step = 2
+    launches_per_step = launch_res + launch_vjp
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()
@@ -851,13 +910,21 @@ def main():
     t_v = float(np.mean(t_vjp)) * 1e-3
     bytes_res = 8.0 * (n + n)          # U in, R out
     bytes_vjp = 8.0 * (n + n + n)      # U, W in, J^T W out
+    # ncu figures per call (summed over the call's launches) exist for the 32^3 k=3 workload
+    # on the slab path ("euler3d_*") and on the face-once path ("euler3d_faces_*")
+    def _prof(table, path, what):
+        if (args.n, args.k) != (32, 3) or path not in (2, 3):
+            return None
+        return table.get(("euler3d_" if path == 2 else "euler3d_faces_") + what)
     per_kernel = {
         "residual": {"ms": t_r * 1e3, "algorithmic_bytes": bytes_res, "hbm_gbs": bytes_res / t_r / 1e9,
-                     "traffic": prof.get("euler3d_residual_bytes_per_launch"),
-                     "fp64_flops": flops.get("euler3d_residual_fp64_flops_per_launch")},
+                     "launches": launch_res, "kernels": PATH_KERNELS[path_res] % "RESIDUAL",
+                     "traffic": _prof(prof, path_res, "residual_bytes_per_launch"),
+                     "fp64_flops": _prof(flops, path_res, "residual_fp64_flops_per_launch")},
         "vjp": {"ms": t_v * 1e3, "algorithmic_bytes": bytes_vjp, "hbm_gbs": bytes_vjp / t_v / 1e9,
-                "traffic": prof.get("euler3d_vjp_bytes_per_launch"),
-                "fp64_flops": flops.get("euler3d_vjp_fp64_flops_per_launch")},
+                "launches": launch_vjp, "kernels": PATH_KERNELS[path_vjp] % "VJP",
+                "traffic": _prof(prof, path_vjp, "vjp_bytes_per_launch"),
+                "fp64_flops": _prof(flops, path_vjp, "vjp_fp64_flops_per_launch")},
     }
     for kk, t in (("residual", t_r), ("vjp", t_v)):
         f = per_kernel[kk]["fp64_flops"]
@@ -882,7 +949,7 @@ def main():
             "ms_residual": float(np.mean(t_res)), "ms_vjp": float(np.mean(t_vjp)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": traffic,
-                         "kernel": "dg_slab_kernel<PhysEuler<3>,3,4,VJP> (dominant launch)",
+                         "kernel": "VJP call (dominant): " + PATH_KERNELS[path_vjp] % "VJP",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650"},
             "fp64": {"kernel": "VJP", "flops_per_launch": fp64_flops,
                      "achieved_tflops": (fp64_flops / t_r / 1e12) if fp64_flops else None,

@@ -108,7 +108,8 @@ class SolverOpts(ctypes.Structure):
         ("max_krylov", ctypes.c_int32),
         ("precond", ctypes.c_int32),
         ("inner_rtol", ctypes.c_double),
-        ("reserved", ctypes.c_int32 * 8),
+        ("precond_update", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
     ]
 
 
@@ -160,6 +161,11 @@ SIGNATURES = {
                                          ctypes.POINTER(Options), ctypes.POINTER(_P)]),
     "bosss_b200_destroy": (ctypes.c_int, [_P]),
     "bosss_b200_get_sizes": (ctypes.c_int, [_P, _I64, _I64, _I32]),
+    "bosss_b200_kernel_info": (ctypes.c_int, [_P, ctypes.c_int32, _I32, _I32]),
+    "bosss_b200_pmg_create": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_void_p)]),
+    "bosss_b200_pmg_apply_device": (ctypes.c_int, [_P, _P, _P, _P]),
+    "bosss_b200_pmg_info": (ctypes.c_int, [_P, _I32, _I32, _I64, _I32]),
+    "bosss_b200_pmg_destroy": (ctypes.c_int, [_P]),
     "bosss_b200_evaluate": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _P, _P, ctypes.c_double]),
     "bosss_b200_evaluate_device": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _P, _P,
                                                   ctypes.c_double, _P]),

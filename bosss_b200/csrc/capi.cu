@@ -20,6 +20,7 @@
 #include "../../include/bosss_b200.h"
 #include "dg_kernel.cuh"
 #include "dg_registry.h"
+#include "bsr.h"
 #include "handle.h"
 #include "faces_euler.h"
 #include "tc_volume.h"
@@ -369,27 +370,6 @@ static int check_nan(bosss_handle* h, const double* out, int64_t n, cudaStream_t
     return 0;
 }
 
-// ------------------------------------------------------------------ block-sparse SpMV
-// One thread per scalar row; blocks are stored column-major so that the threads of a
-// block row read consecutive addresses for each block column.
-__global__ void bsr_spmv_kernel(long long nbr, int br, int bc, const long long* __restrict__ rowptr,
-                                const int* __restrict__ colidx, const double* __restrict__ vals,
-                                const double* __restrict__ x, double alpha, double beta, double* __restrict__ y) {
-    const long long nrows = nbr * br;
-    for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < nrows;
-         row += (long long)gridDim.x * blockDim.x) {
-        const long long i = row / br;
-        const int r = (int)(row - i * br);
-        double acc = 0.0;
-        for (long long b = rowptr[i]; b < rowptr[i + 1]; ++b) {
-            const double* blk = vals + b * (long long)br * bc;
-            const double* xb = x + (long long)colidx[b] * bc;
-            for (int c = 0; c < bc; ++c) acc += blk[(long long)c * br + r] * __ldg(xb + c);
-        }
-        y[row] = (beta == 0.0) ? alpha * acc : beta * y[row] + alpha * acc;
-    }
-}
-
 }  // namespace bosss
 
 extern "C" {
@@ -567,6 +547,7 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     h->variant = VARIANT_GENERIC;   // generic unless some mode runs on the slab kernel
     for (int m = 0; m < 3; ++m) {
         h->kern[m] = reg[KernelKey(phys, D, K, Q, m, mode_variant[m])];
+        h->kern_variant[m] = mode_variant[m];
         if (mode_variant[m] == VARIANT_SLAB) h->variant = VARIANT_SLAB;
     }
     cudaError_t e = cudaSetDevice(dev);
@@ -704,6 +685,25 @@ int bosss_b200_get_sizes(const bosss_handle* h, int64_t* n_domain_dofs, int64_t*
     if (n_domain_dofs) *n_domain_dofs = h->ndom;
     if (n_codomain_dofs) *n_codomain_dofs = h->ncod;
     if (quad_nodes_1d) *quad_nodes_1d = h->Q;
+    return BOSSS_OK;
+}
+
+int bosss_b200_kernel_info(const bosss_handle* h, int32_t mode, int32_t* kernel, int32_t* launches) {
+    if (!h) return fail(BOSSS_ERR_BAD_ARG, "null handle");
+    if (mode < MODE_RES || mode > MODE_VJP) return fail(BOSSS_ERR_BAD_ARG, "bad mode");
+    const bool split = mode == MODE_RES && h->precision == BOSSS_PRECISION_SPLIT_FP32;
+    const bool once = h->faces_once && (mode == MODE_RES || mode == MODE_VJP);
+    const bool slab = h->kern_variant[mode] == VARIANT_SLAB;
+    int k = slab ? 2 : 1, n = 1;
+    if (split) {
+        k = 4;
+        n = once ? 3 : 2;
+    } else if (once) {
+        k = 3;
+        n = 3;
+    }
+    if (kernel) *kernel = k;
+    if (launches) *launches = n;
     return BOSSS_OK;
 }
 
@@ -965,6 +965,8 @@ int bosss_b200_bsr_destroy(bosss_bsr* A) {
     cudaFree(A->d_colidx);
     cudaFree(A->d_vals);
     cudaFree(A->d_vals32);
+    cudaFree(A->d_ell_col);
+    cudaFree(A->d_ell_vals);
     cudaFree(A->dx);
     cudaFree(A->dy);
     if (A->stream) cudaStreamDestroy(A->stream);
@@ -977,13 +979,7 @@ int bosss_b200_bsr_spmv_device(bosss_bsr* A, double alpha, const double* x_dev, 
     if (!A || !x_dev || !y_dev) return fail(BOSSS_ERR_BAD_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(A->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : A->stream;
-    const long long nrows = A->nbr * A->br;
-    if (nrows == 0) return BOSSS_OK;
-    int grid = (int)std::min<long long>((nrows + 255) / 256, 148LL * 16);
-    bsr_spmv_kernel<<<grid, 256, 0, s>>>(A->nbr, A->br, A->bc, (const long long*)A->d_rowptr, A->d_colidx,
-                                          A->d_vals, x_dev, alpha, beta, y_dev);
-    CUDA_TRY(cudaGetLastError());
-    return BOSSS_OK;
+    return bsr_spmv(A, alpha, x_dev, beta, y_dev, s);
 }
 
 int bosss_b200_bsr_spmv(bosss_bsr* A, double alpha, const double* x, double beta, double* y) {

@@ -29,6 +29,7 @@ struct bosss_handle {
     bosss::EvalArgs base{};
     int64_t ndom = 0, ncod = 0;
     bosss::KernelEntry kern[3]{};
+    int kern_variant[3]{};   // VARIANT_GENERIC / VARIANT_SLAB per mode
     bool check_nan = false;
     // device staging for the host-buffer entry points
     double* dU = nullptr;
@@ -41,20 +42,6 @@ struct bosss_handle {
     static constexpr int MAX_CHUNKS = 16;
     cudaEvent_t ev_in[MAX_CHUNKS]{}, ev_done[MAX_CHUNKS]{};
 };
-
-struct bosss_bsr {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int64_t nbr = 0, nbc = 0, nnzb = 0;
-    int br = 0, bc = 0;
-    int64_t* d_rowptr = nullptr;
-    int32_t* d_colidx = nullptr;
-    double* d_vals = nullptr;   // blocks stored column-major (coalesced row-lane loads)
-    float* d_vals32 = nullptr;  // FP32 copy for the inner solves of the mixed-precision refinement
-    double* dx = nullptr;
-    double* dy = nullptr;
-};
-
 
 namespace bosss {
 int fail(int code, const std::string& msg);

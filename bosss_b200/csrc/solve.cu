@@ -19,7 +19,9 @@
 #include <cstring>
 #include <vector>
 
+#include "bsr.h"
 #include "handle.h"
+#include "pmg.h"
 #include "solver.cuh"
 
 namespace bosss {
@@ -166,74 +168,6 @@ static int assemble(bosss_handle* h, const double* U_dev, double time, bosss_bsr
 }
 
 // ------------------------------------------------------------------ block-Jacobi
-// Gauss-Jordan with partial pivoting of the diagonal block of every block row; one CTA
-// per block, the augmented matrix [A | I] in shared memory. Output column-major.
-template <class T>
-__global__ void k_invert_diag(int nb, const long long* __restrict__ rowptr, const double* __restrict__ vals, T* __restrict__ inv,
-                              int* __restrict__ singular) {
-    extern __shared__ double sm[];
-    const int j = blockIdx.x;
-    double* Am = sm;              // nb x nb, row-major
-    double* Im = sm + nb * nb;    // nb x nb, row-major
-    __shared__ int piv;
-    const double* blk = vals + rowptr[j] * (long long)nb * nb;   // diagonal block is the first of the row
-    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-        const int r = t / nb, c = t % nb;
-        Am[t] = blk[(long long)c * nb + r];
-        Im[t] = (r == c) ? 1.0 : 0.0;
-    }
-    __syncthreads();
-    for (int k = 0; k < nb; ++k) {
-        if (threadIdx.x == 0) {
-            int p = k;
-            double best = fabs(Am[k * nb + k]);
-            for (int r = k + 1; r < nb; ++r)
-                if (fabs(Am[r * nb + k]) > best) {
-                    best = fabs(Am[r * nb + k]);
-                    p = r;
-                }
-            piv = p;
-            if (best == 0.0) atomicExch(singular, 1);
-        }
-        __syncthreads();
-        const int p = piv;
-        if (p != k)
-            for (int c = threadIdx.x; c < nb; c += blockDim.x) {
-                double t0 = Am[k * nb + c];
-                Am[k * nb + c] = Am[p * nb + c];
-                Am[p * nb + c] = t0;
-                t0 = Im[k * nb + c];
-                Im[k * nb + c] = Im[p * nb + c];
-                Im[p * nb + c] = t0;
-            }
-        __syncthreads();
-        const double d = Am[k * nb + k];
-        const double inv_d = (d != 0.0) ? 1.0 / d : 0.0;
-        __syncthreads();
-        for (int c = threadIdx.x; c < nb; c += blockDim.x) {
-            Am[k * nb + c] *= inv_d;
-            Im[k * nb + c] *= inv_d;
-        }
-        __syncthreads();
-        for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-            const int r = t / nb, c = t % nb;
-            if (r == k) continue;
-            const double f = Am[r * nb + k];
-            if (c != k) Am[t] -= f * Am[k * nb + c];
-            Im[t] -= f * Im[k * nb + c];
-        }
-        __syncthreads();
-        for (int r = threadIdx.x; r < nb; r += blockDim.x)
-            if (r != k) Am[r * nb + k] = 0.0;
-        __syncthreads();
-    }
-    T* out = inv + (long long)j * nb * nb;
-    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-        const int r = t / nb, c = t % nb;
-        out[(long long)c * nb + r] = (T)Im[t];
-    }
-}
-
 // y_j = Dinv_j x_j (blocks column-major), one thread per scalar row
 template <class T>
 __global__ void k_apply_blockdiag(long long ncell, int nb, const T* __restrict__ inv, const T* __restrict__ x,
@@ -305,6 +239,7 @@ static void fill_defaults(const bosss_solver_opts* o, bosss_solver_opts& r, doub
         if (o->max_krylov > 0) r.max_krylov = o->max_krylov;
         r.precond = o->precond;
         if (o->inner_rtol > 0) r.inner_rtol = o->inner_rtol;
+        r.precond_update = o->precond_update;
     }
 }
 
@@ -367,9 +302,12 @@ int bosss_b200_newton_solve(bosss_handle* h, double* U, double time, const bosss
     CUDA_TRY(cudaSetDevice(h->device));
     cudaStream_t s = h->stream;
     const long long n = h->ndom;
+    if (o.precond < 0 || o.precond > 2) return fail(BOSSS_ERR_BAD_ARG, "unknown preconditioner");
     double *dU = nullptr, *dR = nullptr, *dX = nullptr, *dT = nullptr, *dW = nullptr, *dinv = nullptr;
+    bosss_pmg* mg = nullptr;
     KrylovWork<double> kw;
     auto cleanup = [&]() {
+        pmg_destroy(mg);
         cudaFree(dU);
         cudaFree(dR);
         cudaFree(dX);
@@ -409,13 +347,16 @@ int bosss_b200_newton_solve(bosss_handle* h, double* U, double time, const bosss
         if (it == o.max_outer) break;
         r.outer_iters = it + 1;
         // right-preconditioned J M^-1 z = -R, dU_step = M^-1 z
-        if (o.precond == 1) {
+        const int upd = std::max(o.precond_update, 1);
+        if ((o.precond == 1 || o.precond == 2) && it % upd == 0) {
             cudaFree(dinv);
             dinv = nullptr;
+            pmg_destroy(mg);
+            mg = nullptr;
             bosss_bsr* A = nullptr;
             rc = assemble(h, dU, time, &A);
             if (rc) break;
-            rc = block_jacobi<double>(A, &dinv, s);
+            rc = (o.precond == 1) ? block_jacobi<double>(A, &dinv, s) : pmg_create(h, A, &mg);
             bosss_b200_bsr_destroy(A);
             if (rc) break;
         }
@@ -426,6 +367,13 @@ int bosss_b200_newton_solve(bosss_handle* h, double* U, double time, const bosss
             const double* xin = x;
             if (dinv) {
                 k_apply_blockdiag<double><<<grid_of(n), 256, 0, s>>>(h->base.g.J, nb, dinv, x, dT);
+                xin = dT;
+            } else if (mg) {
+                int rr = pmg_apply(mg, x, dT, s);
+                if (rr) {
+                    inner_rc = rr;
+                    return cudaErrorUnknown;
+                }
                 xin = dT;
             }
             int rr = run_mode(h, MODE_JVP, 1.0, 0.0, dU, xin, y, time, s);
@@ -446,6 +394,10 @@ int bosss_b200_newton_solve(bosss_handle* h, double* U, double time, const bosss
         const double* step = dX;
         if (dinv) {
             k_apply_blockdiag<double><<<grid_of(n), 256, 0, s>>>(h->base.g.J, nb, dinv, dX, dT);
+            step = dT;
+        } else if (mg) {
+            rc = pmg_apply(mg, dX, dT, s);
+            if (rc) break;
             step = dT;
         }
         // backtracking on the residual norm
@@ -514,6 +466,10 @@ int bosss_b200_bsr_solve(bosss_bsr* A, const double* b, double* x, const bosss_s
         return fail(BOSSS_ERR_CUDA, std::string("solver work arrays: ") + cudaGetErrorString(e));
     }
     int rc = 0;
+    if (o.precond == 2) {
+        cleanup();
+        return fail(BOSSS_ERR_BAD_ARG, "bsr_solve: preconditioner 0 (none) or 1 (block-Jacobi)");
+    }
     if (o.precond == 1) {
         rc = block_jacobi<float>(A, &inv, s);
         if (rc) {

@@ -73,6 +73,74 @@ __global__ void k_multiaxpy_add(long long n, int m, const T* __restrict__ Z, lon
     }
 }
 
+// Gauss-Jordan with partial pivoting of the diagonal block of every block row; one CTA
+// per block, the augmented matrix [A | I] in shared memory. Output column-major.
+template <class T>
+__global__ void k_invert_diag(int nb, const long long* __restrict__ rowptr, const double* __restrict__ vals, T* __restrict__ inv,
+                              int* __restrict__ singular) {
+    extern __shared__ double sm[];
+    const int j = blockIdx.x;
+    double* Am = sm;              // nb x nb, row-major
+    double* Im = sm + nb * nb;    // nb x nb, row-major
+    __shared__ int piv;
+    const double* blk = vals + rowptr[j] * (long long)nb * nb;   // diagonal block is the first of the row
+    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+        const int r = t / nb, c = t % nb;
+        Am[t] = blk[(long long)c * nb + r];
+        Im[t] = (r == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < nb; ++k) {
+        if (threadIdx.x == 0) {
+            int p = k;
+            double best = fabs(Am[k * nb + k]);
+            for (int r = k + 1; r < nb; ++r)
+                if (fabs(Am[r * nb + k]) > best) {
+                    best = fabs(Am[r * nb + k]);
+                    p = r;
+                }
+            piv = p;
+            if (best == 0.0) atomicExch(singular, 1);
+        }
+        __syncthreads();
+        const int p = piv;
+        if (p != k)
+            for (int c = threadIdx.x; c < nb; c += blockDim.x) {
+                double t0 = Am[k * nb + c];
+                Am[k * nb + c] = Am[p * nb + c];
+                Am[p * nb + c] = t0;
+                t0 = Im[k * nb + c];
+                Im[k * nb + c] = Im[p * nb + c];
+                Im[p * nb + c] = t0;
+            }
+        __syncthreads();
+        const double d = Am[k * nb + k];
+        const double inv_d = (d != 0.0) ? 1.0 / d : 0.0;
+        __syncthreads();
+        for (int c = threadIdx.x; c < nb; c += blockDim.x) {
+            Am[k * nb + c] *= inv_d;
+            Im[k * nb + c] *= inv_d;
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+            const int r = t / nb, c = t % nb;
+            if (r == k) continue;
+            const double f = Am[r * nb + k];
+            if (c != k) Am[t] -= f * Am[k * nb + c];
+            Im[t] -= f * Im[k * nb + c];
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < nb; r += blockDim.x)
+            if (r != k) Am[r * nb + k] = 0.0;
+        __syncthreads();
+    }
+    T* out = inv + (long long)j * nb * nb;
+    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+        const int r = t / nb, c = t % nb;
+        out[(long long)c * nb + r] = (T)Im[t];
+    }
+}
+
 constexpr int RED_BLOCKS = 296;   // 2 x 148 SMs
 constexpr int RED_THREADS = 512;
 constexpr int MDOT_CH = 8;        // vectors per pass of the multi-dot
@@ -110,7 +178,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_mdot(long long n, int k0, int m
 }
 
 // out[k] = sum_b partials[k * RED_BLOCKS + b] for k < m (one block per k, fixed order)
-__global__ void k_finish_partials(const double* __restrict__ partials, double* __restrict__ out) {
+static __global__ void k_finish_partials(const double* __restrict__ partials, double* __restrict__ out) {
     const int k = blockIdx.x;
     double a = 0.0;
     for (int i = threadIdx.x; i < RED_BLOCKS; i += blockDim.x) a += partials[(long long)k * RED_BLOCKS + i];
@@ -152,7 +220,7 @@ struct GmresDev {
 __host__ __device__ constexpr long long gmres_dev_doubles(int m) { return (long long)(m + 1) * (m + 8); }
 
 // start of a cycle: beta = ||r|| from sc[0]; g = beta e_1; scale 1/beta for V_0
-__global__ void k_gmres_start(double* base, int m) {
+static __global__ void k_gmres_start(double* base, int m) {
     GmresDev d(base, m);
     const double beta = sqrt(fmax(d.sc[0], 0.0));
     for (int i = 0; i <= m; ++i) d.g[i] = 0.0;
@@ -164,7 +232,7 @@ __global__ void k_gmres_start(double* base, int m) {
 
 // Arnoldi step k: h += h2 (second Gram-Schmidt pass), h[k+1] = ||w||, Givens rotations,
 // column k of H, g, residual estimate |g[k+1]|, scale 1/h[k+1] of the new basis vector
-__global__ void k_gmres_step(double* base, int m, int k) {
+static __global__ void k_gmres_step(double* base, int m, int k) {
     GmresDev d(base, m);
     double h[256];
     for (int j = 0; j <= k; ++j) h[j] = d.h[j] + d.h2[j];

@@ -361,8 +361,10 @@ class DifferentialOperator:
                          device, precision, check_nan, kernel)
 
 
-def _solver_opts(rtol=None, atol=None, max_outer=None, restart=None, max_krylov=None, precond=1, inner_rtol=None):
+def _solver_opts(rtol=None, atol=None, max_outer=None, restart=None, max_krylov=None, precond=1, inner_rtol=None,
+                 precond_update=None):
     o = C.SolverOpts()
+    o.precond_update = precond_update or 0
     o.rtol = rtol or 0.0
     o.atol = atol or 0.0
     o.max_outer = max_outer or 0
@@ -376,6 +378,30 @@ def _solver_opts(rtol=None, atol=None, max_outer=None, restart=None, max_krylov=
 def _report(r):
     return {"outer_iters": r.outer_iters, "krylov_iters": r.krylov_iters, "converged": bool(r.converged),
             "residual0": r.residual0, "residual": r.residual}
+
+
+class MultigridPreconditioner:
+    """One V-cycle of ClassicMultigrid over the p-levels (LevelPmg) and aggregation levels of a
+    scalar Jacobian (bosss_b200_pmg_*); ``apply_device`` takes device pointers."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def info(self):
+        npl, nhl, nc, direct = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int32()
+        C.check(C.lib().bosss_b200_pmg_info(self.handle, ctypes.byref(npl), ctypes.byref(nhl), ctypes.byref(nc),
+                                            ctypes.byref(direct)))
+        return {"p_levels": npl.value, "h_levels": nhl.value, "coarsest": nc.value, "direct": bool(direct.value)}
+
+    def apply_device(self, b, x, stream=None):
+        C.check(C.lib().bosss_b200_pmg_apply_device(self.handle, C.ptr(b), C.ptr(x), stream))
+
+    def Dispose(self):
+        if self.handle:
+            C.lib().bosss_b200_pmg_destroy(self.handle)
+            self.handle = None
+
+    __del__ = Dispose
 
 
 class BlockMsrMatrix:
@@ -395,15 +421,11 @@ class BlockMsrMatrix:
         rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
         ci = np.ascontiguousarray(col_idx, dtype=np.int32)
         v = np.ascontiguousarray(values, dtype=np.float64)
-        nnzb = len(ci)
-        bs = v.size // max(nnzb, 1)
-        br = v.shape[1] if v.ndim == 3 else None
-        if br is None:
+        if v.ndim != 3 or v.shape[0] != len(ci):
             raise ValueError("values must have shape (nnz_blocks, row_block, col_block)")
         h = ctypes.c_void_p()
         C.check(C.lib().bosss_b200_bsr_create(n_block_rows, n_block_cols, v.shape[1], v.shape[2], C.ptr(rp),
                                               C.ptr(ci), C.ptr(v), int(device), ctypes.byref(h)))
-        del bs
         return cls(h)
 
     def Dispose(self):
@@ -471,6 +493,13 @@ class Evaluator:
     def __exit__(self, *a):
         self.Dispose()
 
+    def kernel_info(self, mode=C.MODE_RESIDUAL):
+        """(kernel path, launches per whole-grid call) of `mode`: 1 generic, 2 slab, 3 slab
+        volume pass + face-once face kernels, 4 tensor-core volume + face terms."""
+        k, n = ctypes.c_int32(), ctypes.c_int32()
+        C.check(C.lib().bosss_b200_kernel_info(self.handle, int(mode), ctypes.byref(k), ctypes.byref(n)))
+        return k.value, n.value
+
     # -- evaluation
     @staticmethod
     def _is_cuda(a):
@@ -522,6 +551,12 @@ class Evaluator:
         h = ctypes.c_void_p()
         C.check(C.lib().bosss_b200_compute_jacobian(self.handle, C.ptr(U), self.time, ctypes.byref(h)))
         return BlockMsrMatrix(h)
+
+    def Multigrid(self, A):
+        """Multigrid V-cycle preconditioner of the Jacobian A (from ComputeJacobian)."""
+        h = ctypes.c_void_p()
+        C.check(C.lib().bosss_b200_pmg_create(self.handle, A.handle, ctypes.byref(h)))
+        return MultigridPreconditioner(h)
 
     def NewtonSolve(self, U0, **kw):
         """Matrix-free Newton-GMRES for Op(U) = 0; returns (U, report)."""

@@ -192,6 +192,10 @@ int bosss_b200_destroy(bosss_handle* h);
 /* DOF counts of the domain and codomain mappings, and the quadrature nodes per direction. */
 int bosss_b200_get_sizes(const bosss_handle* h, int64_t* n_domain_dofs, int64_t* n_codomain_dofs,
                          int32_t* quad_nodes_1d);
+/* The kernel path in effect for `mode` (0 residual, 1 JVP, 2 VJP): 1 generic fused kernel,
+ * 2 slab kernel, 3 slab volume pass + face-once face kernels, 4 tensor-core volume kernel +
+ * face terms (split-precision residual); and the kernel launches of one whole-grid call. */
+int bosss_b200_kernel_info(const bosss_handle* h, int32_t mode, int32_t* kernel, int32_t* launches);
 
 /* EvaluatorNonLin.Evaluate (DifferentialOperator.cs:1584-1661):
  *   out = beta*out + alpha*Op(U),  host buffers (copies in and out inside the call; above
@@ -268,9 +272,14 @@ typedef struct bosss_solver_opts {
     int32_t max_outer;      /* Newton steps (newton_solve) / refinement steps (bsr_solve) */
     int32_t restart;        /* GMRES restart length m (<= 200) */
     int32_t max_krylov;     /* GMRES iterations per outer step */
-    int32_t precond;        /* 0 = none, 1 = block-Jacobi on the cell blocks of the Jacobian */
+    int32_t precond;        /* 0 = none, 1 = block-Jacobi on the cell blocks of the Jacobian,
+                               2 = multigrid V-cycle (bosss_b200_pmg_create; newton_solve with
+                               scalar operators only) */
     double inner_rtol;      /* relative tolerance of each inner (Krylov) solve */
-    int32_t reserved[8];
+    int32_t precond_update; /* newton_solve: rebuild the preconditioner (Jacobian assembly +
+                               setup) every this many Newton steps, the reference's
+                               constant_newton_it (Newton.cs:70, 762); 0 or 1: every step */
+    int32_t reserved[7];
 } bosss_solver_opts;
 
 typedef struct bosss_solver_report {
@@ -291,6 +300,24 @@ int bosss_b200_newton_solve(bosss_handle* h, double* U, double time, const bosss
  * x: host buffer, initial guess in, solution out. */
 int bosss_b200_bsr_solve(bosss_bsr* A, const double* b, double* x, const bosss_solver_opts* opt,
                          bosss_solver_report* rep);
+
+/* Multigrid preconditioner of a scalar operator's cell-block Jacobian A (from
+ * bosss_b200_compute_jacobian) on the handle's whole Cartesian grid (ClassicMultigrid.Solve,
+ * ClassicMultigrid.cs:335-420, over the p-levels of LevelPmg and the aggregation grids of
+ * CoarseningAlgorithms.CreateSequence): p-levels of degree K, K-1, ..., 1 (leading sub-blocks of
+ * the hierarchical basis, one block-Jacobi sweep before and after the coarse correction), the
+ * piecewise-constant level and its 2x2x2 aggregates (two damped Jacobi sweeps each side), a
+ * dense coarsest solve. One V-cycle per apply, a fixed linear operator (suitable as a right
+ * preconditioner of GMRES). A is copied; it may be destroyed after create. */
+typedef struct bosss_pmg bosss_pmg;
+int bosss_b200_pmg_create(const bosss_handle* h, const bosss_bsr* A, bosss_pmg** out);
+/* x = M^-1 b, device vectors, enqueued on `stream` (NULL: the preconditioner's stream). */
+int bosss_b200_pmg_apply_device(bosss_pmg* M, const double* b_dev, double* x_dev, void* stream);
+/* Number of p-levels and structured levels, unknowns of the coarsest level, and whether the
+ * coarsest level is solved directly (1) or by Jacobi sweeps (0, singular coarsest matrix). */
+int bosss_b200_pmg_info(const bosss_pmg* M, int32_t* n_p_levels, int32_t* n_h_levels, int64_t* coarsest,
+                        int32_t* coarsest_direct);
+int bosss_b200_pmg_destroy(bosss_pmg* M);
 
 /* Jacobian assembly of the operator at state U into a new block-sparse matrix
  * (EvaluatorLinear.ComputeMatrix, LECVolumeQuadrature2.cs:132 / LECEdgeQuadrature2.cs:127 ->

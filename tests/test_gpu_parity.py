@@ -432,3 +432,32 @@ def test_block_sparse_spmv_full_c3_pattern():
         assert rel(y, orc.bsr_spmv(rp, ci, vals, 1.0, x, 0.0, y0)) <= 1e-14
     finally:
         A.Dispose()
+
+
+@pytest.mark.parametrize("shape", ["ragged_rectangular", "one_wide_row"])
+def test_block_sparse_spmv_irregular_patterns(shape):
+    """SpMV on patterns away from the Cartesian one: ragged rows, rectangular blocks, more
+    block columns than rows and empty rows (sliced-ELL copy with zero padding), and a pattern
+    with one very wide row (the ELL padding would not pay: the block-row kernel)."""
+    r = np.random.default_rng(13)
+    nbr, nbc, br, bc = (300, 410, 3, 5) if shape == "ragged_rectangular" else (200, 200, 4, 4)
+    rows = []
+    for i in range(nbr):
+        if shape == "ragged_rectangular":
+            k = 4 if r.random() < 0.9 else int(r.integers(0, 4))   # some short and empty rows
+        else:
+            k = 150 if i == 7 else 2
+        rows.append(np.sort(r.choice(nbc, size=k, replace=False)))
+    rp = np.zeros(nbr + 1, dtype=np.int64)
+    rp[1:] = np.cumsum([len(c) for c in rows])
+    ci = np.concatenate(rows).astype(np.int32)
+    vals = r.uniform(-1, 1, (len(ci), br, bc))
+    x = r.uniform(-1, 1, nbc * bc)
+    y0 = r.uniform(-1, 1, nbr * br)
+    ref = orc.bsr_spmv(rp, ci, vals, 0.5, x, -2.0, y0)
+    A = O.BlockMsrMatrix.from_blocks(nbr, nbc, rp, ci, vals)
+    try:
+        y = A.SpMV(0.5, x, -2.0, y0.copy())
+        assert rel(y, ref) <= 1e-14
+    finally:
+        A.Dispose()
