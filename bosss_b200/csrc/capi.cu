@@ -334,7 +334,8 @@ static int launch_eval(bosss_handle* h, int mode, EvalArgs a, cudaStream_t s) {
     } else if (once) {
         EvalArgs v = a;
         v.volume_only = 1;
-        CUDA_TRY(h->kern[mode].launch(v, s));
+        if (h->kern_vol[mode].launch) CUDA_TRY(h->kern_vol[mode].launch(v, s));
+        else CUDA_TRY(h->kern[mode].launch(v, s));
         return faces_once_launch(h, mode, a, s);
     }
     CUDA_TRY(h->kern[mode].launch(a, s));
@@ -351,8 +352,8 @@ int run_mode(bosss_handle* h, int mode, double alpha, double beta, const double*
     a.beta = beta;
     a.time = time;
     CUDA_TRY(cudaSetDevice(h->device));
-    if ((a.vol_flag || a.face_flag) && h->variant != VARIANT_GENERIC)
-        return fail(BOSSS_ERR_BAD_ARG, "species masks need the generic kernel");
+    if ((a.vol_flag || a.face_flag) && (h->faces_once || h->precision != BOSSS_PRECISION_FP64))
+        return fail(BOSSS_ERR_BAD_ARG, "species masks: plain FP64 generic or slab kernels only");
     if (h->base.g.J > 0) return launch_eval(h, mode, a, s);
     return 0;
 }
@@ -434,10 +435,11 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
                 return fail(BOSSS_ERR_BAD_ARG, "a part is periodic only in directions it spans completely");
         }
     }
+    // HLLC on a grid with boundary faces: the outer states come from the boundary-state table
+    // (OptimizedHLLCFlux.BorderEdgeFlux); the generic kernel reads it
+    bool euler_bounded = false;
     if (phys == PHYS_EULER)
-        for (int d = 0; d < D; ++d)
-            if (!gper[d])
-                return fail(BOSSS_ERR_BAD_ARG, "HLLC fluxes need a boundary-condition map: only periodic grids");
+        for (int d = 0; d < D; ++d) euler_bounded = euler_bounded || !gper[d];
     if (phys == PHYS_SIP && ph.has_sip && K < 1)
         return fail(BOSSS_ERR_BAD_ARG, "SIP needs DG degree >= 1 (IsValidDomainDegreeCombination)");
     const int order = quad_order(*op);
@@ -452,7 +454,7 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     if (want < 0 || want > 3) return fail(BOSSS_ERR_BAD_ARG, "bad kernel selector");
     bool have_slab = true, have_generic = true;
     for (int m = 0; m < 3; ++m) {
-        have_slab = have_slab && reg.count(KernelKey(phys, D, K, Q, m, VARIANT_SLAB));
+        have_slab = have_slab && !euler_bounded && reg.count(KernelKey(phys, D, K, Q, m, VARIANT_SLAB));
         have_generic = have_generic && reg.count(KernelKey(phys, D, K, Q, m, VARIANT_GENERIC));
     }
     if ((want == 2 || want == 3) && !have_slab) return fail(BOSSS_ERR_BAD_ARG, "no slab kernel for this operator");
@@ -558,11 +560,16 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     }
     // face-once face terms (3D Euler): selected explicitly (kernel 3) or automatically
     if ((want == 3 || want == 0) && faces_once_supported(h) && h->variant == VARIANT_SLAB) h->faces_once = true;
+    if (h->faces_once)
+        for (int m : {MODE_RES, MODE_VJP}) {
+            auto it = reg.find(KernelKey(phys, D, K, Q, m, VARIANT_SLAB_VOL));
+            if (it != reg.end()) h->kern_vol[m] = it->second;
+        }
     if (want == 3 && !h->faces_once) {
         bosss_b200_destroy(h);
         return fail(BOSSS_ERR_BAD_ARG, "the face-once path needs 3D Euler on a whole periodic grid");
     }
-    if (phys == PHYS_CNS) {
+    if (phys == PHYS_CNS || euler_bounded) {
         // boundary faces numbered cell by cell, direction, side; Q^(D-1) nodes each
         std::vector<long long> off((size_t)J * 2 * D, -1);
         long long nb = 0;

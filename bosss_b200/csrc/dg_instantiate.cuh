@@ -38,24 +38,24 @@ void reg_one(int phys) {
     }
 }
 
-template <class Phys, int K, int Q, int MODE>
+template <class Phys, int K, int Q, int MODE, int PASS = 0>
 cudaError_t launch_slab_kernel(const EvalArgs& a, cudaStream_t s) {
-    using C = SlabCfg<Phys, K, Q, MODE>;
+    using C = SlabCfg<Phys, K, Q, MODE, PASS>;
     int dev = 0;
     cudaGetDevice(&dev);
     static unsigned long long attr_done = 0ull;
     if (!(attr_done & (1ull << (dev & 63)))) {
-        cudaError_t e = cudaFuncSetAttribute(dg_slab_kernel<Phys, K, Q, MODE>,
+        cudaError_t e = cudaFuncSetAttribute(dg_slab_kernel<Phys, K, Q, MODE, PASS>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM_BYTES);
         if (e != cudaSuccess) return e;
         // the tiles are sized for two resident CTAs: ask for the largest shared-memory carveout
-        e = cudaFuncSetAttribute(dg_slab_kernel<Phys, K, Q, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        e = cudaFuncSetAttribute(dg_slab_kernel<Phys, K, Q, MODE, PASS>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         attr_done |= (1ull << (dev & 63));
     }
     const long long blocks = (a.cend - a.cbeg + C::CPB - 1) / C::CPB;
     if (blocks <= 0) return cudaSuccess;
-    dg_slab_kernel<Phys, K, Q, MODE><<<(unsigned)blocks, C::NT, C::SMEM_BYTES, s>>>(a);
+    dg_slab_kernel<Phys, K, Q, MODE, PASS><<<(unsigned)blocks, C::NT, C::SMEM_BYTES, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -66,6 +66,19 @@ void reg_slab_one(int phys) {
         kernel_registry()[KernelKey(phys, 3, K, Q, MODE, VARIANT_SLAB)] =
             KernelEntry{&launch_slab_kernel<Phys, K, Q, MODE>, C::CPB, C::SMEM_BYTES};
     }
+}
+
+// volume-only slab instances (residual and VJP) for the face-once path
+template <class Phys, int K, int Q>
+void reg_slab_volume(int phys) {
+    using R = SlabCfg<Phys, K, Q, MODE_RES, 1>;
+    using V = SlabCfg<Phys, K, Q, MODE_VJP, 1>;
+    if constexpr (R::SMEM_BYTES <= 227 * 1024 && R::NT <= 512)
+        kernel_registry()[KernelKey(phys, 3, K, Q, MODE_RES, VARIANT_SLAB_VOL)] =
+            KernelEntry{&launch_slab_kernel<Phys, K, Q, MODE_RES, 1>, R::CPB, R::SMEM_BYTES};
+    if constexpr (V::SMEM_BYTES <= 227 * 1024 && V::NT <= 512)
+        kernel_registry()[KernelKey(phys, 3, K, Q, MODE_VJP, VARIANT_SLAB_VOL)] =
+            KernelEntry{&launch_slab_kernel<Phys, K, Q, MODE_VJP, 1>, V::CPB, V::SMEM_BYTES};
 }
 
 template <class Phys, int K, int Q>

@@ -423,8 +423,21 @@ struct PhysEuler {
     __host__ __device__ static void boundary(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
                                              const double* n, const double* x, const double* ub, T* gA,
                                              T (*GAv)[D]) {
-        // no boundary-condition map on the device: create() rejects non-periodic Euler grids
-        (void)p; (void)pnlty; (void)UA; (void)GA; (void)n; (void)x; (void)ub; (void)gA; (void)GAv;
+        // OptimizedHLLCFlux.BorderEdgeFlux (OptimizedHLLCFlux.cs:61-131): the outer state of the
+        // boundary condition (here the boundary-state table's value at this node, a constant of
+        // the linearisation), then the inner-edge HLLC flux with the outward normal
+        (void)GA;
+        if (!ub) return;   // create() requires the boundary-state table on non-periodic grids
+        T Uo[NV], GB[NV][D], gB[NC], GBv[NC][D];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            Uo[i] = T(ub[i]);
+#pragma unroll
+            for (int d = 0; d < D; ++d) GB[i][d] = T(0.0);
+        }
+#pragma unroll
+        for (int e = 0; e < NC; ++e) gB[e] = T(0.0);
+        inner<T>(p, pnlty, UA, GA, Uo, GB, n, x, gA, GAv, gB, GBv);
     }
 
     // ---- reverse-mode adjoints (VJP): one primal sweep plus one reverse sweep per node in

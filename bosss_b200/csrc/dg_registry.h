@@ -16,7 +16,7 @@ struct KernelEntry {
     size_t smem_bytes;
 };
 
-enum KernelVariant { VARIANT_GENERIC = 0, VARIANT_SLAB = 1 };
+enum KernelVariant { VARIANT_GENERIC = 0, VARIANT_SLAB = 1, VARIANT_SLAB_VOL = 2 };   // 2: volume terms only
 using KernelKey = std::tuple<int, int, int, int, int, int>;   // phys, D, K, Q, mode, variant
 std::map<KernelKey, KernelEntry>& kernel_registry();
 

@@ -21,7 +21,9 @@
 
 namespace bosss {
 
-template <class Phys, int K, int Q, int MODE>
+// PASS: 0 = volume and face terms (runtime flags may skip either), 1 = volume terms only
+// (compiled without the face passes: the volume pass of the face-once path)
+template <class Phys, int K, int Q, int MODE, int PASS = 0>
 struct SlabCfg {
     using B = Cfg<Phys, K, Q, MODE>;
     static constexpr int D = 3;
@@ -66,7 +68,7 @@ struct SlabCfg {
     static constexpr int TRB = (NV * NCI0 + NF1 * NCI1F) * FF;      // one (face, side) trace block
     static constexpr int S_FACE = 2 * 2 * TRB + 2 * NO * NCOF * FF;
     static constexpr int S_RED = NO * SPLIT * Q * NP;
-    static constexpr int S_W0 = S_VOL > S_FACE ? S_VOL : S_FACE;
+    static constexpr int S_W0 = (PASS == 1 || S_VOL > S_FACE) ? S_VOL : S_FACE;
     static constexpr int S_WORK = S_W0 > S_RED ? S_W0 : S_RED;
     static constexpr int S_CELL = S_CIN + S_WORK;
     static constexpr int BUDGET = 110 * 1024 / 8;
@@ -589,9 +591,9 @@ __device__ __forceinline__ void slab_face_traces(const EvalArgs& args, const Tab
 // of the CTA do the work, any further threads only take part in the barriers (the batched
 // persistent kernel runs tiles of several degrees in CTAs of one size). T: the 1D tables,
 // passed apart from args so that a caller can keep them in the kernel-parameter bank.
-template <class Phys, int K, int Q, int MODE>
+template <class Phys, int K, int Q, int MODE, int PASS = 0>
 __device__ __forceinline__ void slab_tile(const EvalArgs& args, const Tables1D& T, long long c0, double* smem) {
-    using C = SlabCfg<Phys, K, Q, MODE>;
+    using C = SlabCfg<Phys, K, Q, MODE, PASS>;
     constexpr int NP = C::NP, NV = C::NV, NO = C::NO, CPB = C::CPB, NT = C::NT, SPLIT = C::SPLIT;
     constexpr int SLV = C::SLV, FV = C::FV, SLF = C::SLF, FF = C::FF, QF = Q * Q;
     const GridConst& g = args.g;
@@ -648,6 +650,10 @@ __device__ __forceinline__ void slab_tile(const EvalArgs& args, const Tables1D& 
         const double fac = T.w[qx] * T.w[qy] * T.w[qz] * g.detJ * g.scaling;
         const double* nb = WK(c);
         double* ob = WK(c) + OUT0;
+        if (args.vol_flag && args.vol_flag[c0 + c] != 1) {   // XDG species mask: term skipped
+            for (int e = 0; e < C::NCOV * NO; ++e) ob[e * FV + off] = 0.0;
+            continue;
+        }
         volume_point<Phys, MODE, C::G_STATE, C::G_SECOND_VOL, C::VOL_OV, C::VOL_OG>(
             args.ph, x, fac, g.twoh, [&](int f, int comp) { return nb[C::vnode(f) + comp * FV + off]; },
             [&](int oo, int comp, double v) {
@@ -685,6 +691,11 @@ __device__ __forceinline__ void slab_tile(const EvalArgs& args, const Tables1D& 
             if (c >= ncell) continue;
             const int q1 = qf % Q, q2 = qf / Q;
             const int off = q2 * SLF + q1;
+            if (args.face_flag && args.face_flag[(c0 + c) * 6 + 2 * DIR + s] != 1) {   // XDG species mask
+                double* ob = WK(c) + OUTF0 + s * NO * C::NCOF * FF;
+                for (int e = 0; e < NO * C::NCOF; ++e) ob[e * FF + off] = 0.0;
+                continue;
+            }
             int cijk[3];
             cell_ijk(g, c0 + c, cijk);
             const long long nbc = neighbour(g, cijk, DIR, s);
@@ -738,10 +749,12 @@ __device__ __forceinline__ void slab_tile(const EvalArgs& args, const Tables1D& 
         }
         __syncthreads();
     };
-    if (!args.volume_only) {   // uniform over the CTA
-        face_pass(std::integral_constant<int, 0>{});
-        face_pass(std::integral_constant<int, 1>{});
-        face_pass(std::integral_constant<int, 2>{});
+    if constexpr (PASS == 0) {
+        if (!args.volume_only) {   // uniform over the CTA
+            face_pass(std::integral_constant<int, 0>{});
+            face_pass(std::integral_constant<int, 1>{});
+            face_pass(std::integral_constant<int, 2>{});
+        }
     }
 
     // ---------------------------------------------------------- reduce partials and store
@@ -765,11 +778,12 @@ __device__ __forceinline__ void slab_tile(const EvalArgs& args, const Tables1D& 
     }
 }
 
-template <class Phys, int K, int Q, int MODE>
-__global__ void __launch_bounds__(SlabCfg<Phys, K, Q, MODE>::NT, SlabCfg<Phys, K, Q, MODE>::MINB)
+template <class Phys, int K, int Q, int MODE, int PASS = 0>
+__global__ void __launch_bounds__(SlabCfg<Phys, K, Q, MODE, PASS>::NT, SlabCfg<Phys, K, Q, MODE, PASS>::MINB)
 dg_slab_kernel(const __grid_constant__ EvalArgs args) {
     extern __shared__ double smem[];
-    slab_tile<Phys, K, Q, MODE>(args, args.tab, args.cbeg + (long long)blockIdx.x * SlabCfg<Phys, K, Q, MODE>::CPB, smem);
+    slab_tile<Phys, K, Q, MODE, PASS>(args, args.tab,
+                                      args.cbeg + (long long)blockIdx.x * SlabCfg<Phys, K, Q, MODE, PASS>::CPB, smem);
 }
 
 }  // namespace bosss

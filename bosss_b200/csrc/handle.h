@@ -30,6 +30,7 @@ struct bosss_handle {
     int64_t ndom = 0, ncod = 0;
     bosss::KernelEntry kern[3]{};
     int kern_variant[3]{};   // VARIANT_GENERIC / VARIANT_SLAB per mode
+    bosss::KernelEntry kern_vol[3]{};   // face-once path: volume-only slab instances (launch null: none)
     bool check_nan = false;
     // device staging for the host-buffer entry points
     double* dU = nullptr;

@@ -9,5 +9,9 @@ void register_euler3() {
     reg_slab_modes<PhysEuler<3>, 2, 3>(PHYS_EULER);
     reg_slab_modes<PhysEuler<3>, 3, 4>(PHYS_EULER);
     reg_slab_modes<PhysEuler<3>, 4, 5>(PHYS_EULER);
+    reg_slab_volume<PhysEuler<3>, 1, 2>(PHYS_EULER);
+    reg_slab_volume<PhysEuler<3>, 2, 3>(PHYS_EULER);
+    reg_slab_volume<PhysEuler<3>, 3, 4>(PHYS_EULER);
+    reg_slab_volume<PhysEuler<3>, 4, 5>(PHYS_EULER);
 }
 }  // namespace bosss

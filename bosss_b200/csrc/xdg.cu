@@ -1146,11 +1146,11 @@ int bosss_b200_xdg_create(const bosss_op_desc* opA, const bosss_op_desc* opB, co
         if (xopt->moment_degree >= 0) xo.moment_degree = xopt->moment_degree;
         if (xopt->subdivision > 0) xo.subdivision = xopt->subdivision;
     }
-    // the species masks of the bulk evaluation are read by the generic tile kernel only
+    // the species masks of the bulk evaluation are read by the generic and the slab kernels
     bosss_options hopt{};
     if (opt) hopt = *opt;
-    if (hopt.kernel == 2) return fail(BOSSS_ERR_BAD_ARG, "XDG evaluation runs on the generic kernel (species masks)");
-    hopt.kernel = 1;
+    if (hopt.kernel == 3) return fail(BOSSS_ERR_BAD_ARG, "XDG evaluation: kernel 0, 1 or 2");
+    if (hopt.precision != BOSSS_PRECISION_FP64) return fail(BOSSS_ERR_BAD_ARG, "XDG evaluation runs in FP64");
     bosss_xdg* X = new bosss_xdg();
     for (int s = 0; s < 2; ++s) {
         int rc = bosss_b200_create(s == 0 ? opA : opB, grid, &hopt, &X->h[s]);

@@ -690,7 +690,7 @@ class XdgEvaluator:
     sphere ``phi = |x - c| - r``. Vectors are full-grid species frames."""
 
     def __init__(self, opA, opB, grid, degree, center, radius, device=0, cut_nodes_1d=5, fallback_nodes_1d=9,
-                 moment_degree=-1, subdivision=8):
+                 moment_degree=-1, subdivision=8, kernel=C.KERNEL_AUTO):
         self.handle = None
         self.grid, self.degree = grid, degree
         self.descA = opA.descriptor([degree], [degree], grid.dim)
@@ -705,6 +705,7 @@ class XdgEvaluator:
         xo.moment_degree, xo.subdivision = moment_degree, subdivision
         opt = C.Options()
         opt.device = int(device)
+        opt.kernel = int(kernel)
         h = ctypes.c_void_p()
         C.check(C.lib().bosss_b200_xdg_create(ctypes.byref(self.descA), ctypes.byref(self.descB),
                                               ctypes.byref(self.gdesc), ctypes.byref(ls), ctypes.byref(xo),

@@ -116,12 +116,14 @@ def project_nodal(dim, k, nq, h, nodal):
     return (nodal * W[None, :]) @ phi * (detJ * scaling)
 
 
-def euler3d(n=32, k=3, seed=2000, gamma=1.4, quad_order=None, nx=None):
+def euler3d(n=32, k=3, seed=2000, gamma=1.4, quad_order=None, nx=None, periodic=(True, True, True)):
     """``nx``: cells along x (default n) on [0, nx/n] -- the same cell size, an elongated
-    periodic box (the global grid of an x-slab partition with n planes per part)."""
+    periodic box (the global grid of an x-slab partition with n planes per part).
+    ``periodic``: per direction; boundary faces need the boundary-state table
+    (:func:`euler_boundary_states`)."""
     quad_order = 2 * k + 1 if quad_order is None else quad_order
     nx = n if nx is None else nx
-    g = O.Cartesian3DGrid(np.linspace(0.0, nx / n, nx + 1), _linspace_nodes(n), _linspace_nodes(n), True, True, True)
+    g = O.Cartesian3DGrid(np.linspace(0.0, nx / n, nx + 1), _linspace_nodes(n), _linspace_nodes(n), *periodic)
     names = ["rho", "m0", "m1", "m2", "rhoE"]
     op = O.DifferentialOperator(names, [], ["R_" + s for s in names], O.QuadOrderFunc.FixedOrder(quad_order))
     mat = O.Material(gamma)
@@ -151,6 +153,53 @@ def euler3d(n=32, k=3, seed=2000, gamma=1.4, quad_order=None, nx=None):
                    {"workload": ("euler3d_hllc_%d^3_k%d" % (n, k)) if nx == n else
                     ("euler3d_hllc_%dx%d^2_k%d" % (nx, n, k)), "cells": J, "k": k, "seed": seed,
                     "gamma": gamma, "quad_order": quad_order})
+
+
+def euler2d(n=16, k=2, seed=2500, gamma=1.4, quad_order=None, periodic=(True, True)):
+    """2D Euler / HLLC on [0,1]^2 with the seeded state of :func:`euler3d` (two velocity
+    components)."""
+    quad_order = 2 * k + 1 if quad_order is None else quad_order
+    g = O.Cartesian2DGrid(_linspace_nodes(n), _linspace_nodes(n), *periodic)
+    names = ["rho", "m0", "m1", "rhoE"]
+    op = O.DifferentialOperator(names, [], ["R_" + s for s in names], O.QuadOrderFunc.FixedOrder(quad_order))
+    mat = O.Material(gamma)
+    op.EquationComponents["R_rho"].Add(O.OptimizedHLLCDensityFlux(mat, 2))
+    for d in range(2):
+        op.EquationComponents["R_m%d" % d].Add(O.OptimizedHLLCMomentumFlux(mat, d, 2))
+    op.EquationComponents["R_rhoE"].Add(O.OptimizedHLLCEnergyFlux(mat, 2))
+    op.Commit()
+    dom = [O.DGField(g, k, s) for s in names]
+    cod = [O.DGField(g, k, "R_" + s) for s in names]
+    nq = (quad_order + 2) // 2
+    J = g.NoOfCells
+    Q = nq ** 2
+    r = rng(seed)
+    rho = 1.0 + 0.1 * r.uniform(-1, 1, (J, Q))
+    vel = 0.3 * r.uniform(-1, 1, (2, J, Q))
+    p = 1.0 + 0.1 * r.uniform(-1, 1, (J, Q))
+    gMs = gamma * mat.Mach ** 2
+    E = p / (gamma - 1.0) + 0.5 * gMs * rho * (vel ** 2).sum(axis=0)
+    Np = dom[0].Np
+    U = np.empty((J, 4 * Np))
+    for f, val in enumerate([rho, rho * vel[0], rho * vel[1], E]):
+        U[:, f * Np:(f + 1) * Np] = project_nodal(2, k, nq, [1.0 / n] * 2, val)
+    return Problem("euler2d", op, g, dom, cod, U.ravel(),
+                   {"workload": "euler2d_hllc_%d^2_k%d" % (n, k), "cells": J, "k": k, "seed": seed,
+                    "gamma": gamma, "quad_order": quad_order})
+
+
+def euler_boundary_states(xyz, gamma=1.4, mach=None):
+    """Conservative outer states at boundary face nodes (rows of ``xyz``): a smooth prescribed
+    inflow field, rho = 1 + 0.1 sin(2 pi x), u_d = 0.3 cos(2 pi (x_d + d / 4)),
+    p = 1 + 0.1 cos(2 pi sum x) -- what a far-field / supersonic-inlet map returns."""
+    xyz = np.atleast_2d(xyz)
+    D = xyz.shape[1]
+    mach = 1.0 / np.sqrt(gamma) if mach is None else mach
+    rho = 1.0 + 0.1 * np.sin(2 * np.pi * xyz[:, 0])
+    vel = np.stack([0.3 * np.cos(2 * np.pi * (xyz[:, d] + d / 4.0)) for d in range(D)])
+    p = 1.0 + 0.1 * np.cos(2 * np.pi * xyz.sum(axis=1))
+    E = p / (gamma - 1.0) + 0.5 * gamma * mach ** 2 * rho * (vel ** 2).sum(axis=0)
+    return np.stack([rho] + [rho * vel[d] for d in range(D)] + [E], axis=1)
 
 
 def nonlinear_diffusion3d(n=48, k=2, seed=3000, penalty_base=4.0, source=0.0):

@@ -74,7 +74,12 @@ enum bosss_component_type {
     /* OptimizedHLLC{Density,Momentum,Energy}Flux,
      * CompressibleFlowCommon/Convection/OptimizedHLLC*Flux.cs; arguments = all D+2 conservative
      * variables (rho, m_0..m_{D-1}, rhoE). params[0] = gamma, params[1] = Mach;
-     * momentum: params[2] = component index. Only periodic grids (no boundary-condition map). */
+     * momentum: params[2] = component index. Boundary faces (non-periodic directions) take the
+     * outer state from the boundary-state table (bosss_b200_set_boundary_state) and evaluate
+     * the inner-edge HLLC flux with it, as OptimizedHLLCFlux.BorderEdgeFlux
+     * (OptimizedHLLCFlux.cs:61-131) does with the state of its boundary-condition map; the
+     * table holds prescribed states (inflow / far field), not state-dependent conditions
+     * (walls, extrapolated outflow). Such grids run on the generic kernel. */
     BOSSS_COMP_HLLC_DENSITY_FLUX = 10,
     BOSSS_COMP_HLLC_MOMENTUM_FLUX = 11,
     BOSSS_COMP_HLLC_ENERGY_FLUX = 12,
@@ -209,7 +214,7 @@ int bosss_b200_evaluate_device(bosss_handle* h, double alpha, double beta, const
                                double* out_dev, double time, void* stream);
 
 /* Boundary-state table of an operator whose boundary terms take a prescribed outer state
- * (the CNS viscous components): boundary_nodes returns the number of boundary face nodes
+ * (the CNS viscous components, the HLLC fluxes on non-periodic grids): boundary_nodes returns the number of boundary face nodes
  * and, if xyz is not NULL, their physical coordinates (D per node), numbered cell by cell
  * (local order), then face direction d, then side (lower, upper), then the face's Gauss node
  * (the direction after d fastest); set_boundary_state uploads n_nodes * n_domain values, the

@@ -527,16 +527,23 @@ static std::string setup(Problem& P, const bosss_op_desc* op, const bosss_grid_d
         }
         P.cj[j] = (surf + bnd) * 0.5 / vol;
     }
-    // boundary face node numbering of the boundary-state table
+    // boundary face node numbering of the boundary-state table: faces on the boundary of the
+    // (global) grid; the outer faces of a part's ghost planes have no table entry
     P.bnd_off.assign((size_t)P.J * 2 * P.D, -1);
     P.n_bnd_nodes = 0;
     for (int j = 0; j < P.J; ++j)
         for (int d = 0; d < P.D; ++d)
-            for (int s = 0; s < 2; ++s)
-                if (neighbour(P, j, d, s) < 0) {
+            for (int s = 0; s < 2; ++s) {
+                bool boundary = neighbour(P, j, d, s) < 0;
+                if (part) {
+                    const int gi = cell_index_along(P, j, d) + g->global_offset[d];
+                    boundary = !g->global_periodic[d] && (s == 0 ? gi == 0 : gi == g->global_n[d] - 1);
+                }
+                if (boundary) {
                     P.bnd_off[(size_t)j * 2 * P.D + 2 * d + s] = P.n_bnd_nodes;
                     P.n_bnd_nodes += P.nQf;
                 }
+            }
     // component checks
     for (int c = 0; c < op->n_components; ++c) {
         const auto& cp = op->components[c];
@@ -553,8 +560,6 @@ static std::string setup(Problem& P, const bosss_op_desc* op, const bosss_grid_d
             case BOSSS_COMP_HLLC_MOMENTUM_FLUX:
             case BOSSS_COMP_HLLC_ENERGY_FLUX:
                 if (cp.n_args != P.D + 2) return "HLLC needs D+2 arguments";
-                for (int d = 0; d < P.D; ++d)
-                    if (!(part ? g->global_periodic[d] : g->periodic[d])) return "HLLC: only periodic grids";
                 break;
             case ORC_COMP_CNS_SIPG_DENSITY:
             case ORC_COMP_CNS_SIPG_MOMENTUM:
@@ -961,6 +966,24 @@ static void boundary_edge_terms(const Problem& P, const bosss_component& cp, int
                         GAv[k] -= Go[k][l][j] * jump * T(n[l]);
                     }
             gA += flux;
+            break;
+        }
+        case BOSSS_COMP_HLLC_DENSITY_FLUX:
+        case BOSSS_COMP_HLLC_MOMENTUM_FLUX:
+        case BOSSS_COMP_HLLC_ENERGY_FLUX: {
+            // OptimizedHLLCFlux.BorderEdgeFlux (OptimizedHLLCFlux.cs:61-131): Uout from the
+            // boundary condition (the table's state), then InnerEdgeFlux(Uin, Uout) with the
+            // outward normal; only the IN side is kept
+            if (!Ubnd) break;   // rejected by the entry points
+            T Ub[BOSSS_MAX_VARS];
+            T GB[BOSSS_MAX_VARS][3];
+            for (int f = 0; f < P.op.n_domain; ++f) {
+                Ub[f] = T(Ubnd[f]);
+                for (int d = 0; d < 3; ++d) GB[f][d] = T(0.0);
+            }
+            T gB = T(0.0), GBv[3] = {T(0.0), T(0.0), T(0.0)};
+            inner_edge_terms(P, cp, jIn, jIn, UA, GA, (const T*)Ub, (const T(*)[3])GB, n, gA, GAv, gB, GBv);
+            (void)x;
             break;
         }
         default: break;
@@ -1524,8 +1547,11 @@ static int setup_bnd(Problem& P, const bosss_op_desc* op, const bosss_grid_desc*
     P.bnd = bnd;
     if (!bnd && P.n_bnd_nodes > 0)
         for (int c = 0; c < op->n_components; ++c)
-            if (op->components[c].type == ORC_COMP_CNS_SIPG_MOMENTUM || op->components[c].type == ORC_COMP_CNS_SIPG_ENERGY) {
-                g_err = "CNS SIPG on a grid with boundary faces needs the boundary-state table";
+            if (op->components[c].type == ORC_COMP_CNS_SIPG_MOMENTUM || op->components[c].type == ORC_COMP_CNS_SIPG_ENERGY ||
+                op->components[c].type == BOSSS_COMP_HLLC_DENSITY_FLUX ||
+                op->components[c].type == BOSSS_COMP_HLLC_MOMENTUM_FLUX ||
+                op->components[c].type == BOSSS_COMP_HLLC_ENERGY_FLUX) {
+                g_err = "CNS SIPG and HLLC on a grid with boundary faces need the boundary-state table";
                 return BOSSS_ERR_BAD_ARG;
             }
     return 0;

@@ -116,7 +116,7 @@ def vjp(opd, gd, U, W, bnd=None):
     return out
 
 
-def jacobian_dense(opd, gd, U):
+def jacobian_dense(opd, gd, U, bnd=None):
     """Exact Jacobian (dense, small problems only) assembled from the oracle's
     cell-block Jacobian."""
     nd, nc, _ = sizes(opd, gd)
@@ -127,7 +127,8 @@ def jacobian_dense(opd, gd, U):
     blocks = np.zeros(J * NB * Nc * Nd)
     nbr = np.zeros(J * NB, dtype=np.int32)
     U = np.ascontiguousarray(U, dtype=np.float64)
-    _check(lib().orc_jacobian_blocks(ctypes.byref(opd), ctypes.byref(gd), None, _p(U), _p(blocks), _p(nbr)))
+    keep, bp = _bnd(opd, gd, bnd)
+    _check(lib().orc_jacobian_blocks(ctypes.byref(opd), ctypes.byref(gd), bp, _p(U), _p(blocks), _p(nbr)))
     blocks = blocks.reshape(J, NB, Nc, Nd)
     nbr = nbr.reshape(J, NB)
     A = np.zeros((nc, nd))
@@ -142,7 +143,7 @@ def jacobian_dense(opd, gd, U):
     return A
 
 
-def jacobian_blocks(opd, gd, U):
+def jacobian_blocks(opd, gd, U, bnd=None):
     """Cell-block Jacobian: (blocks[J, 1+2D, Nc, Nd], nbr[J, 1+2D])."""
     nd, nc, _ = sizes(opd, gd)
     D = gd.dim
@@ -152,7 +153,8 @@ def jacobian_blocks(opd, gd, U):
     blocks = np.zeros(J * NB * Nc * Nd)
     nbr = np.zeros(J * NB, dtype=np.int32)
     U = np.ascontiguousarray(U, dtype=np.float64)
-    _check(lib().orc_jacobian_blocks(ctypes.byref(opd), ctypes.byref(gd), None, _p(U), _p(blocks), _p(nbr)))
+    keep, bp = _bnd(opd, gd, bnd)
+    _check(lib().orc_jacobian_blocks(ctypes.byref(opd), ctypes.byref(gd), bp, _p(U), _p(blocks), _p(nbr)))
     return blocks.reshape(J, NB, Nc, Nd), nbr.reshape(J, NB)
 
 

@@ -13,6 +13,7 @@
 import numpy as np
 import pytest
 
+from bosss_b200 import _capi as C
 from bosss_b200 import operator as O
 from bosss_b200 import problems as P
 from oracle import oracle as orc
@@ -103,6 +104,19 @@ def test_xdg_evaluate_matches_oracle(xdg_small):
         X.Evaluate(s, 0.5, 0.25, out, U)
         assert rel(out, 0.25 * prev + 0.5 * ref) <= 1e-12
         assert np.array_equal(out[absent], 0.25 * prev[absent])
+
+
+def test_xdg_masked_slab_equals_masked_generic():
+    """The species masks are read by both bulk kernels: the default handles (slab residual for
+    the 3D SIP bulk) and handles forced onto the generic tile give the same species residuals."""
+    opA, opB, g, c, UA, UB = small_case(n=12)
+    with O.XdgEvaluator(opA, opB, g, 2, c, 0.4) as Xs, O.XdgEvaluator(opA, opB, g, 2, c, 0.4,
+                                                                      kernel=C.KERNEL_GENERIC) as Xg:
+        for s, U in enumerate((UA, UB)):
+            a, b = np.zeros_like(U), np.zeros_like(U)
+            Xs.Evaluate(s, 1.0, 0.0, a, U)
+            Xg.Evaluate(s, 1.0, 0.0, b, U)
+            assert rel(a, b) <= 1e-13, (s, rel(a, b))
 
 
 def test_xdg_full_size_matches_oracle():
