@@ -17,10 +17,9 @@ struct bosss_bsr {
     float* d_vals32 = nullptr;  // FP32 copy for the inner solves of the mixed-precision refinement
     double* dx = nullptr;
     double* dy = nullptr;
-    // sliced-ELL copy for the SpMV (built on the first product): `ell_w` block slots per block
-    // row; ell_col[s * nbr + i] the block column of slot s of row i (padding: column 0, zero block);
-    // ell_vals[((s * bc + c) * nbr + i) * br + r] entry (r, c) of that block, so the threads of
-    // consecutive scalar rows read consecutive addresses for every (slot, column)
+    // sliced-ELL copy for the SpMV (built on the first product, spmv.cu): `ell_w` block slots
+    // per block row; ell_col[s * nbr + i] the block column of slot s of row i (padding: column
+    // 0, zero block); values in slices of 32 scalar rows, per slice slot-major then column
     int ell_w = 0;
     int32_t* d_ell_col = nullptr;
     double* d_ell_vals = nullptr;

@@ -558,8 +558,18 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
         delete h;
         return fail(BOSSS_ERR_CUDA, std::string("stream creation: ") + cudaGetErrorString(e));
     }
-    // face-once face terms (3D Euler): selected explicitly (kernel 3) or automatically
-    if ((want == 3 || want == 0) && faces_once_supported(h) && h->variant == VARIANT_SLAB) h->faces_once = true;
+    // face-once face terms (3D Euler): on request only (kernel 3) -- measured on B200 at Euler
+    // 32^3 k=3 slower than the slab kernel's two-sided faces (residual 0.51 vs 0.31 ms, VJP 0.83
+    // vs 0.60 ms); the face buffer is allocated here, not at the first evaluation, so that
+    // evaluations can be captured in CUDA graphs
+    if (want == 3 && faces_once_supported(h) && h->variant == VARIANT_SLAB) {
+        h->faces_once = true;
+        if (faces_once_alloc(h) != BOSSS_OK) {
+            const std::string msg = g_last_error;
+            bosss_b200_destroy(h);
+            return fail(BOSSS_ERR_CUDA, msg);
+        }
+    }
     if (h->faces_once)
         for (int m : {MODE_RES, MODE_VJP}) {
             auto it = reg.find(KernelKey(phys, D, K, Q, m, VARIANT_SLAB_VOL));
