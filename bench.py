@@ -401,7 +401,10 @@ def run_spmv(args):
                    "l2": "flushed between steps (512 MB write outside the timed events)"},
         "rel_err_vs_oracle": err,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None, "kernel": "k_ell_spmv (sliced ELL copy of the block-sparse matrix)",
+                     "frac": achieved / hbm_peak,
+                     "traffic": (load_json(os.path.join(ROOT, "profiles", "traffic.json")) or {}).get(
+                         "bsr_spmv_hex48_k2_bytes_per_launch"),
+                     "kernel": "k_ell_spmv (sliced ELL copy of the block-sparse matrix, 32-row slices)",
                      "algorithmic_bytes": bytes_},
         "e2e": {"value": rows / e2e_s, "unit": "rows/s", "h2d_bytes_per_step": 8 * rows,
                 "d2h_bytes_per_step": 8 * rows},
