@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=32)
     ap.add_argument("--k", type=int, default=3)
-    ap.add_argument("--workload", default="euler3d", choices=["euler3d", "batched", "newton", "xdg", "rk", "spmv"],
+    ap.add_argument("--workload", default="euler3d", choices=["euler3d", "batched", "batched-solve", "newton", "xdg", "rk", "spmv"],
                     help="euler3d: the headline (residual + VJP, Euler/HLLC 32^3 k=3); batched: 256 "
                          "independent advection-diffusion instances (16..48^3, k=1..4) in one captured "
                          "graph; newton: matrix-free Newton-GMRES on -div((1+u^2) grad u) = 1, 48^3; rk: "
@@ -228,6 +228,58 @@ def cpu_baseline_sample(args):
             "sample": "median of %d steps (residual + exact VJP) of %s (same operator and rule, 1/8 of the 32^3 "
                       "cells), C++ FP64 oracle, OpenMP %d threads; single_core_value: median of %d steps on 1 thread"
                       % (len(t_all), pr.config["workload"], cores, len(t_one))}
+
+
+def run_batched_solve(args):
+    """Per-instance implicit-step solves over the batched mix (``bosss_b200_batch_solve``):
+    (I/dt_i + A_i) x_i = b_i for every instance, dt_i = h_i / |a_i| (one cell per time step
+    at the instance's transport speed), FP32 GMRES(30) with block-Jacobi inside FP64
+    refinement to 1e-10; then the adjoint systems on the VJP. value = DOFs solved per second
+    (forward + adjoint); the oracle checks the true residuals of a sample of instances."""
+    import torch
+    from bosss_b200 import operator as O
+    from bosss_b200 import problems as P
+    from oracle import oracle as orc
+    probs = P.batched_advection_diffusion(n_instances=args.instances, seed=5000)
+    n = sum(p.n_dofs for p in probs)
+    dev = torch.device("cuda", 0)
+    b = np.random.default_rng(8).uniform(-1, 1, n)
+    dts = np.array([(1.0 / p.grid.n[0]) / np.linalg.norm(p.config["velocity"]) for p in probs])
+    with O.BatchEvaluator(probs) as B:
+        off = B.dom_offsets
+        bt = torch.from_numpy(b).to(dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x, reps = B.solve(dts, bt, restart=30)
+        torch.cuda.synchronize()
+        t_fwd = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        xa, repa = B.solve(dts, bt, transpose=True, restart=30)
+        torch.cuda.synchronize()
+        t_adj = time.perf_counter() - t0
+        x, xa = x.cpu().numpy(), xa.cpu().numpy()
+    worst = 0.0
+    for i in range(0, len(probs), max(1, len(probs) // 8)):   # oracle check of a sample
+        p = probs[i]
+        if p.n_dofs > 400000:
+            continue
+        sl = slice(off[i], off[i + 1])
+        z = np.zeros(p.n_dofs)
+        r1 = x[sl] / dts[i] + orc.jvp(*p.descs(), z, x[sl]) - b[sl]
+        r2 = xa[sl] / dts[i] + orc.vjp(*p.descs(), z, xa[sl]) - b[sl]
+        worst = max(worst, np.linalg.norm(r1) / np.linalg.norm(b[sl]), np.linalg.norm(r2) / np.linalg.norm(b[sl]))
+    line = {"metric": "batched_implicit_solve_dofs_per_s", "value": 2 * n / (t_fwd + t_adj), "unit": "DOF/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f64 (FP32 inner GMRES)", "data": "synthetic",
+            "config": {"workload": "batched_advdiff_%d_instances_implicit_step_solves" % len(probs), "dofs": n,
+                       "dt": "h / |a| per instance", "restart": 30, "precond": "block-Jacobi (probed)",
+                       "rtol": 1e-10},
+            "s_forward": t_fwd, "s_adjoint": t_adj,
+            "converged": int(sum(r["converged"] for r in reps + repa)), "systems": 2 * len(probs),
+            "krylov_iters_forward": int(sum(r["krylov_iters"] for r in reps)),
+            "krylov_iters_adjoint": int(sum(r["krylov_iters"] for r in repa)),
+            "max_outer_iters": int(max(r["outer_iters"] for r in reps + repa)),
+            "oracle_max_rel_residual_sample": worst}
+    print(json.dumps(line), flush=True)
 
 
 def run_batched(args):
@@ -741,6 +793,8 @@ def main():
         return run_reference(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "batched-solve":
+        return run_batched_solve(args)
     if args.workload == "spmv":
         return run_spmv(args)
     if args.workload == "newton":

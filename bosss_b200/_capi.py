@@ -162,6 +162,7 @@ SIGNATURES = {
     "bosss_b200_destroy": (ctypes.c_int, [_P]),
     "bosss_b200_get_sizes": (ctypes.c_int, [_P, _I64, _I64, _I32]),
     "bosss_b200_kernel_info": (ctypes.c_int, [_P, ctypes.c_int32, _I32, _I32]),
+    "bosss_b200_batch_solve": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, _P, ctypes.POINTER(SolverOpts), _P]),
     "bosss_b200_pmg_create": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_void_p)]),
     "bosss_b200_pmg_apply_device": (ctypes.c_int, [_P, _P, _P, _P]),
     "bosss_b200_pmg_info": (ctypes.c_int, [_P, _I32, _I32, _I64, _I32]),

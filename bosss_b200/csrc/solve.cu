@@ -19,6 +19,7 @@
 #include <cstring>
 #include <vector>
 
+#include "batch.h"
 #include "bsr.h"
 #include "handle.h"
 #include "pmg.h"
@@ -275,6 +276,57 @@ static double norm2(const double* x, long long n, double* partials, cudaStream_t
     double acc = 0.0;
     for (double v : hp) acc += v;
     return std::sqrt(std::max(acc, 0.0));
+}
+
+// ------------------------------------------------------------------ per-instance batched solves
+// distance-1 colouring (face neighbours differ): per direction the smallest modulus m >= 2
+// with n mod m != 1 on periodic directions (so that cells n-1 and 0 differ too); m = 1 for a
+// single cell
+static Colouring make_colouring1(const GridConst& g) {
+    Colouring c;
+    for (int d = 0; d < g.D; ++d) {
+        const int n = g.n[d];
+        int m = 1;
+        if (n > 1) {
+            m = 2;
+            while (g.periodic[d] && n % m == 1) ++m;
+        }
+        c.m[d] = m;
+        c.ncol *= m;
+    }
+    return c;
+}
+
+// column i0 of the diagonal cell blocks of (I/dt + J) from the probe product JV (blocks
+// column-major; the probe covered the cells of colour `col`)
+__global__ void k_scatter_diag(GridConst g, int m0, int m1, int m2, int col, int nb, int i0, double idt,
+                               const double* __restrict__ JV, double* __restrict__ blocks) {
+    const long long n = (long long)g.J * nb;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long j = t / nb;
+        const int r = (int)(t - j * nb);
+        if (cell_colour(g, j, m0, m1, m2) != col) continue;
+        blocks[j * (long long)nb * nb + (long long)i0 * nb + r] = JV[t] + (r == i0 ? idt : 0.0);
+    }
+}
+
+// in-place transpose of every nb x nb block
+__global__ void k_transpose_blocks(long long nblk, int nb, double* __restrict__ blocks) {
+    const long long n = nblk * nb * nb;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long b = t / ((long long)nb * nb);
+        const int e = (int)(t - b * nb * nb), c = e / nb, r = e % nb;
+        if (r < c) {
+            double* B = blocks + b * (long long)nb * nb;
+            const double v = B[c * nb + r];
+            B[c * nb + r] = B[r * nb + c];
+            B[r * nb + c] = v;
+        }
+    }
+}
+
+__global__ void k_iota(long long n, long long* __restrict__ p) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) p[t] = t;
 }
 
 }  // namespace bosss
@@ -534,6 +586,184 @@ int bosss_b200_bsr_solve(bosss_bsr* A, const double* b, double* x, const bosss_s
         if (e2 != cudaSuccess) rc = fail(BOSSS_ERR_CUDA, cudaGetErrorString(e2));
     }
     if (rep) *rep = r;
+    cleanup();
+    return rc;
+}
+
+
+int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, const double* U_dev,
+                           const double* b_dev, double* x_dev, const bosss_solver_opts* opt,
+                           bosss_solver_report* reports) {
+    if (!B || !dt || !b_dev || !x_dev) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    if (transpose != 0 && transpose != 1) return fail(BOSSS_ERR_BAD_ARG, "transpose: 0 or 1");
+    for (int i = 0; i < B->n; ++i) {
+        if (!(dt[i] > 0.0) || !std::isfinite(dt[i])) return fail(BOSSS_ERR_BAD_ARG, "dt must be positive");
+        if (B->h[i]->ndom != B->h[i]->ncod) return fail(BOSSS_ERR_BAD_ARG, "batch solve needs square operators");
+    }
+    bosss_solver_opts o;
+    fill_defaults(opt, o, 1e-10, 30);
+    if (o.precond != 0 && o.precond != 1) return fail(BOSSS_ERR_BAD_ARG, "batch solve: preconditioner 0 or 1");
+    CUDA_TRY(cudaSetDevice(B->device));
+    cudaStream_t s = B->stream;
+    long long nmax = 0, bmax = 0;
+    for (int i = 0; i < B->n; ++i) {
+        const bosss_handle* h = B->h[i];
+        const long long nb = h->ndom / h->base.g.J;
+        nmax = std::max<long long>(nmax, h->ndom);
+        bmax = std::max<long long>(bmax, (long long)h->base.g.J * nb * nb);
+    }
+    double *r64 = nullptr, *t64 = nullptr, *y64 = nullptr, *u0 = nullptr, *blk = nullptr;
+    float *r32 = nullptr, *c32 = nullptr, *t32 = nullptr, *inv = nullptr;
+    long long* rp = nullptr;
+    int* sing = nullptr;
+    KrylovWork<float> kw;
+    auto cleanup = [&]() {
+        cudaFree(r64);
+        cudaFree(t64);
+        cudaFree(y64);
+        cudaFree(u0);
+        cudaFree(blk);
+        cudaFree(r32);
+        cudaFree(c32);
+        cudaFree(t32);
+        cudaFree(inv);
+        cudaFree(rp);
+        cudaFree(sing);
+    };
+    cudaError_t e = cudaMalloc(&r64, sizeof(double) * nmax);
+    if (e == cudaSuccess) e = cudaMalloc(&t64, sizeof(double) * nmax);
+    if (e == cudaSuccess) e = cudaMalloc(&y64, sizeof(double) * nmax);
+    if (e == cudaSuccess && !U_dev) e = cudaMalloc(&u0, sizeof(double) * nmax);
+    if (e == cudaSuccess) e = cudaMalloc(&r32, sizeof(float) * nmax);
+    if (e == cudaSuccess) e = cudaMalloc(&c32, sizeof(float) * nmax);
+    if (e == cudaSuccess) e = cudaMalloc(&t32, sizeof(float) * nmax);
+    if (e == cudaSuccess && o.precond == 1) e = cudaMalloc(&blk, sizeof(double) * bmax);
+    if (e == cudaSuccess && o.precond == 1) e = cudaMalloc(&inv, sizeof(float) * bmax);
+    if (e == cudaSuccess && o.precond == 1) e = cudaMalloc(&rp, sizeof(long long) * (nmax + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&sing, sizeof(int));
+    if (e == cudaSuccess) e = kw.alloc(nmax, o.restart);
+    if (e == cudaSuccess && u0) e = cudaMemsetAsync(u0, 0, sizeof(double) * nmax, s);
+    if (e != cudaSuccess) {
+        cleanup();
+        return fail(BOSSS_ERR_CUDA, std::string("batch solve work arrays: ") + cudaGetErrorString(e));
+    }
+    int rc = 0;
+    auto cu = [&](cudaError_t e2, const char* what) {
+        if (e2 != cudaSuccess && !rc) rc = fail(BOSSS_ERR_CUDA, std::string("batch solve (") + what + "): " +
+                                                                  cudaGetErrorString(e2));
+        return rc == 0;
+    };
+    const int mode = transpose ? MODE_VJP : MODE_JVP;
+    for (int i = 0; i < B->n && !rc; ++i) {
+        bosss_handle* h = B->h[i];
+        const GridConst& g = h->base.g;
+        const long long n = h->ndom, off = B->dom_off[i];
+        const int nb = (int)(n / g.J);
+        const double idt = 1.0 / dt[i];
+        const double* U = U_dev ? U_dev + off : u0;
+        const double* bi = b_dev + off;
+        double* xi = x_dev + off;
+        // y = x/dt + J x (transpose: + J^T x), FP64
+        auto op64 = [&](const double* xin, double* yout) -> int {
+            int r2 = run_mode(h, mode, 1.0, 0.0, U, xin, yout, 0.0, s);
+            if (r2) return r2;
+            k_axpby<double><<<grid_of(n), 256, 0, s>>>(n, idt, xin, 1.0, yout);
+            return cudaGetLastError() == cudaSuccess ? 0 : fail(BOSSS_ERR_CUDA, "batch solve: vector update");
+        };
+        bosss_solver_report r{};
+        // block-Jacobi: the diagonal cell blocks of I/dt + J, probed over a distance-1 colouring
+        if (o.precond == 1) {
+            const Colouring c = make_colouring1(g);
+            for (int col = 0; col < c.ncol && !rc; ++col)
+                for (int i0 = 0; i0 < nb && !rc; ++i0) {
+                    k_probe<<<grid_of(n), 256, 0, s>>>(g, c.m[0], c.m[1], c.m[2], col, nb, i0, t64);
+                    rc = run_mode(h, MODE_JVP, 1.0, 0.0, U, t64, y64, 0.0, s);
+                    if (!rc)
+                        k_scatter_diag<<<grid_of(n), 256, 0, s>>>(g, c.m[0], c.m[1], c.m[2], col, nb, i0, idt, y64, blk);
+                }
+            if (rc) break;
+            if (transpose) k_transpose_blocks<<<grid_of((long long)g.J * nb * nb), 256, 0, s>>>(g.J, nb, blk);
+            k_iota<<<grid_of(g.J + 1), 256, 0, s>>>(g.J + 1, rp);
+            const size_t smem = (size_t)2 * nb * nb * 8;
+            if (!cu(cudaMemsetAsync(sing, 0, sizeof(int), s), "memset") ||
+                !cu(cudaFuncSetAttribute(k_invert_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                    "attribute"))
+                break;
+            k_invert_diag<float><<<(unsigned)g.J, 128, smem, s>>>(nb, rp, blk, inv, sing);
+            int flag = 0;
+            if (!cu(cudaGetLastError(), "block inverse") ||
+                !cu(cudaMemcpyAsync(&flag, sing, sizeof(int), cudaMemcpyDeviceToHost, s), "copy") ||
+                !cu(cudaStreamSynchronize(s), "synchronize"))
+                break;
+            if (flag) {
+                rc = fail(BOSSS_ERR_BAD_ARG, "batch solve: singular diagonal block");
+                break;
+            }
+        }
+        const double bnorm = norm2(bi, n, kw.partials, s);
+        for (int it = 0; it <= o.max_outer; ++it) {
+            // r = b - (I/dt + J) x in FP64
+            rc = op64(xi, r64);
+            if (rc) break;
+            k_axpby<double><<<grid_of(n), 256, 0, s>>>(n, 1.0, bi, -1.0, r64);
+            const double res = norm2(r64, n, kw.partials, s);
+            if (it == 0) r.residual0 = res;
+            r.residual = res;
+            if (!std::isfinite(res)) {
+                rc = fail(BOSSS_ERR_NAN, "non-finite residual in the batch solve");
+                break;
+            }
+            if (res <= std::max(o.rtol * bnorm, o.atol)) {
+                r.converged = 1;
+                break;
+            }
+            if (it == o.max_outer) break;
+            r.outer_iters = it + 1;
+            // FP32 GMRES for the correction, right block-Jacobi, operator applied in FP64
+            k_convert<double, float><<<grid_of(n), 256, 0, s>>>(n, r64, r32);
+            if (!cu(cudaMemsetAsync(c32, 0, sizeof(float) * n, s), "memset")) break;
+            int inner_rc = 0;
+            auto apply = [&](const float* v, float* y) -> cudaError_t {
+                const float* vin = v;
+                if (inv) {
+                    k_apply_blockdiag<float><<<grid_of(n), 256, 0, s>>>(g.J, nb, inv, v, t32);
+                    vin = t32;
+                }
+                k_convert<float, double><<<grid_of(n), 256, 0, s>>>(n, vin, t64);
+                int r2 = op64(t64, y64);
+                if (r2) {
+                    inner_rc = r2;
+                    return cudaErrorUnknown;
+                }
+                k_convert<double, float><<<grid_of(n), 256, 0, s>>>(n, y64, y);
+                return cudaGetLastError();
+            };
+            GmresResult gr = gmres<float>(n, apply, r32, c32, o.restart, o.max_krylov, o.inner_rtol, 0.0, kw.V, kw.w,
+                                          kw.partials, kw.hbuf, s);
+            r.krylov_iters += gr.iters;
+            if (inner_rc) {
+                rc = inner_rc;
+                break;
+            }
+            if (gr.error) {
+                rc = fail(BOSSS_ERR_CUDA, "GMRES: " + std::string(cudaGetErrorString((cudaError_t)gr.error)));
+                break;
+            }
+            const float* corr = c32;
+            if (inv) {
+                k_apply_blockdiag<float><<<grid_of(n), 256, 0, s>>>(g.J, nb, inv, c32, t32);
+                corr = t32;
+            }
+            k_convert<float, double><<<grid_of(n), 256, 0, s>>>(n, corr, t64);
+            k_axpby<double><<<grid_of(n), 256, 0, s>>>(n, 1.0, t64, 1.0, xi);
+            if (!cu(cudaGetLastError(), "update")) break;
+        }
+        if (reports) reports[i] = r;
+    }
+    if (!rc) {
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(BOSSS_ERR_CUDA, cudaGetErrorString(e));
+    }
     cleanup();
     return rc;
 }

@@ -661,6 +661,20 @@ class BatchEvaluator:
         C.check(C.lib().bosss_b200_batch_evaluate(self.handle, mode, alpha, beta, C.ptr(U), C.ptr(V), C.ptr(out), 0.0))
         return out
 
+    def solve(self, dt, b, x=None, U=None, transpose=False, **kw):
+        """Per-instance implicit-step systems (I/dt_i + J_i) x_i = b_i (``transpose``: the
+        adjoint systems), FP32 GMRES inside FP64 refinement; CUDA tensors. ``dt``: one value or
+        one per instance. Returns (x, reports)."""
+        import torch
+        dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (self.n,)))
+        x = torch.zeros_like(b) if x is None else x
+        o = _solver_opts(**kw)
+        reps = (C.SolverReport * self.n)()
+        torch.cuda.synchronize()
+        C.check(C.lib().bosss_b200_batch_solve(self.handle, int(bool(transpose)), C.ptr(dts), C.ptr(U), C.ptr(b),
+                                               C.ptr(x), ctypes.byref(o), ctypes.cast(reps, ctypes.c_void_p)))
+        return x, [_report(r) for r in reps]
+
     def capture(self, U, W, R, G):
         """Capture residual R = Op(U) and adjoint G = J^T W (CUDA tensors) into a CUDA graph."""
         C.check(C.lib().bosss_b200_batch_capture(self.handle, C.ptr(U), C.ptr(W), C.ptr(R), C.ptr(G), 0.0))

@@ -367,6 +367,25 @@ int bosss_b200_batch_autotune(bosss_batch* b, const double* U_dev, const double*
  * per (K, Q) class with the single-grid launch configuration. */
 int bosss_b200_batch_tiles(const bosss_batch* b, int32_t K, int32_t Q, int32_t* tiles, int32_t* lpt);
 
+/* Per-instance implicit-step solves over the batch: for every instance i
+ *   (I/dt[i] + J_i(U)) x_i = b_i          (transpose = 0; JVP as the operator)
+ *   (I/dt[i] + J_i(U))^T x_i = b_i        (transpose = 1; the adjoint system on the VJP)
+ * -- the system of ImplicitEuler.PerformTimeStep, (diag(1/dt) + M) x = state/dt - affine
+ * (ImplicitEuler.cs:86-116; the mass matrix of the orthonormal basis is the identity), and its
+ * adjoint. FP32 GMRES(restart) on
+ * FP32 vectors, the operator applied in FP64, inside FP64 iterative refinement until
+ * ||b_i - A_i x_i|| <= max(rtol ||b_i||, atol) (defaults: rtol 1e-10, 30 refinement steps,
+ * inner tolerance 1e-3; SoftGMRES.cs on a BlockMsrMatrix in the reference, here
+ * matrix-free); precond 1 (default): block-Jacobi on the diagonal cell blocks of
+ * I/dt + J_i, probed with a face-neighbour colouring; 0: none. Device vectors (concatenated
+ * instance vectors, bosss_b200_batch_get_sizes offsets): U the state of the linearisation
+ * (NULL: zero; the Jacobian of the linear advection-diffusion family does not depend on it),
+ * b the right-hand sides, x the initial guesses in and the solutions out. reports: NULL or
+ * n entries. Returns after the solves have completed. */
+int bosss_b200_batch_solve(bosss_batch* b, int32_t transpose, const double* dt, const double* U_dev,
+                           const double* b_dev, double* x_dev, const bosss_solver_opts* opt,
+                           bosss_solver_report* reports);
+
 /* ---- XDG: per-species bulk evaluation with moment-fitted cut-cell rules ----
  * XEvaluatorNonlin.Evaluate, bulk part (XSpatialOperatorMk2_XEvaluators.cs:372-511): for
  * species A (phi < 0) and B (phi >= 0) the species' bulk operator (XLaplace_Bulk =
