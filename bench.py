@@ -240,7 +240,9 @@ def run_batched_solve(args):
     from bosss_b200 import operator as O
     from bosss_b200 import problems as P
     from oracle import oracle as orc
-    probs = P.batched_advection_diffusion(n_instances=args.instances, seed=5000)
+    # SIPLaplace discretises +nu Laplace(u) (ipLaplace.cs:183-186): nu = -0.01 makes the operator
+    # dissipative (du/dt = -Op(u)), so that I/dt + J is the implicit Euler matrix of the mix
+    probs = P.batched_advection_diffusion(n_instances=args.instances, seed=5000, nu=-0.01)
     n = sum(p.n_dofs for p in probs)
     dev = torch.device("cuda", 0)
     b = np.random.default_rng(8).uniform(-1, 1, n)

@@ -219,6 +219,10 @@ def nonlinear_diffusion3d(n=48, k=2, seed=3000, penalty_base=4.0, source=0.0):
 
 
 def advection_diffusion3d(n=16, k=2, seed=5000, nu=0.01, penalty_base=4.0, velocity=None, periodic=True):
+    """Upwind transport with a ~ U[-1,1]^3 plus SIPLaplace(nu). SIPLaplace discretises
+    +nu Laplace(u) (its volume form is -nu grad u . grad v, ipLaplace.cs:183-186), so the
+    operator is div(a u) + nu Laplace(u): nu < 0 gives the dissipative advection-diffusion
+    operator of du/dt = -Op(u)."""
     r = rng(seed)
     a = r.uniform(-1, 1, 3) if velocity is None else np.asarray(velocity, dtype=float)
     g = O.Cartesian3DGrid(_linspace_nodes(n), _linspace_nodes(n), _linspace_nodes(n), periodic, periodic, periodic)

@@ -21,7 +21,14 @@ def rel(a, b):
 
 
 def _batch():
-    return P.batched_advection_diffusion(n_instances=6, seed=78, sizes=(3, 4, 5), degrees=(1, 2, 3))
+    # SIPLaplace discretises +nu Laplace(u) (ipLaplace.cs:183-186), so nu < 0 makes the
+    # advection-diffusion operator dissipative (du/dt = -Op(u) stable) and I/dt + J positive
+    return P.batched_advection_diffusion(n_instances=6, seed=78, sizes=(3, 4, 5), degrees=(1, 2, 3), nu=-0.01)
+
+
+def _dt(probs):
+    # one cell per time step at the instance's transport speed
+    return np.array([(1.0 / p.grid.n[0]) / np.linalg.norm(p.config["velocity"]) for p in probs])
 
 
 @pytest.mark.parametrize("precond", [1, 0], ids=["block_jacobi", "none"])
@@ -30,7 +37,7 @@ def test_batch_solve_forward_and_adjoint(precond):
     probs = _batch()
     n = sum(p.n_dofs for p in probs)
     b = np.random.default_rng(3).uniform(-1, 1, n)
-    dt = np.array([0.05 + 0.01 * i for i in range(len(probs))])
+    dt = _dt(probs)
     with O.BatchEvaluator(probs) as B:
         off = B.dom_offsets
         bt = torch.from_numpy(b).cuda()
