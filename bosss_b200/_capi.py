@@ -131,7 +131,12 @@ class LevelSetDesc(ctypes.Structure):
 
 class XdgOpts(ctypes.Structure):
     _fields_ = [("cut_nodes_1d", ctypes.c_int32), ("fallback_nodes_1d", ctypes.c_int32),
-                ("moment_degree", ctypes.c_int32), ("subdivision", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8)]
+                ("moment_degree", ctypes.c_int32), ("subdivision", ctypes.c_int32), ("rule", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 7)]
+
+
+XDG_RULE_MOMENT_FITTING = 0
+XDG_RULE_SAYE = 1
 
 
 LEVELSET_SPHERE = 1
@@ -162,6 +167,7 @@ SIGNATURES = {
     "bosss_b200_destroy": (ctypes.c_int, [_P]),
     "bosss_b200_get_sizes": (ctypes.c_int, [_P, _I64, _I64, _I32]),
     "bosss_b200_kernel_info": (ctypes.c_int, [_P, ctypes.c_int32, _I32, _I32]),
+    "bosss_b200_saye_rule": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, ctypes.c_int32, _I64, _P, _P]),
     "bosss_b200_batch_solve": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, _P, ctypes.POINTER(SolverOpts), _P]),
     "bosss_b200_pmg_create": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_void_p)]),
     "bosss_b200_pmg_apply_device": (ctypes.c_int, [_P, _P, _P, _P]),

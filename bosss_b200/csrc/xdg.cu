@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "handle.h"
@@ -847,6 +848,300 @@ struct bosss_xdg {
 
 namespace bosss {
 
+// ---------------------------------------------------------------------------------------
+// Saye-type rules for the species part of a cut cell or cut face (the reference's default
+// rule family, SayeGaussRule_Algorithm.cs / _Cube.cs / _Square.cs, after R. Saye, "High-order
+// quadrature methods for implicitly defined surfaces and volumes in hyperrectangles", SIAM J.
+// Sci. Comput. 37 (2015)), written for the sphere level set in reference coordinates of the
+// item ([-1,1]^dim). Recursion over the free directions of a box: functions with one sign on
+// the box are dropped (or empty the box, if the sign is the wrong one); with none left, a
+// tensor Gauss rule; else a height direction k in which every function is strictly monotone
+// (the largest |d phi / d x_k| at the centre among those), the functions restricted to the two
+// faces x_k = lo_k, hi_k become the (sign-free, split-only) functions of the box without k,
+// whose rule is built recursively; at each of its nodes the line in direction k is split at
+// the functions' roots and the pieces with the required sign get a Gauss rule. Boxes without
+// such a direction are halved in every free direction (at most 8 times; then a tensor rule
+// filtered by the sign at the nodes).
+struct SayeFn {
+    unsigned fixmask;   // reference directions fixed at fixval
+    double fixval[3];
+    int sign;           // required sign of phi (+1 / -1), 0: split only
+};
+
+struct SayeItem {
+    const LevelSetDev* L;
+    int dim, dir, sp;
+    double center[3], h[3];
+    const std::vector<double>* gx;
+    const std::vector<double>* gw;
+    std::vector<double>* nodes;   // 3 per node (reference coordinates)
+    std::vector<double>* weights;
+    // physical point of the full reference coordinates r (dim entries used)
+    void phys(const double* r, double* x) const {
+        for (int d = 0; d < 3; ++d) x[d] = center[d];
+        if (dim == 3) {
+            for (int d = 0; d < 3; ++d) x[d] += 0.5 * h[d] * r[d];
+        } else {
+            const int t1 = (dir == 0) ? 1 : 0, t2 = (dir == 2) ? 1 : 2;
+            x[t1] += 0.5 * h[t1] * r[0];
+            x[t2] += 0.5 * h[t2] * r[1];
+        }
+    }
+    int pdir(int k) const {   // physical direction of reference direction k
+        if (dim == 3) return k;
+        const int t1 = (dir == 0) ? 1 : 0, t2 = (dir == 2) ? 1 : 2;
+        return k == 0 ? t1 : t2;
+    }
+    double value(const SayeFn& f, const double* r) const {
+        double rr[3] = {r[0], r[1], r[2]}, x[3];
+        for (int d = 0; d < dim; ++d)
+            if (f.fixmask & (1u << d)) rr[d] = f.fixval[d];
+        phys(rr, x);
+        return ls_phi(*L, x);
+    }
+    // physical box of f over the reference box [lo, hi] (fixed directions degenerate)
+    void pbox(const SayeFn& f, const double* lo, const double* hi, double* plo, double* phi_, int& mask) const {
+        double a[3] = {lo[0], lo[1], lo[2]}, b[3] = {hi[0], hi[1], hi[2]};
+        for (int d = 0; d < dim; ++d)
+            if (f.fixmask & (1u << d)) a[d] = b[d] = f.fixval[d];
+        double xa[3], xb[3];
+        phys(a, xa);
+        phys(b, xb);
+        mask = 0;
+        for (int d = 0; d < 3; ++d) {
+            plo[d] = std::min(xa[d], xb[d]);
+            phi_[d] = std::max(xa[d], xb[d]);
+            if (phi_[d] > plo[d]) mask |= 1 << d;
+        }
+    }
+    int sign_on(const SayeFn& f, const double* lo, const double* hi) const {
+        double plo[3], phi_[3];
+        int mask;
+        pbox(f, lo, hi, plo, phi_, mask);
+        return ls_box(*L, plo, phi_, mask);
+    }
+    // usable height direction k over the box: the sphere's d phi / d x_m = (x_m - c_m) / |x - c|
+    // keeps its sign iff c_m lies outside the physical range; it is also kept away from zero by
+    // asking c_m to be at least a quarter of the box width outside (closer boxes are split, so
+    // that the height function has no near-vertical tangent inside a piece)
+    bool monotone(const SayeFn& f, const double* lo, const double* hi, int k) const {
+        double plo[3], phi_[3];
+        int mask;
+        pbox(f, lo, hi, plo, phi_, mask);
+        const int m = pdir(k);
+        const double w = 0.25 * (phi_[m] - plo[m]);
+        return L->c[m] < plo[m] - w || L->c[m] > phi_[m] + w;
+    }
+    double slope(const SayeFn& f, const double* r, int k) const {
+        double rr[3] = {r[0], r[1], r[2]}, x[3];
+        for (int d = 0; d < dim; ++d)
+            if (f.fixmask & (1u << d)) rr[d] = f.fixval[d];
+        phys(rr, x);
+        const double dist = std::sqrt((x[0] - L->c[0]) * (x[0] - L->c[0]) + (x[1] - L->c[1]) * (x[1] - L->c[1]) +
+                                      (x[2] - L->c[2]) * (x[2] - L->c[2]));
+        const int m = pdir(k);
+        return dist > 0.0 ? (x[m] - L->c[m]) / dist * 0.5 * h[m] : 0.0;
+    }
+};
+
+// root of the monotone function t -> f(r with r[k] = t) in (a, b), f(a) f(b) < 0
+static double saye_root(const SayeItem& S, const SayeFn& f, double* r, int k, double a, double b, double fa) {
+    double lo = a, hi = b, flo = fa;
+    for (int it = 0; it < 200 && hi - lo > 1e-15 * std::max(1.0, std::fabs(lo)); ++it) {
+        const double m = 0.5 * (lo + hi);
+        r[k] = m;
+        const double fm = S.value(f, r);
+        if (fm == 0.0) return m;
+        if ((fm < 0.0) == (flo < 0.0)) {
+            lo = m;
+            flo = fm;
+        } else {
+            hi = m;
+        }
+    }
+    return 0.5 * (lo + hi);
+}
+
+// emit(r, w): nodes of the free directions `free` (bit mask) of the box [lo, hi]; r holds
+// the values of all directions, entries of non-free directions set by the caller
+using SayeEmit = std::function<void(double*, double)>;
+static void saye_box(const SayeItem& S, unsigned free, const double* lo, const double* hi, std::vector<SayeFn> fns,
+                     int depth, double* r, const SayeEmit& emit);
+
+static void saye_tensor(const SayeItem& S, unsigned free, const double* lo, const double* hi, double* r,
+                        const std::vector<SayeFn>* filter, const SayeEmit& emit) {
+    int dirs[3], nf = 0;
+    for (int d = 0; d < S.dim; ++d)
+        if (free & (1u << d)) dirs[nf++] = d;
+    const std::vector<double>& gx = *S.gx;
+    const std::vector<double>& gw = *S.gw;
+    const int q = (int)gx.size();
+    int tot = 1;
+    for (int i = 0; i < nf; ++i) tot *= q;
+    for (int t = 0; t < tot; ++t) {
+        double w = 1.0;
+        int u = t;
+        for (int i = 0; i < nf; ++i) {
+            const int d = dirs[i], j = u % q;
+            u /= q;
+            r[d] = 0.5 * (lo[d] + hi[d]) + 0.5 * (hi[d] - lo[d]) * gx[j];
+            w *= 0.5 * (hi[d] - lo[d]) * gw[j];
+        }
+        bool ok = true;
+        if (filter)
+            for (const SayeFn& f : *filter)
+                if (f.sign != 0) {
+                    const double v = S.value(f, r);
+                    if (f.sign < 0 ? !(v < 0.0) : (v < 0.0)) ok = false;
+                }
+        if (ok) emit(r, w);
+    }
+}
+
+// 1D integration along k at the current r: split at the functions' roots, keep the pieces
+// whose midpoint has every required sign
+static void saye_line(const SayeItem& S, int k, double a, double b, const std::vector<SayeFn>& fns, double* r,
+                      double w0, const SayeEmit& emit) {
+    std::vector<double> br = {a, b};
+    for (const SayeFn& f : fns) {
+        r[k] = a;
+        const double fa = S.value(f, r);
+        r[k] = b;
+        const double fb = S.value(f, r);
+        if ((fa < 0.0) != (fb < 0.0) && fa != 0.0 && fb != 0.0) br.push_back(saye_root(S, f, r, k, a, b, fa));
+    }
+    std::sort(br.begin(), br.end());
+    const std::vector<double>& gx = *S.gx;
+    const std::vector<double>& gw = *S.gw;
+    for (size_t i = 0; i + 1 < br.size(); ++i) {
+        const double t0 = br[i], t1 = br[i + 1];
+        if (!(t1 > t0)) continue;
+        r[k] = 0.5 * (t0 + t1);
+        bool ok = true;
+        for (const SayeFn& f : fns)
+            if (f.sign != 0) {
+                const double v = S.value(f, r);
+                if (f.sign < 0 ? !(v < 0.0) : (v < 0.0)) ok = false;
+            }
+        if (!ok) continue;
+        for (size_t j = 0; j < gx.size(); ++j) {
+            r[k] = 0.5 * (t0 + t1) + 0.5 * (t1 - t0) * gx[j];
+            emit(r, w0 * 0.5 * (t1 - t0) * gw[j]);
+        }
+    }
+}
+
+static void saye_box(const SayeItem& S, unsigned free, const double* lo, const double* hi, std::vector<SayeFn> fns,
+                     int depth, double* r, const SayeEmit& emit) {
+    // drop functions of one sign on the box
+    std::vector<SayeFn> live;
+    for (const SayeFn& f : fns) {
+        const int sg = S.sign_on(f, lo, hi);
+        if (sg == 0) {
+            live.push_back(f);
+            continue;
+        }
+        if (f.sign != 0 && sg != f.sign) return;   // the box lies in the other species
+    }
+    if (live.empty()) {
+        saye_tensor(S, free, lo, hi, r, nullptr, emit);
+        return;
+    }
+    int nf = 0, only = -1;
+    for (int d = 0; d < S.dim; ++d)
+        if (free & (1u << d)) {
+            ++nf;
+            only = d;
+        }
+    if (nf == 1) {
+        saye_line(S, only, lo[only], hi[only], live, r, 1.0, emit);
+        return;
+    }
+    // height direction: every live function strictly monotone, largest slope of the first
+    double rc[3] = {r[0], r[1], r[2]};
+    for (int d = 0; d < S.dim; ++d)
+        if (free & (1u << d)) rc[d] = 0.5 * (lo[d] + hi[d]);
+    int k = -1;
+    double best = -1.0;
+    for (int d = 0; d < S.dim; ++d) {
+        if (!(free & (1u << d))) continue;
+        bool mono = true;
+        for (const SayeFn& f : live) mono = mono && S.monotone(f, lo, hi, d);
+        if (!mono) continue;
+        const double sl = std::fabs(S.slope(live[0], rc, d));
+        if (sl > best) {
+            best = sl;
+            k = d;
+        }
+    }
+    if (k < 0) {
+        if (depth >= 8) {
+            saye_tensor(S, free, lo, hi, r, &live, emit);
+            return;
+        }
+        const int nch = 1 << nf;
+        for (int c = 0; c < nch; ++c) {
+            double l2[3] = {lo[0], lo[1], lo[2]}, h2[3] = {hi[0], hi[1], hi[2]};
+            int bit = 0;
+            for (int d = 0; d < S.dim; ++d) {
+                if (!(free & (1u << d))) continue;
+                const double mid = 0.5 * (lo[d] + hi[d]);
+                if ((c >> bit) & 1) l2[d] = mid;
+                else h2[d] = mid;
+                ++bit;
+            }
+            saye_box(S, free, l2, h2, live, depth + 1, r, emit);
+        }
+        return;
+    }
+    // reduced problem without k: the live functions on the two faces x_k = lo_k, hi_k
+    std::vector<SayeFn> red;
+    for (const SayeFn& f : live)
+        for (int side = 0; side < 2; ++side) {
+            SayeFn g = f;
+            g.fixmask |= 1u << k;
+            g.fixval[k] = side ? hi[k] : lo[k];
+            g.sign = 0;
+            red.push_back(g);
+        }
+    const double a = lo[k], b = hi[k];
+    const SayeEmit inner = [&](double* rr, double w) { saye_line(S, k, a, b, live, rr, w, emit); };
+    saye_box(S, free & ~(1u << k), lo, hi, red, depth, r, inner);
+}
+
+// Saye-type rule of an item's species part: appends nodes (reference coordinates, 3 per node)
+// and weights (reference measure); returns the node count
+static int saye_item_rule(const LevelSetDev& L, const CutItem& it, const std::vector<double>& gx,
+                          const std::vector<double>& gw, std::vector<double>& nodes, std::vector<double>& weights) {
+    SayeItem S;
+    S.L = &L;
+    S.dim = it.dim;
+    S.dir = it.dir;
+    S.sp = it.sp;
+    for (int d = 0; d < 3; ++d) {
+        S.center[d] = it.center[d];
+        S.h[d] = it.h[d];
+    }
+    S.gx = &gx;
+    S.gw = &gw;
+    S.nodes = &nodes;
+    S.weights = &weights;
+    const double lo[3] = {-1.0, -1.0, it.dim == 3 ? -1.0 : 0.0}, hi[3] = {1.0, 1.0, it.dim == 3 ? 1.0 : 0.0};
+    SayeFn f{};
+    f.fixmask = 0;
+    f.sign = it.sp;   // species A: phi < 0, B: phi >= 0
+    const size_t n0 = weights.size();
+    double r[3] = {0.0, 0.0, 0.0};
+    const SayeEmit emit = [&](double* rr, double w) {
+        nodes.push_back(rr[0]);
+        nodes.push_back(rr[1]);
+        nodes.push_back(it.dim == 3 ? rr[2] : 0.0);
+        weights.push_back(w);
+    };
+    saye_box(S, it.dim == 3 ? 7u : 3u, lo, hi, {f}, 0, r, emit);
+    return (int)(weights.size() - n0);
+}
+
 static int build_species(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
     const GridConst& g = X->h[s]->base.g;
     const int sp = s == 0 ? -1 : +1;
@@ -860,6 +1155,7 @@ static int build_species(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
     auto& nodes = X->nodes[s];
     items.clear();
     nodes.clear();
+    X->weights[s].clear();
     const int pmax = xo.moment_degree;
     auto add_item = [&](long long cell, int dim, int dir, int side, const double* center, const double* hh) {
         CutItem it{};
@@ -872,6 +1168,12 @@ static int build_species(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
         for (int d = 0; d < 3; ++d) {
             it.center[d] = center[d];
             it.h[d] = hh[d];
+        }
+        if (xo.rule == 1) {   // Saye-type rule: nodes and weights directly
+            it.node_off = (long long)nodes.size() / 3;
+            it.nnodes = saye_item_rule(X->ls, it, gx5, gw5, nodes, X->weights[s]);
+            items.push_back(it);
+            return;
         }
         // candidate nodes: tensor Gauss nodes of the species part, finer set for small parts
         auto collect = [&](const std::vector<double>& gx, bool all) {
@@ -961,7 +1263,8 @@ static int upload_and_fit(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
     CUDA_TRY(cudaMalloc(&X->d_face[s], X->face[s].size()));
     CUDA_TRY(cudaMemcpy(X->d_vol[s], X->vol[s].data(), X->vol[s].size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(X->d_face[s], X->face[s].data(), X->face[s].size(), cudaMemcpyHostToDevice));
-    X->weights[s].assign(nn, 0.0);
+    const bool saye = xo.rule == 1;   // weights already set by the Saye-type rules
+    if (!saye) X->weights[s].assign(nn, 0.0);
     X->fitted_deg[s].assign(n, -1);
     X->fit_resid[s].assign(n, 0.0);
     if (n == 0) return BOSSS_OK;
@@ -987,14 +1290,40 @@ static int upload_and_fit(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
     }
     k_moments<<<n, 256>>>(X->d_items[s], n, X->ls, sub, d_mom);
     CUDA_TRY(cudaGetLastError());
-    k_weight_solve<<<n, 128>>>(X->d_items[s], n, X->d_nodes[s], d_mom, X->d_weights[s], d_deg, d_res);
-    CUDA_TRY(cudaGetLastError());
+    if (!saye) {
+        k_weight_solve<<<n, 128>>>(X->d_items[s], n, X->d_nodes[s], d_mom, X->d_weights[s], d_deg, d_res);
+        CUDA_TRY(cudaGetLastError());
+    }
     CUDA_TRY(cudaDeviceSynchronize());
-    CUDA_TRY(cudaMemcpy(X->weights[s].data(), X->d_weights[s], sizeof(double) * nn, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(X->fitted_deg[s].data(), d_deg, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(X->fit_resid[s].data(), d_res, sizeof(double) * n, cudaMemcpyDeviceToHost));
     X->moments[s].assign((size_t)XDG_MAXM * n, 0.0);
     CUDA_TRY(cudaMemcpy(X->moments[s].data(), d_mom, sizeof(double) * XDG_MAXM * n, cudaMemcpyDeviceToHost));
+    if (saye) {
+        // the rule's residual against the integrated moments: || Phi w - b || / || b ||
+        if (nn) CUDA_TRY(cudaMemcpy(X->d_weights[s], X->weights[s].data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
+        for (int r = 0; r < n; ++r) {
+            const CutItem& it = items[r];
+            const int M = it.dim == 3 ? nmodes3(it.p) : nmodes2(it.p);
+            double acc[XDG_MAXM] = {0.0}, v[XDG_MAXM];
+            for (int q = 0; q < it.nnodes; ++q) {
+                const double* xi = &X->nodes[s][(it.node_off + q) * 3];
+                if (it.dim == 3) basis3(it.p, xi, v);
+                else basis2(it.p, xi, v);
+                for (int m = 0; m < M; ++m) acc[m] += X->weights[s][it.node_off + q] * v[m];
+            }
+            double num = 0.0, den = 0.0;
+            for (int m = 0; m < M; ++m) {
+                const double b = X->moments[s][(size_t)r * XDG_MAXM + m];
+                num += (acc[m] - b) * (acc[m] - b);
+                den += b * b;
+            }
+            X->fit_resid[s][r] = std::sqrt(num) / std::max(std::sqrt(den), 1e-300);
+            X->fitted_deg[s][r] = it.p;
+        }
+    } else {
+        CUDA_TRY(cudaMemcpy(X->weights[s].data(), X->d_weights[s], sizeof(double) * nn, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(X->fitted_deg[s].data(), d_deg, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(X->fit_resid[s].data(), d_res, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    }
     cudaFree(d_mom);
     cudaFree(d_deg);
     cudaFree(d_res);
@@ -1145,7 +1474,9 @@ int bosss_b200_xdg_create(const bosss_op_desc* opA, const bosss_op_desc* opB, co
         if (xopt->fallback_nodes_1d > 0) xo.fallback_nodes_1d = xopt->fallback_nodes_1d;
         if (xopt->moment_degree >= 0) xo.moment_degree = xopt->moment_degree;
         if (xopt->subdivision > 0) xo.subdivision = xopt->subdivision;
+        xo.rule = xopt->rule;
     }
+    if (xo.rule != 0 && xo.rule != 1) return fail(BOSSS_ERR_BAD_ARG, "XDG rule family: 0 or 1");
     // the species masks of the bulk evaluation are read by the generic and the slab kernels
     bosss_options hopt{};
     if (opt) hopt = *opt;
@@ -1255,6 +1586,41 @@ int bosss_b200_xdg_set_length_scales(bosss_xdg* X, int32_t species, const double
         X->len[species] = X->len_default[species];
     }
     return apply_length_scales(X, species);
+}
+
+int bosss_b200_saye_rule(const bosss_levelset_desc* ls, int32_t dim, int32_t dir, int32_t species,
+                         const double* center, const double* h, int32_t nodes_1d, int64_t* n_nodes, double* nodes,
+                         double* weights) {
+    if (!ls || !center || !h || !n_nodes) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    if (ls->type != BOSSS_LEVELSET_SPHERE || !(ls->params[3] > 0.0))
+        return fail(BOSSS_ERR_BAD_ARG, "Saye rule: sphere level set phi = |x - c| - r, r > 0");
+    if ((dim != 2 && dim != 3) || dir < 0 || dir > 2 || (species != -1 && species != 1) || nodes_1d < 1 ||
+        nodes_1d > 16)
+        return fail(BOSSS_ERR_BAD_ARG, "Saye rule: dim 2 or 3, dir 0..2, species -1 or +1, 1..16 nodes");
+    for (int d = 0; d < 3; ++d)
+        if (!(h[d] > 0.0)) return fail(BOSSS_ERR_BAD_ARG, "Saye rule: positive cell size");
+    LevelSetDev L{};
+    L.type = ls->type;
+    for (int d = 0; d < 3; ++d) L.c[d] = ls->params[d];
+    L.r = ls->params[3];
+    CutItem it{};
+    it.dim = dim;
+    it.dir = dir;
+    it.sp = species;
+    for (int d = 0; d < 3; ++d) {
+        it.center[d] = center[d];
+        it.h[d] = h[d];
+    }
+    std::vector<double> gx, gw, nd, wt;
+    gauss(nodes_1d, gx, gw);
+    const int n = saye_item_rule(L, it, gx, gw, nd, wt);
+    if (nodes && weights) {
+        if (*n_nodes < n) return fail(BOSSS_ERR_BAD_ARG, "Saye rule: arrays too small");
+        std::memcpy(nodes, nd.data(), sizeof(double) * nd.size());
+        std::memcpy(weights, wt.data(), sizeof(double) * wt.size());
+    }
+    *n_nodes = n;
+    return BOSSS_OK;
 }
 
 int bosss_b200_xdg_destroy(bosss_xdg* X) {

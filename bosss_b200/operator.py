@@ -704,7 +704,7 @@ class XdgEvaluator:
     sphere ``phi = |x - c| - r``. Vectors are full-grid species frames."""
 
     def __init__(self, opA, opB, grid, degree, center, radius, device=0, cut_nodes_1d=5, fallback_nodes_1d=9,
-                 moment_degree=-1, subdivision=8, kernel=C.KERNEL_AUTO):
+                 moment_degree=-1, subdivision=8, kernel=C.KERNEL_AUTO, rule=C.XDG_RULE_MOMENT_FITTING):
         self.handle = None
         self.grid, self.degree = grid, degree
         self.descA = opA.descriptor([degree], [degree], grid.dim)
@@ -717,6 +717,7 @@ class XdgEvaluator:
         xo = C.XdgOpts()
         xo.cut_nodes_1d, xo.fallback_nodes_1d = cut_nodes_1d, fallback_nodes_1d
         xo.moment_degree, xo.subdivision = moment_degree, subdivision
+        xo.rule = int(rule)
         opt = C.Options()
         opt.device = int(device)
         opt.kernel = int(kernel)

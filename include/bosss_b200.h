@@ -409,7 +409,12 @@ typedef struct bosss_xdg_opts {
     int32_t fallback_nodes_1d;  /* candidates for species parts with < 8 nodes (default 9) */
     int32_t moment_degree;      /* fitted polynomial degree (default min(2k, 4)); <0: default */
     int32_t subdivision;        /* moment integration: S x S coarse boxes, cut ones S x S again (default 8) */
-    int32_t reserved[8];
+    int32_t rule;               /* cut-cell rule family: 0 = moment fitting on Gauss-node subsets (default),
+                                   1 = Saye-type recursive Gauss rules (the reference's default,
+                                   SayeGaussRule_*.cs), cut_nodes_1d Gauss nodes per direction and
+                                   piece; moments are still integrated and the rules' residual
+                                   against them is reported as the fit residual */
+    int32_t reserved[7];
 } bosss_xdg_opts;
 
 typedef struct bosss_xdg bosss_xdg;
@@ -428,6 +433,16 @@ int bosss_b200_xdg_info(const bosss_xdg* X, int32_t species, int64_t* n_cells, i
  * (reference coordinates of the cell, or of the face in its two in-plane directions);
  * weights[nodes]; vol_flags[J] and face_flags[J*6] (0 absent, 1 standard rule, 2 cut rule).
  * Any output pointer may be NULL. */
+/* Saye-type rule of one species part of a box, host computation (no device needed): the part
+ * {phi < 0} (species -1) or {phi >= 0} (species +1) of the cell [center - h/2, center + h/2]
+ * (dim 3) or of its face normal to `dir` through `center` (dim 2; center[dir] is the face
+ * coordinate), nodes_1d Gauss nodes per direction and piece. Nodes in reference coordinates
+ * of the cell / face ([-1,1]^dim, 3 per node, unused entries 0), weights in the reference
+ * measure. Call with nodes = weights = NULL to get the count in *n_nodes, then with arrays of
+ * that size. */
+int bosss_b200_saye_rule(const bosss_levelset_desc* ls, int32_t dim, int32_t dir, int32_t species,
+                         const double* center, const double* h, int32_t nodes_1d, int64_t* n_nodes, double* nodes,
+                         double* weights);
 int bosss_b200_xdg_get_rules(const bosss_xdg* X, int32_t species, int64_t* n_items, int64_t* item_info,
                              int64_t* node_offsets, double* nodes, double* weights, unsigned char* vol_flags,
                              unsigned char* face_flags);

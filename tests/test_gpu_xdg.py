@@ -119,6 +119,31 @@ def test_xdg_masked_slab_equals_masked_generic():
             assert rel(a, b) <= 1e-13, (s, rel(a, b))
 
 
+def test_saye_rules_evaluate_and_volume():
+    """Saye-type rules (rule family 1, 8 Gauss nodes per direction and piece): the species-A
+    rules plus the full cells give the ball volume to 1e-9 (the moment-fitted family: 1e-4,
+    the accuracy of its subdivided moment integration), and the evaluation with these rules
+    equals the oracle's with the same rules."""
+    opA, opB, g, c, UA, UB = small_case()
+    with O.XdgEvaluator(opA, opB, g, 2, c, 0.4, rule=C.XDG_RULE_SAYE, cut_nodes_1d=8) as X:
+        h = 2.0 / 10
+        detJ = (h / 2) ** 3
+        R0 = X.rules(0)
+        v = np.sum(R0["vol_flags"] == 1) * 8 * detJ
+        for r, (cell, dim, d, side, deg) in enumerate(R0["info"]):
+            if dim == 3:
+                v += R0["weights"][R0["offsets"][r]:R0["offsets"][r + 1]].sum() * detJ
+        exact = 4.0 / 3.0 * np.pi * 0.4 ** 3
+        assert abs(v - exact) <= 1e-9 * exact, (v, exact)
+        for s, (op, U) in enumerate([(opA, UA), (opB, UB)]):
+            R = X.rules(s)
+            ref = orc.xdg_evaluate(op.descriptor([2], [2], 3), g.desc(), R, U, length_scales=X.length_scales(s))
+            out = np.zeros_like(U)
+            X.Evaluate(s, 1.0, 0.0, out, U)
+            assert rel(out, ref) <= 1e-12, (s, rel(out, ref))
+            assert X.info(s)["max_fit_residual"] <= 1e-3
+
+
 def test_xdg_full_size_matches_oracle():
     """The full 128^3, k=2 case: both species against the oracle with the same rules."""
     import torch
