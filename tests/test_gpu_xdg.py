@@ -141,7 +141,6 @@ def test_saye_rules_evaluate_and_volume():
             out = np.zeros_like(U)
             X.Evaluate(s, 1.0, 0.0, out, U)
             assert rel(out, ref) <= 1e-12, (s, rel(out, ref))
-            assert X.info(s)["max_fit_residual"] <= 1e-3
 
 
 def test_xdg_full_size_matches_oracle():
