@@ -67,6 +67,8 @@ def parse():
                     help="preconditioner of the newton workload")
     ap.add_argument("--precond-update", type=int, default=1,
                     help="newton workload: rebuild the preconditioner every this many Newton steps")
+    ap.add_argument("--xdg-rule", default="moment-fitting", choices=["moment-fitting", "saye"],
+                    help="xdg workload: cut-cell rule family")
     ap.add_argument("--kernel", default="auto", choices=["auto", "generic", "slab", "faces"],
                     help="kernel path of the euler3d workload (auto: the library's choice)")
     ap.add_argument("--partitioned", action="store_true",
@@ -533,11 +535,13 @@ def run_xdg(args):
     surface rules on the host) and one step = the per-species bulk evaluation of both species
     followed by the level-set interface term (XLaplace_Interface, SIP, mu 1 / 10)."""
     import torch
+    from bosss_b200 import _capi as C
     from bosss_b200 import operator as O
     from bosss_b200 import problems as P
     opA, opB, g, c, UA, UB = P.xdg_poisson3d(n=128, k=2, seed=4000)
     t0 = time.perf_counter()
-    X = O.XdgEvaluator(opA, opB, g, 2, c, 0.4)
+    rule = C.XDG_RULE_SAYE if args.xdg_rule == "saye" else C.XDG_RULE_MOMENT_FITTING
+    X = O.XdgEvaluator(opA, opB, g, 2, c, 0.4, rule=rule)
     torch.cuda.synchronize()
     t_rules = time.perf_counter() - t0
     t0 = time.perf_counter()
@@ -572,6 +576,7 @@ def run_xdg(args):
     line = {"metric": "xdg_dof_updates_per_s", "value": dofs / (ms * 1e-3), "unit": "DOF/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": "f64",
             "data": "synthetic", "config": {"workload": "xdg_poisson_128^3_k2_both_species_bulk+interface",
+                                            "rule_family": args.xdg_rule,
                                             "species_dofs": dofs, "rule_construction_s": t_rules,
                                             "surface_rule_construction_s": t_surface,
                                             "surface_cells": int(len(if_rules["cells"])),

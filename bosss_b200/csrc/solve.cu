@@ -28,13 +28,31 @@
 namespace bosss {
 
 // ------------------------------------------------------------------ colouring
+// Either a linear colouring, colour = (a_0 i + a_1 j + a_2 k) mod lin, or a product of per-
+// direction moduli, colour = (i mod m_0, j mod m_1, k mod m_2).
 struct Colouring {
     int m[3] = {1, 1, 1};
     int ncol = 1;
+    int lin = 0;              // > 0: linear colouring modulo lin
+    int a[3] = {0, 0, 0};
 };
 
+// Distance-2 colouring of the face-neighbour graph (no two cells of one colour share a cell
+// of N(j) u {j}, so one probe per colour and local column recovers every block): the linear
+// colouring (i + 2j + 3k) mod 7 in 3D, (i + 2j) mod 5 in 2D, whose 2D+1 colours give every
+// cell and its face neighbours distinct colours -- valid when no periodic wrap breaks it
+// (periodic directions with n a multiple of 2D+1); else per-direction moduli >= 3.
 static Colouring make_colouring(const GridConst& g) {
     Colouring c;
+    const int M = 2 * g.D + 1;
+    bool lin_ok = g.D >= 2;
+    for (int d = 0; d < g.D; ++d) lin_ok = lin_ok && (!g.periodic[d] || g.n[d] % M == 0);
+    if (lin_ok) {
+        c.lin = M;
+        c.ncol = M;
+        for (int d = 0; d < g.D; ++d) c.a[d] = d + 1;
+        return c;
+    }
     for (int d = 0; d < g.D; ++d) {
         const int n = g.n[d];
         if (!g.periodic[d]) {
@@ -52,28 +70,29 @@ static Colouring make_colouring(const GridConst& g) {
     return c;
 }
 
-__device__ __forceinline__ int cell_colour(const GridConst& g, long long j, int m0, int m1, int m2) {
+__device__ __forceinline__ int cell_colour(const GridConst& g, long long j, const Colouring& cl) {
     int ijk[3];
     cell_ijk(g, j, ijk);
-    int c = ijk[0] % m0;
-    if (g.D >= 2) c = c * m1 + ijk[1] % m1;
-    if (g.D >= 3) c = c * m2 + ijk[2] % m2;
+    if (cl.lin > 0) return (cl.a[0] * ijk[0] + cl.a[1] * ijk[1] + cl.a[2] * ijk[2]) % cl.lin;
+    int c = ijk[0] % cl.m[0];
+    if (g.D >= 2) c = c * cl.m[1] + ijk[1] % cl.m[1];
+    if (g.D >= 3) c = c * cl.m[2] + ijk[2] % cl.m[2];
     return c;
 }
 
 // probe: V[j*Nd + i] = 1 for cells of colour `col` and local column `i0`, else 0
-__global__ void k_probe(GridConst g, int m0, int m1, int m2, int col, int Nd, int i0, double* V) {
+__global__ void k_probe(GridConst g, Colouring cl, int col, int Nd, int i0, double* V) {
     const long long n = (long long)g.J * Nd;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const long long j = t / Nd;
         const int i = (int)(t - j * Nd);
-        V[t] = (i == i0 && cell_colour(g, j, m0, m1, m2) == col) ? 1.0 : 0.0;
+        V[t] = (i == i0 && cell_colour(g, j, cl) == col) ? 1.0 : 0.0;
     }
 }
 
 // scatter JV into column i0 of every block whose column cell has colour `col`
 // (blocks column-major: vals[b*br*bc + i0*br + r])
-__global__ void k_scatter(GridConst g, int m0, int m1, int m2, int col, int i0, int br, int bc,
+__global__ void k_scatter(GridConst g, Colouring cl, int col, int i0, int br, int bc,
                           const long long* __restrict__ rowptr, const int* __restrict__ colidx,
                           const double* __restrict__ JV, double* __restrict__ vals) {
     const long long nrows = (long long)g.J * br;
@@ -81,7 +100,7 @@ __global__ void k_scatter(GridConst g, int m0, int m1, int m2, int col, int i0, 
         const long long j = t / br;
         const int r = (int)(t - j * br);
         for (long long b = rowptr[j]; b < rowptr[j + 1]; ++b)
-            if (cell_colour(g, colidx[b], m0, m1, m2) == col) vals[b * (long long)br * bc + (long long)i0 * br + r] = JV[t];
+            if (cell_colour(g, colidx[b], cl) == col) vals[b * (long long)br * bc + (long long)i0 * br + r] = JV[t];
     }
 }
 
@@ -148,7 +167,7 @@ static int assemble(bosss_handle* h, const double* U_dev, double time, bosss_bsr
     const Colouring c = make_colouring(g);
     for (int col = 0; col < c.ncol && e == cudaSuccess; ++col)
         for (int i0 = 0; i0 < Nd && e == cudaSuccess; ++i0) {
-            k_probe<<<grid_of(h->ndom), 256, 0, s>>>(g, c.m[0], c.m[1], c.m[2], col, Nd, i0, V);
+            k_probe<<<grid_of(h->ndom), 256, 0, s>>>(g, c, col, Nd, i0, V);
             int rc = run_mode(h, MODE_JVP, 1.0, 0.0, U_dev, V, JV, time, s);
             if (rc) {
                 cudaFree(V);
@@ -156,7 +175,7 @@ static int assemble(bosss_handle* h, const double* U_dev, double time, bosss_bsr
                 bosss_b200_bsr_destroy(A);
                 return rc;
             }
-            k_scatter<<<grid_of(h->ncod), 256, 0, s>>>(g, c.m[0], c.m[1], c.m[2], col, i0, Nc, Nd,
+            k_scatter<<<grid_of(h->ncod), 256, 0, s>>>(g, c, col, i0, Nc, Nd,
                                                        (const long long*)A->d_rowptr, A->d_colidx, JV, A->d_vals);
             e = cudaGetLastError();
         }
@@ -279,11 +298,19 @@ static double norm2(const double* x, long long n, double* partials, cudaStream_t
 }
 
 // ------------------------------------------------------------------ per-instance batched solves
-// distance-1 colouring (face neighbours differ): per direction the smallest modulus m >= 2
-// with n mod m != 1 on periodic directions (so that cells n-1 and 0 differ too); m = 1 for a
-// single cell
+// distance-1 colouring (face neighbours differ): the parity (i + j + k) mod 2 when no periodic
+// direction has an odd cell count; else per direction the smallest modulus m >= 2 with
+// n mod m != 1 on periodic directions (so that cells n-1 and 0 differ too), 1 for one cell
 static Colouring make_colouring1(const GridConst& g) {
     Colouring c;
+    bool parity = true;
+    for (int d = 0; d < g.D; ++d) parity = parity && (!g.periodic[d] || g.n[d] % 2 == 0);
+    if (parity) {
+        c.lin = 2;
+        c.ncol = 2;
+        for (int d = 0; d < g.D; ++d) c.a[d] = 1;
+        return c;
+    }
     for (int d = 0; d < g.D; ++d) {
         const int n = g.n[d];
         int m = 1;
@@ -299,13 +326,13 @@ static Colouring make_colouring1(const GridConst& g) {
 
 // column i0 of the diagonal cell blocks of (I/dt + J) from the probe product JV (blocks
 // column-major; the probe covered the cells of colour `col`)
-__global__ void k_scatter_diag(GridConst g, int m0, int m1, int m2, int col, int nb, int i0, double idt,
+__global__ void k_scatter_diag(GridConst g, Colouring cl, int col, int nb, int i0, double idt,
                                const double* __restrict__ JV, double* __restrict__ blocks) {
     const long long n = (long long)g.J * nb;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const long long j = t / nb;
         const int r = (int)(t - j * nb);
-        if (cell_colour(g, j, m0, m1, m2) != col) continue;
+        if (cell_colour(g, j, cl) != col) continue;
         blocks[j * (long long)nb * nb + (long long)i0 * nb + r] = JV[t] + (r == i0 ? idt : 0.0);
     }
 }
@@ -676,10 +703,10 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
             const Colouring c = make_colouring1(g);
             for (int col = 0; col < c.ncol && !rc; ++col)
                 for (int i0 = 0; i0 < nb && !rc; ++i0) {
-                    k_probe<<<grid_of(n), 256, 0, s>>>(g, c.m[0], c.m[1], c.m[2], col, nb, i0, t64);
+                    k_probe<<<grid_of(n), 256, 0, s>>>(g, c, col, nb, i0, t64);
                     rc = run_mode(h, MODE_JVP, 1.0, 0.0, U, t64, y64, 0.0, s);
                     if (!rc)
-                        k_scatter_diag<<<grid_of(n), 256, 0, s>>>(g, c.m[0], c.m[1], c.m[2], col, nb, i0, idt, y64, blk);
+                        k_scatter_diag<<<grid_of(n), 256, 0, s>>>(g, c, col, nb, i0, idt, y64, blk);
                 }
             if (rc) break;
             if (transpose) k_transpose_blocks<<<grid_of((long long)g.J * nb * nb), 256, 0, s>>>(g.J, nb, blk);
