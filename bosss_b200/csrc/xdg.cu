@@ -1316,7 +1316,9 @@ static int upload_and_fit(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
                 num += (acc[m] - b) * (acc[m] - b);
                 den += b * b;
             }
-            X->fit_resid[s][r] = std::sqrt(num) / std::max(std::sqrt(den), 1e-300);
+            // relative to the moments, floored at 1e-10 of the reference measure: sliver parts
+            // whose subdivided moments vanish would otherwise divide by zero
+            X->fit_resid[s][r] = std::sqrt(num) / std::max(std::sqrt(den), 1e-10);
             X->fitted_deg[s][r] = it.p;
         }
     } else {
