@@ -473,7 +473,7 @@ __device__ __forceinline__ double bgrad(const double (&L)[3][K + 1], const doubl
 
 template <int K>
 __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const double* __restrict__ nodes,
-                           const double* __restrict__ weights, EvalArgs a) {
+                           const double* __restrict__ weights, EvalArgs a, double* __restrict__ item_out) {
     using Phys = PhysScalar<3, true>;
     constexpr int NP = np_of(3, K);
     const int r = blockIdx.x;
@@ -481,7 +481,6 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
     const CutItem it = items[r];
     const GridConst& g = a.g;
     __shared__ double cA[NP], cB[NP];
-    __shared__ double RA[NP], RB[NP];
     int ijk[3];
     cell_ijk(g, it.cell, ijk);
     long long other = -1;
@@ -489,8 +488,6 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
     for (int n = threadIdx.x; n < NP; n += blockDim.x) {
         cA[n] = a.U[it.cell * NP + n];
         cB[n] = (other >= 0) ? a.U[other * NP + n] : 0.0;
-        RA[n] = 0.0;
-        RB[n] = 0.0;
     }
     __syncthreads();
     double rA[NP], rB[NP];
@@ -595,15 +592,46 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
             }
         }
     }
+    // fixed-order reduction over the block (2 warps): warp shuffles, then the two warps' sums;
+    // the item's contributions go to its slot of item_out (own cell, then the face
+    // neighbour), which k_cut_gather adds into the cells in a fixed order -- no atomics, so
+    // the result is the same bits run to run
+    __shared__ double red[2][2][NP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     #pragma unroll
     for (int n = 0; n < NP; ++n) {
-        atomicAdd(&RA[n], rA[n]);
-        if (it.dim == 2 && other >= 0) atomicAdd(&RB[n], rB[n]);
+        double va = rA[n], vb = rB[n];
+        for (int o = 16; o > 0; o >>= 1) {
+            va += __shfl_down_sync(0xffffffffu, va, o);
+            vb += __shfl_down_sync(0xffffffffu, vb, o);
+        }
+        if (lane == 0) {
+            red[warp][0][n] = va;
+            red[warp][1][n] = vb;
+        }
     }
     __syncthreads();
+    const bool two = it.dim == 2 && other >= 0;
     for (int n = threadIdx.x; n < NP; n += blockDim.x) {
-        atomicAdd(&a.out[it.cell * NP + n], a.alpha * RA[n]);
-        if (it.dim == 2 && other >= 0) atomicAdd(&a.out[other * NP + n], a.alpha * RB[n]);
+        item_out[((long long)r * 2 + 0) * NP + n] = a.alpha * (red[0][0][n] + red[1][0][n]);
+        item_out[((long long)r * 2 + 1) * NP + n] = two ? a.alpha * (red[0][1][n] + red[1][1][n]) : 0.0;
+    }
+}
+
+// out[cell] += the cut items' contributions to the cell, in item order (cells of the gather
+// list: g_cell[i], sources g_src[g_off[i] .. g_off[i+1]) = item * 2 + side)
+template <int K>
+__global__ void k_cut_gather(long long ncells, const long long* __restrict__ g_off, const long long* __restrict__ g_cell,
+                             const long long* __restrict__ g_src, const double* __restrict__ item_out,
+                             double* __restrict__ out) {
+    constexpr int NP = np_of(3, K);
+    const long long n = ncells * NP;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long i = t / NP;
+        const int m = (int)(t - i * NP);
+        double acc = 0.0;
+        for (long long e = g_off[i]; e < g_off[i + 1]; ++e) acc += item_out[g_src[e] * NP + m];
+        out[g_cell[i] * NP + m] += acc;
     }
 }
 
@@ -685,15 +713,29 @@ __global__ void k_interface_eval(const long long* __restrict__ cells, const long
             rB[n] += w * (-flux * ph[n] + symB * gn[n]);
         }
     }
+    // fixed-order reduction over the block (2 warps of 32): the same bits run to run
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int n = 0; n < NP; ++n) {
-        atomicAdd(&RA[n], rA[n]);
-        atomicAdd(&RB[n], rB[n]);
+        double va = rA[n], vb = rB[n];
+        for (int o = 16; o > 0; o >>= 1) {
+            va += __shfl_down_sync(0xffffffffu, va, o);
+            vb += __shfl_down_sync(0xffffffffu, vb, o);
+        }
+        if (lane == 0 && warp == 1) {
+            RA[n] = va;
+            RB[n] = vb;
+        }
+        if (lane == 0 && warp == 0) {
+            rA[n] = va;
+            rB[n] = vb;
+        }
     }
     __syncthreads();
-    for (int n = threadIdx.x; n < NP; n += blockDim.x) {
-        outA[cell * NP + n] += f.alpha * RA[n];
-        outB[cell * NP + n] += f.alpha * RB[n];
-    }
+    if (threadIdx.x == 0)
+        for (int n = 0; n < NP; ++n) {
+            outA[cell * NP + n] += f.alpha * (rA[n] + RA[n]);
+            outB[cell * NP + n] += f.alpha * (rB[n] + RB[n]);
+        }
 }
 
 // Surface rule of the sphere |x - c| = R inside the box [lo, hi] (physical coordinates), by
@@ -816,6 +858,13 @@ struct bosss_xdg {
     std::vector<unsigned char> vol[2], face[2];
     std::vector<CutItem> items[2];
     CutItem* d_items[2] = {nullptr, nullptr};
+    // deterministic accumulation of the cut items: per-item outputs (item, side, NP) and the
+    // per-cell gather lists (cells, CSR offsets, sources item * 2 + side, in item order)
+    double* d_item_out[2] = {nullptr, nullptr};
+    long long* d_g_off[2] = {nullptr, nullptr};
+    long long* d_g_cell[2] = {nullptr, nullptr};
+    long long* d_g_src[2] = {nullptr, nullptr};
+    long long n_gcells[2] = {0, 0};
     double* d_nodes[2] = {nullptr, nullptr};
     double* d_weights[2] = {nullptr, nullptr};
     std::vector<double> nodes[2], weights[2];
@@ -1272,6 +1321,48 @@ static int upload_and_fit(bosss_xdg* X, int s, const bosss_xdg_opts& xo) {
     CUDA_TRY(cudaMalloc(&X->d_nodes[s], sizeof(double) * 3 * nn));
     CUDA_TRY(cudaMalloc(&X->d_weights[s], sizeof(double) * nn));
     CUDA_TRY(cudaMemcpy(X->d_items[s], items.data(), sizeof(CutItem) * n, cudaMemcpyHostToDevice));
+    {
+        // gather lists: every cell an item contributes to (its cell, and a cut face's neighbour)
+        const GridConst& g = X->h[s]->base.g;
+        std::vector<std::vector<long long>> src((size_t)g.J);
+        std::vector<long long> touched;
+        auto add = [&](long long cell, long long e) {
+            if (src[cell].empty()) touched.push_back(cell);
+            src[cell].push_back(e);
+        };
+        for (int r = 0; r < n; ++r) {
+            const CutItem& it = items[r];
+            add(it.cell, 2LL * r);
+            if (it.dim != 2) continue;
+            int ijk[3];
+            for (int d = 0; d < 3; ++d) ijk[d] = (int)((it.cell / g.stride[d]) % g.n[d]);
+            int i = ijk[it.dir] + (it.side ? 1 : -1);
+            if (i < 0 || i >= g.n[it.dir]) {
+                if (!g.periodic[it.dir]) continue;
+                i = (i + g.n[it.dir]) % g.n[it.dir];
+            }
+            long long other = 0;
+            for (int d = 0; d < 3; ++d) other += (long long)((d == it.dir) ? i : ijk[d]) * g.stride[d];
+            add(other, 2LL * r + 1);
+        }
+        std::sort(touched.begin(), touched.end());
+        std::vector<long long> off(1, 0), flat;
+        for (long long c : touched) {
+            flat.insert(flat.end(), src[c].begin(), src[c].end());
+            off.push_back((long long)flat.size());
+        }
+        const int NP = np_of(3, X->K);
+        X->n_gcells[s] = (long long)touched.size();
+        CUDA_TRY(cudaMalloc(&X->d_item_out[s], sizeof(double) * (size_t)n * 2 * NP));
+        CUDA_TRY(cudaMalloc(&X->d_g_off[s], sizeof(long long) * off.size()));
+        CUDA_TRY(cudaMalloc(&X->d_g_cell[s], sizeof(long long) * std::max<size_t>(touched.size(), 1)));
+        CUDA_TRY(cudaMalloc(&X->d_g_src[s], sizeof(long long) * std::max<size_t>(flat.size(), 1)));
+        CUDA_TRY(cudaMemcpy(X->d_g_off[s], off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice));
+        if (!touched.empty())
+            CUDA_TRY(cudaMemcpy(X->d_g_cell[s], touched.data(), sizeof(long long) * touched.size(), cudaMemcpyHostToDevice));
+        if (!flat.empty())
+            CUDA_TRY(cudaMemcpy(X->d_g_src[s], flat.data(), sizeof(long long) * flat.size(), cudaMemcpyHostToDevice));
+    }
     CUDA_TRY(cudaMemcpy(X->d_nodes[s], X->nodes[s].data(), sizeof(double) * 3 * nn, cudaMemcpyHostToDevice));
     double* d_mom = nullptr;
     int* d_deg = nullptr;
@@ -1633,6 +1724,10 @@ int bosss_b200_xdg_destroy(bosss_xdg* X) {
         cudaFree(X->d_vol[s]);
         cudaFree(X->d_face[s]);
         cudaFree(X->d_items[s]);
+        cudaFree(X->d_item_out[s]);
+        cudaFree(X->d_g_off[s]);
+        cudaFree(X->d_g_cell[s]);
+        cudaFree(X->d_g_src[s]);
         cudaFree(X->d_nodes[s]);
         cudaFree(X->d_weights[s]);
         bosss_b200_destroy(X->h[s]);
@@ -1758,10 +1853,19 @@ int bosss_b200_xdg_evaluate_device(bosss_xdg* X, int32_t species, double alpha, 
         a.alpha = alpha;
         a.time = time;
         switch (X->K) {
-            case 1: k_cut_eval<1><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a); break;
-            case 2: k_cut_eval<2><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a); break;
-            case 3: k_cut_eval<3><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a); break;
-            default: k_cut_eval<4><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a); break;
+            case 1: k_cut_eval<1><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a, X->d_item_out[s]); break;
+            case 2: k_cut_eval<2><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a, X->d_item_out[s]); break;
+            case 3: k_cut_eval<3><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a, X->d_item_out[s]); break;
+            default: k_cut_eval<4><<<n, 64, 0, st>>>(X->d_items[s], n, X->d_nodes[s], X->d_weights[s], a, X->d_item_out[s]); break;
+        }
+        CUDA_TRY(cudaGetLastError());
+        const long long nc = X->n_gcells[s], NPc = np_of(3, X->K);
+        const int gg = (int)std::max<long long>(1, std::min<long long>((nc * NPc + 255) / 256, 148LL * 16));
+        switch (X->K) {
+            case 1: k_cut_gather<1><<<gg, 256, 0, st>>>(nc, X->d_g_off[s], X->d_g_cell[s], X->d_g_src[s], X->d_item_out[s], out_dev); break;
+            case 2: k_cut_gather<2><<<gg, 256, 0, st>>>(nc, X->d_g_off[s], X->d_g_cell[s], X->d_g_src[s], X->d_item_out[s], out_dev); break;
+            case 3: k_cut_gather<3><<<gg, 256, 0, st>>>(nc, X->d_g_off[s], X->d_g_cell[s], X->d_g_src[s], X->d_item_out[s], out_dev); break;
+            default: k_cut_gather<4><<<gg, 256, 0, st>>>(nc, X->d_g_off[s], X->d_g_cell[s], X->d_g_src[s], X->d_item_out[s], out_dev); break;
         }
         CUDA_TRY(cudaGetLastError());
     }

@@ -119,6 +119,25 @@ def test_xdg_masked_slab_equals_masked_generic():
             assert rel(a, b) <= 1e-13, (s, rel(a, b))
 
 
+def test_xdg_evaluation_is_bitwise_reproducible(xdg_small):
+    """Cut items reduce in a fixed order (no atomics), so repeated evaluations give the same
+    bits, bulk and interface term."""
+    import torch
+    opA, opB, g, c, UA, UB, X = xdg_small
+    X.SetInterface(1.0, 10.0, 4.0, X.SIP, 6)
+    outs = []
+    for _ in range(3):
+        a, b = torch.zeros(UA.size, dtype=torch.float64, device="cuda"), torch.zeros(UB.size, dtype=torch.float64, device="cuda")
+        uA, uB = torch.from_numpy(UA).cuda(), torch.from_numpy(UB).cuda()
+        X.Evaluate(0, 1.0, 0.0, a, uA)
+        X.Evaluate(1, 1.0, 0.0, b, uB)
+        X.EvaluateInterface(1.0, uA, uB, a, b)
+        torch.cuda.synchronize()
+        outs.append((a.cpu(), b.cpu()))
+    for a, b in outs[1:]:
+        assert torch.equal(a, outs[0][0]) and torch.equal(b, outs[0][1])
+
+
 def test_saye_rules_evaluate_and_volume():
     """Saye-type rules (rule family 1, 8 Gauss nodes per direction and piece): the species-A
     rules plus the full cells give the ball volume to 1e-9 (the moment-fitted family: 1e-4,
