@@ -135,6 +135,7 @@ class XdgOpts(ctypes.Structure):
                 ("reserved", ctypes.c_int32 * 7)]
 
 
+BOUNDARY_PRESCRIBED, BOUNDARY_OUTLET, BOUNDARY_SLIP_WALL = 0, 1, 2
 XDG_RULE_MOMENT_FITTING = 0
 XDG_RULE_SAYE = 1
 
@@ -167,6 +168,7 @@ SIGNATURES = {
     "bosss_b200_destroy": (ctypes.c_int, [_P]),
     "bosss_b200_get_sizes": (ctypes.c_int, [_P, _I64, _I64, _I32]),
     "bosss_b200_kernel_info": (ctypes.c_int, [_P, ctypes.c_int32, _I32, _I32]),
+    "bosss_b200_set_boundary_kinds": (ctypes.c_int, [_P, _P]),
     "bosss_b200_saye_rule": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, ctypes.c_int32, _I64, _P, _P]),
     "bosss_b200_batch_solve": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, _P, ctypes.POINTER(SolverOpts), _P]),
     "bosss_b200_pmg_create": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_void_p)]),

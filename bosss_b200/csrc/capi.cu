@@ -318,7 +318,7 @@ __global__ void nan_scan_kernel(const double* x, long long n, int* flag) {
 // A face-once handle (3D Euler) evaluates residual and VJP as the slab kernel's volume pass
 // (or the tensor-core volume kernel) followed by the face kernels of faces_euler.cu.
 static int launch_eval(bosss_handle* h, int mode, EvalArgs a, cudaStream_t s) {
-    if (h->n_bnd_nodes > 0 && !a.bnd_state)
+    if (h->n_bnd_nodes > 0 && !a.bnd_state && h->bnd_table_needed)
         return fail(BOSSS_ERR_BAD_ARG, "the operator's boundary terms need the boundary-state table "
                                        "(bosss_b200_set_boundary_state)");
     const bool split = mode == MODE_RES && h->precision == BOSSS_PRECISION_SPLIT_FP32;
@@ -642,6 +642,7 @@ int bosss_b200_destroy(bosss_handle* h) {
     if (h->stream) cudaStreamDestroy(h->stream);
     cudaFree(h->d_bnd_off);
     cudaFree(h->d_bnd_state);
+    cudaFree(h->d_bnd_kind);
     cudaFree(h->dFace);
     tc_volume_destroy(h);
     delete h;
@@ -693,6 +694,26 @@ int bosss_b200_set_boundary_state(bosss_handle* h, const double* state) {
     CUDA_TRY(cudaMemcpy(h->d_bnd_state, state, sizeof(double) * n, cudaMemcpyHostToDevice));
     h->base.bnd_off = h->d_bnd_off;
     h->base.bnd_state = h->d_bnd_state;
+    return BOSSS_OK;
+}
+
+int bosss_b200_set_boundary_kinds(bosss_handle* h, const int32_t* kinds) {
+    if (!h || !kinds) return fail(BOSSS_ERR_BAD_ARG, "null argument");
+    if (h->n_bnd_nodes == 0) return fail(BOSSS_ERR_BAD_ARG, "the operator takes no boundary-state table");
+    bool any0 = false;
+    for (int64_t i = 0; i < h->n_bnd_nodes; ++i) {
+        if (kinds[i] < 0 || kinds[i] > 2) return fail(BOSSS_ERR_BAD_ARG, "boundary kind: 0, 1 or 2");
+        if (kinds[i] != 0 && h->phys != PHYS_EULER)
+            return fail(BOSSS_ERR_BAD_ARG, "boundary kinds 1 and 2 (outlet, slip wall): HLLC fluxes only");
+        any0 = any0 || kinds[i] == 0;
+    }
+    CUDA_TRY(cudaSetDevice(h->device));
+    if (!h->d_bnd_kind) CUDA_TRY(cudaMalloc(&h->d_bnd_kind, sizeof(int) * (size_t)h->n_bnd_nodes));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    CUDA_TRY(cudaMemcpy(h->d_bnd_kind, kinds, sizeof(int) * (size_t)h->n_bnd_nodes, cudaMemcpyHostToDevice));
+    h->base.bnd_off = h->d_bnd_off;
+    h->base.bnd_kind = h->d_bnd_kind;
+    h->bnd_table_needed = any0;
     return BOSSS_OK;
 }
 

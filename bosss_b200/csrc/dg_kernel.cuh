@@ -66,6 +66,10 @@ struct EvalArgs {
     // terms take a prescribed outer state (CNS viscous terms)
     const long long* bnd_off;
     const double* bnd_state;
+    // optional boundary-condition kind per boundary face node (same numbering; null: all 0):
+    // 0 the table's outer state, 1 the inner state (supersonic outlet), 2 the inner state with
+    // its normal momentum reflected (adiabatic slip wall); kinds 1 and 2: HLLC fluxes only
+    const int* bnd_kind;
 };
 
 template <class Phys, int K, int Q, int MODE>
@@ -715,9 +719,13 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
                 pnlty = Phys::BND_PEN * args.ph.pen * penalty_size(args.cell_pf, g, ijk);
             }
             const double* ub = nullptr;   // outer state of the boundary-state table at this node
-            if (!inner && args.bnd_state) {
+            int bkind = 0;                // boundary-condition kind of the node
+            if (!inner && args.bnd_off) {
                 const long long o = args.bnd_off[(c0 + cl) * (2 * D) + 2 * d + s];
-                if (o >= 0) ub = args.bnd_state + (o + qf) * NV;
+                if (o >= 0) {
+                    if (args.bnd_state) ub = args.bnd_state + (o + qf) * NV;
+                    if (args.bnd_kind) bkind = args.bnd_kind[o + qf];
+                }
             }
             const bool selfA = !inner || s == 1;   // own cell is IN (lower) unless it is the upper cell
             const double* trOwn = TR(cl) + ((s * 2 + 0) * NFI) * NCI * QF;
@@ -746,7 +754,7 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
                     for (int dd = 0; dd < D; ++dd) GAv[e][dd] = GBv[e][dd] = 0.0;
                 }
                 if (inner) Phys::inner(args.ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, ub, gA, GAv);
+                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, ub, bkind, gA, GAv);
 #pragma unroll
                 for (int e = 0; e < NC; ++e) {
                     const double gv = selfA ? gA[e] : gB[e];
@@ -774,7 +782,7 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
                     }
                 }
                 if (inner) Phys::inner(args.ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, ub, gA, GAv);
+                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, ub, bkind, gA, GAv);
 #pragma unroll
                 for (int e = 0; e < NC; ++e) {
                     const double gv = selfA ? gA[e].d[0] : gB[e].d[0];
@@ -805,7 +813,7 @@ __device__ __forceinline__ void cell_tile(const EvalArgs& args, long long c0, do
                         for (int dd = 0; dd < D; ++dd) (selfA ? GA : GB)[i][dd].d[i * (1 + D) + 1 + dd] = 1.0;
                 }
                 if (inner) Phys::inner(args.ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, ub, gA, GAv);
+                else Phys::boundary(args.ph, pnlty, UA, GA, nrm, x, ub, bkind, gA, GAv);
                 T phi(0.0);
 #pragma unroll
                 for (int e = 0; e < NC; ++e) {

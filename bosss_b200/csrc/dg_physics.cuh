@@ -105,11 +105,14 @@ struct PhysScalar {
         }
     }
 
-    // ub: the boundary-state table's outer values at this node (null without a table; unused here)
+    // ub: the boundary-state table's outer values at this node (null without a table; unused here);
+    // kind: the node's boundary-condition kind (0 here: create() rejects other kinds)
     template <class T>
     __device__ static void boundary(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
-                                    const double* n, const double* x, const double* ub, T* gA, T (*GAv)[D]) {
+                                    const double* n, const double* x, const double* ub, int kind, T* gA,
+                                    T (*GAv)[D]) {
         (void)ub;
+        (void)kind;
         if (p.has_transport) {
             double an = 0.0;
 #pragma unroll
@@ -266,9 +269,10 @@ struct PhysCNSVisc {
 
     template <class T>
     __host__ __device__ static void boundary(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
-                                             const double* n, const double* x, const double* ub, T* gA,
+                                             const double* n, const double* x, const double* ub, int kind, T* gA,
                                              T (*GAv)[D]) {
         (void)x;
+        (void)kind;   // prescribed states only (set_boundary_kinds rejects other kinds for this operator)
         if (!ub) return;   // create() requires the boundary-state table when the grid has boundary faces
         T Uo[NV], J[NV][D];
 #pragma unroll
@@ -421,17 +425,26 @@ struct PhysEuler {
 
     template <class T>
     __host__ __device__ static void boundary(const PhysParams& p, double pnlty, const T* UA, const T (*GA)[D],
-                                             const double* n, const double* x, const double* ub, T* gA,
+                                             const double* n, const double* x, const double* ub, int kind, T* gA,
                                              T (*GAv)[D]) {
         // OptimizedHLLCFlux.BorderEdgeFlux (OptimizedHLLCFlux.cs:61-131): the outer state of the
-        // boundary condition (here the boundary-state table's value at this node, a constant of
-        // the linearisation), then the inner-edge HLLC flux with the outward normal
+        // boundary condition, then the inner-edge HLLC flux with the outward normal. Outer state:
+        // kind 0 the boundary-state table's value (a constant of the linearisation), kind 1 the
+        // inner state (SupersonicOutlet.GetBoundaryState), kind 2 the inner state with the
+        // normal momentum reflected, m - 2 (m . n) n (AdiabaticSlipWall.GetBoundaryState without
+        // wall velocities)
         (void)GA;
-        if (!ub) return;   // create() requires the boundary-state table on non-periodic grids
+        if (kind == 0 && !ub) return;   // the entry points require the table for kind-0 nodes
         T Uo[NV], GB[NV][D], gB[NC], GBv[NC][D];
+        T mn = T(0.0);
+        if (kind == 2)
+#pragma unroll
+            for (int d = 0; d < D; ++d) mn += UA[1 + d] * n[d];
 #pragma unroll
         for (int i = 0; i < NV; ++i) {
-            Uo[i] = T(ub[i]);
+            if (kind == 0) Uo[i] = T(ub[i]);
+            else if (kind == 2 && i >= 1 && i <= D) Uo[i] = UA[i] - 2.0 * mn * n[i - 1];
+            else Uo[i] = UA[i];
 #pragma unroll
             for (int d = 0; d < D; ++d) GB[i][d] = T(0.0);
         }

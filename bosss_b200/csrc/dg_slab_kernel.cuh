@@ -240,7 +240,7 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
             for (int d = 0; d < D; ++d) GAv[e][d] = GBv[e][d] = 0.0;
         }
         if (inner) Phys::inner(ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, nullptr, gA, GAv);
+        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, nullptr, 0, gA, GAv);
 #pragma unroll
         for (int e = 0; e < NC; ++e) {
             if (OV) out(e, 0, (selfA ? gA[e] : gB[e]) * fac);
@@ -266,7 +266,7 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
             }
         }
         if (inner) Phys::inner(ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, nullptr, gA, GAv);
+        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, nullptr, 0, gA, GAv);
 #pragma unroll
         for (int e = 0; e < NC; ++e) {
             if (OV) out(e, 0, (selfA ? gA[e].d[0] : gB[e].d[0]) * fac);
@@ -313,7 +313,7 @@ __device__ __forceinline__ void face_point(const PhysParams& ph, bool inner, boo
                 for (int d = 0; d < D; ++d) (selfA ? GA[i][d] : GB[i][d]).d[i * (1 + D) + 1 + d] = 1.0;
         }
         if (inner) Phys::inner(ph, pnlty, UA, GA, UB, GB, nrm, x, gA, GAv, gB, GBv);
-        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, nullptr, gA, GAv);
+        else Phys::boundary(ph, pnlty, UA, GA, nrm, x, nullptr, 0, gA, GAv);
         T phi(0.0);
 #pragma unroll
         for (int e = 0; e < NC; ++e) {

@@ -21,6 +21,8 @@ struct bosss_handle {
     int64_t n_bnd_nodes = 0;
     long long* d_bnd_off = nullptr;
     double* d_bnd_state = nullptr;
+    int* d_bnd_kind = nullptr;          // boundary-condition kinds (null: all prescribed states)
+    bool bnd_table_needed = true;       // some node takes the table's state (kind 0)
     // face-once path (3D Euler residual and VJP): enabled flag and the face buffer
     bool faces_once = false;
     double* dFace = nullptr;

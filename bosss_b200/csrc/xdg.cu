@@ -582,7 +582,7 @@ __global__ void k_cut_eval(const CutItem* __restrict__ items, int nitems, const 
                 nrm[it.dir] = it.side ? 1.0 : -1.0;
                 const double pnlty = 2.0 * a.ph.pen * penalty_size(a.cell_pf, g, ijk);
                 double U1[1] = {uA}, gi[1] = {0.0}, Gi[1][3] = {{0, 0, 0}};
-                Phys::boundary(a.ph, pnlty, U1, GA, nrm, x, nullptr, gi, Gi);
+                Phys::boundary(a.ph, pnlty, U1, GA, nrm, x, nullptr, 0, gi, Gi);
                 #pragma unroll
                 for (int n = 0; n < NP; ++n) {
                     double acc = gi[0] * bphi<K>(LA, n);

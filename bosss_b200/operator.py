@@ -581,6 +581,13 @@ class Evaluator:
         a = np.ascontiguousarray(state, dtype=np.float64)
         C.check(C.lib().bosss_b200_set_boundary_state(self.handle, C.ptr(a)))
 
+    def SetBoundaryKinds(self, kinds):
+        """Boundary-condition kind per boundary face node (HLLC): 0 prescribed state from the
+        table, 1 supersonic outlet (inner state), 2 adiabatic slip wall (normal momentum
+        reflected)."""
+        a = np.ascontiguousarray(kinds, dtype=np.int32)
+        C.check(C.lib().bosss_b200_set_boundary_kinds(self.handle, C.ptr(a)))
+
     def residual_vjp(self, U, W, R=None, G=None, alpha=1.0, beta=0.0):
         """Host arrays: ``R = beta*R + alpha*Op(U)`` and ``G = J(U)^T W`` in one pipelined call
         (U and W cross PCIe once). Returns (R, G)."""

@@ -78,8 +78,9 @@ enum bosss_component_type {
      * outer state from the boundary-state table (bosss_b200_set_boundary_state) and evaluate
      * the inner-edge HLLC flux with it, as OptimizedHLLCFlux.BorderEdgeFlux
      * (OptimizedHLLCFlux.cs:61-131) does with the state of its boundary-condition map; the
-     * table holds prescribed states (inflow / far field), not state-dependent conditions
-     * (walls, extrapolated outflow). Such grids run on the generic kernel. */
+     * table holds prescribed states (inflow / far field), bosss_b200_set_boundary_kinds marks
+     * supersonic-outlet and adiabatic-slip-wall nodes, whose outer states follow the inner one.
+     * Such grids run on the generic kernel. */
     BOSSS_COMP_HLLC_DENSITY_FLUX = 10,
     BOSSS_COMP_HLLC_MOMENTUM_FLUX = 11,
     BOSSS_COMP_HLLC_ENERGY_FLUX = 12,
@@ -224,6 +225,13 @@ int bosss_b200_evaluate_device(bosss_handle* h, double alpha, double beta, const
  * fail with BOSSS_ERR_BAD_ARG until the table is set. */
 int bosss_b200_boundary_nodes(const bosss_handle* h, int64_t* n_nodes, double* xyz);
 int bosss_b200_set_boundary_state(bosss_handle* h, const double* state);
+/* Boundary-condition kind of every boundary face node (same numbering), for the HLLC fluxes:
+ * 0 the table's outer state (SupersonicInlet and other prescribed states; the default), 1 the
+ * inner state (SupersonicOutlet.GetBoundaryState), 2 the inner state with the normal momentum
+ * reflected, m - 2 (m . n) n (AdiabaticSlipWall.GetBoundaryState without wall velocities).
+ * Kinds 1 and 2 depend on the state, so they enter the JVP and VJP. Other operators accept
+ * kind 0 only. When no node has kind 0 the boundary-state table is not needed. */
+int bosss_b200_set_boundary_kinds(bosss_handle* h, const int32_t* kinds);
 
 /* Directional derivative J(U)*V of the nonlinear operator; replaces the FD `dirder`
  * of the matrix-free Newton-GMRES (Newton.cs:1450-1495). Host buffers. */

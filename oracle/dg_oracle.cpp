@@ -355,6 +355,10 @@ struct Problem {
     // face direction d, then side s (0 lower, 1 upper), then face node q; bnd_off[j*2D + 2d + s]
     // is the first node of that boundary face (-1: interior face).
     const double* bnd = nullptr;
+    // boundary-condition kind per boundary face node (null: all 0): 0 the table's state, 1 the
+    // inner state (SupersonicOutlet), 2 the inner state with the normal momentum reflected
+    // (AdiabaticSlipWall); kinds 1 and 2 for the HLLC fluxes
+    const int* kinds = nullptr;
     std::vector<long long> bnd_off;
     long long n_bnd_nodes = 0;
 };
@@ -909,8 +913,8 @@ static void inner_edge_terms(const Problem& P, const bosss_component& cp, int jI
 // the problem has no table).
 template <class T>
 static void boundary_edge_terms(const Problem& P, const bosss_component& cp, int jIn, const T* UA,
-                                const T (*GA)[3], const double* n, const double* x, const double* Ubnd, T& gA,
-                                T* GAv) {
+                                const T (*GA)[3], const double* n, const double* x, const double* Ubnd, int kind,
+                                T& gA, T* GAv) {
     const int D = P.D;
     switch (cp.type) {
         case BOSSS_COMP_SCALAR_TRANSPORT_FLUX: {
@@ -972,15 +976,20 @@ static void boundary_edge_terms(const Problem& P, const bosss_component& cp, int
         case BOSSS_COMP_HLLC_MOMENTUM_FLUX:
         case BOSSS_COMP_HLLC_ENERGY_FLUX: {
             // OptimizedHLLCFlux.BorderEdgeFlux (OptimizedHLLCFlux.cs:61-131): Uout from the
-            // boundary condition (the table's state), then InnerEdgeFlux(Uin, Uout) with the
-            // outward normal; only the IN side is kept
-            if (!Ubnd) break;   // rejected by the entry points
+            // boundary condition, then InnerEdgeFlux(Uin, Uout) with the outward normal; only the
+            // IN side is kept. Uout: the table's state (kind 0), Uin (SupersonicOutlet.cs, kind 1),
+            // Uin with m - 2 (m . n) n (AdiabaticSlipWall.cs, kind 2)
+            if (kind == 0 && !Ubnd) break;   // rejected by the entry points
             T Ub[BOSSS_MAX_VARS];
             T GB[BOSSS_MAX_VARS][3];
+            T mn = T(0.0);
+            for (int d = 0; d < D; ++d) mn += UA[cp.args[1 + d]] * T(n[d]);
             for (int f = 0; f < P.op.n_domain; ++f) {
-                Ub[f] = T(Ubnd[f]);
+                Ub[f] = (kind == 0) ? T(Ubnd[f]) : UA[f];
                 for (int d = 0; d < 3; ++d) GB[f][d] = T(0.0);
             }
+            if (kind == 2)
+                for (int d = 0; d < D; ++d) Ub[cp.args[1 + d]] = UA[cp.args[1 + d]] - T(2.0) * mn * T(n[d]);
             T gB = T(0.0), GBv[3] = {T(0.0), T(0.0), T(0.0)};
             inner_edge_terms(P, cp, jIn, jIn, UA, GA, (const T*)Ub, (const T(*)[3])GB, n, gA, GAv, gB, GBv);
             (void)x;
@@ -996,6 +1005,13 @@ static const double* bnd_node(const Problem& P, int j, int d, int s, int q) {
     if (!P.bnd) return nullptr;
     const long long o = P.bnd_off[(size_t)j * 2 * P.D + 2 * d + s];
     return o < 0 ? nullptr : P.bnd + (size_t)(o + q) * P.op.n_domain;
+}
+
+// boundary-condition kind at node q of boundary face (j, d, s)
+static int bnd_kind(const Problem& P, int j, int d, int s, int q) {
+    if (!P.kinds) return 0;
+    const long long o = P.bnd_off[(size_t)j * 2 * P.D + 2 * d + s];
+    return o < 0 ? 0 : P.kinds[o + q];
 }
 
 // vflags / fflags (nullable): XDG species masks -- a cell's volume integral is taken only where
@@ -1110,7 +1126,8 @@ static void evaluate(const Problem& P, double alpha, double beta, const T* U, T*
                     const auto& cp = P.op.components[ci];
                     if (cp.codomain != e) continue;
                     if (ed.out >= 0) inner_edge_terms(P, cp, ed.in, ed.out, UA, GA, UB, GB, nrm, gA, GAv, gB, GBv);
-                    else boundary_edge_terms(P, cp, ed.in, UA, GA, nrm, x, bnd_node(P, ed.in, d, fIn % 2, q), gA, GAv);
+                    else boundary_edge_terms(P, cp, ed.in, UA, GA, nrm, x, bnd_node(P, ed.in, d, fIn % 2, q),
+                                             bnd_kind(P, ed.in, d, fIn % 2, q), gA, GAv);
                 }
                 int k = P.op.codomain_degree[e], Np = P.cod_np[e];
                 const double* ip = &P.fphi[k][((size_t)fIn * Qf + q) * Np];
@@ -1265,7 +1282,8 @@ static void vjp(const Problem& P, const double* U, const double* W, double* out)
                     const auto& cp = P.op.components[ci];
                     if (cp.codomain != e) continue;
                     if (ed.out >= 0) inner_edge_terms(P, cp, ed.in, ed.out, UA, GA, UB, GB, nrm, gA, GAv, gB, GBv);
-                    else boundary_edge_terms(P, cp, ed.in, UA, GA, nrm, x, bnd_node(P, ed.in, d, fIn % 2, q), gA, GAv);
+                    else boundary_edge_terms(P, cp, ed.in, UA, GA, nrm, x, bnd_node(P, ed.in, d, fIn % 2, q),
+                                             bnd_kind(P, ed.in, d, fIn % 2, q), gA, GAv);
                 }
                 int k = P.op.codomain_degree[e], Np = P.cod_np[e];
                 for (int side = 0; side < 2; ++side) {
@@ -1401,7 +1419,7 @@ static void face_integral(const Problem& P, int jin, int jout, int d, double sgn
                 const auto& cp = P.op.components[ci];
                 if (cp.codomain != e) continue;
                 if (jout >= 0) inner_edge_terms<double>(P, cp, jin, jout, UA, GA, UB, GB, nrm, gA, GAv, gB, GBv);
-                else boundary_edge_terms<double>(P, cp, jin, UA, GA, nrm, x, nullptr, gA, GAv);
+                else boundary_edge_terms<double>(P, cp, jin, UA, GA, nrm, x, nullptr, 0, gA, GAv);
             }
             int k = P.op.codomain_degree[e], Np = P.cod_np[e];
             for (int m = 0; m < Np; ++m) {
@@ -1541,11 +1559,19 @@ int orc_basis_eval(int D, int k, int npts, const double* pts, double* phi, doubl
 }
 
 // setup plus the boundary-state table (bnd may be null unless a component needs it)
+static thread_local const int* g_kinds = nullptr;   // set by orc_set_boundary_kinds
+
 static int setup_bnd(Problem& P, const bosss_op_desc* op, const bosss_grid_desc* g, const double* bnd) {
     g_err = setup(P, op, g);
     if (!g_err.empty()) return BOSSS_ERR_BAD_ARG;
     P.bnd = bnd;
-    if (!bnd && P.n_bnd_nodes > 0)
+    P.kinds = g_kinds;
+    bool need_table = true;
+    if (g_kinds) {
+        need_table = false;
+        for (long long i = 0; i < P.n_bnd_nodes; ++i) need_table = need_table || g_kinds[i] == 0;
+    }
+    if (!bnd && P.n_bnd_nodes > 0 && need_table)
         for (int c = 0; c < op->n_components; ++c)
             if (op->components[c].type == ORC_COMP_CNS_SIPG_MOMENTUM || op->components[c].type == ORC_COMP_CNS_SIPG_ENERGY ||
                 op->components[c].type == BOSSS_COMP_HLLC_DENSITY_FLUX ||
@@ -1554,6 +1580,13 @@ static int setup_bnd(Problem& P, const bosss_op_desc* op, const bosss_grid_desc*
                 g_err = "CNS SIPG and HLLC on a grid with boundary faces need the boundary-state table";
                 return BOSSS_ERR_BAD_ARG;
             }
+    return 0;
+}
+
+// boundary-condition kinds of the boundary face nodes for the following calls (null: all 0;
+// the array must stay alive until the next call)
+int orc_set_boundary_kinds(const int* kinds) {
+    g_kinds = kinds;
     return 0;
 }
 

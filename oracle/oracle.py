@@ -32,6 +32,7 @@ def lib():
         L.orc_vjp.argtypes = [P, P, P, P, P, P]
         L.orc_jacobian_blocks.argtypes = [P, P, P, P, P, P]
         L.orc_boundary_nodes.argtypes = [P, P, P]
+        L.orc_set_boundary_kinds.argtypes = [P]
         L.orc_bsr_spmv.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, P, P, P, ctypes.c_double, P,
                                    ctypes.c_double, P]
         L.orc_sizes.argtypes = [P, P, P, P, P]
@@ -76,6 +77,21 @@ def _bnd(opd, gd, bnd):
     b = np.ascontiguousarray(bnd, dtype=np.float64)
     assert b.shape == (n_boundary_nodes(opd, gd), opd.n_domain), b.shape
     return b, _p(b)
+
+
+class boundary_kinds:
+    """Context: boundary-condition kinds (0 table state, 1 outlet, 2 slip wall) per boundary
+    face node for the oracle calls inside the block."""
+
+    def __init__(self, kinds):
+        self.kinds = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
+
+    def __enter__(self):
+        lib().orc_set_boundary_kinds(None if self.kinds is None else _p(self.kinds))
+        return self
+
+    def __exit__(self, *a):
+        lib().orc_set_boundary_kinds(None)
 
 
 def n_boundary_nodes(opd, gd):

@@ -84,3 +84,43 @@ def test_bounded_euler_needs_table_and_generic_kernel():
         with pytest.raises(C.BosssError) as ei:
             pr3.evaluator(kernel=kern)
         assert ei.value.code == C.ERR_BAD_ARG
+
+
+@pytest.mark.parametrize("name,make", CASES[:3], ids=[c[0] for c in CASES[:3]])
+def test_boundary_kinds_match_oracle(name, make):
+    """Outlet (inner state) and slip-wall (normal momentum reflected) nodes mixed with
+    prescribed ones: residual, JVP and VJP against the oracle."""
+    import test_oracle_euler_boundary as TB
+    pr = make()
+    opd, gd = pr.descs()
+    r = np.random.default_rng(11)
+    V = r.uniform(-1, 1, pr.n_dofs)
+    W = r.uniform(-1, 1, pr.n_dofs)
+    nq = orc.sizes(opd, gd)[2]
+    kinds = TB.boundary_kinds_by_face(gd, nq, lambda d, s: (d + s) % 3)
+    with pr.evaluator() as ev:
+        bnd = P.euler_boundary_states(ev.boundary_nodes())
+        ev.SetBoundaryState(bnd)
+        ev.SetBoundaryKinds(kinds)
+        R = np.zeros(pr.n_dofs)
+        ev.Evaluate(1.0, 0.0, R, pr.U)
+        JV = ev.jvp(pr.U, V)
+        G = ev.vjp(pr.U, W)
+    with orc.boundary_kinds(kinds):
+        assert rel(R, orc.evaluate(opd, gd, pr.U, bnd=bnd)) <= TOL
+        assert rel(JV, orc.jvp(opd, gd, pr.U, V, bnd=bnd)) <= TOL
+        assert rel(G, orc.vjp(opd, gd, pr.U, W, bnd=bnd)) <= TOL
+
+
+def test_walls_and_outlets_need_no_table():
+    pr = P.euler2d(n=4, k=1, seed=88, periodic=(False, False))
+    opd, gd = pr.descs()
+    with pr.evaluator() as ev:
+        n = len(ev.boundary_nodes())
+        ev.SetBoundaryKinds(np.full(n, 2, dtype=np.int32))
+        R = np.zeros(pr.n_dofs)
+        ev.Evaluate(1.0, 0.0, R, pr.U)
+        with pytest.raises(C.BosssError):
+            ev.SetBoundaryKinds(np.full(n, 3, dtype=np.int32))
+    with orc.boundary_kinds(np.full(n, 2, dtype=np.int32)):
+        assert rel(R, orc.evaluate(opd, gd, pr.U)) <= TOL
