@@ -512,7 +512,8 @@ int bosss_b200_create(const bosss_op_desc* op, const bosss_grid_desc* grid, cons
     }
     h->base.cbeg = 0;
     h->base.cend = J;
-    if (grid->cell_order == BOSSS_CELLS_GLOBALID) {
+    // 2D: GlobalID = ix*nY + iy (Grid2D.cs:182) is the generator order
+    if (grid->cell_order == BOSSS_CELLS_GLOBALID && D == 3) {
         g.stride[0] = 1;
         g.stride[1] = g.n[0];
         g.stride[2] = (long long)g.n[0] * g.n[1];

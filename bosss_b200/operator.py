@@ -95,11 +95,20 @@ class CartesianGrid:
         """(J, dim) integer cell indices in local order."""
         J = self.NoOfCells
         j = np.arange(J)
-        if self.cell_order == C.CELLS_GENERATOR:
+        if self.cell_order == C.CELLS_GENERATOR or self.dim == 2:
+            # generator order; in 2D also the GlobalID order (Grid2D.cs:182)
             idx = np.unravel_index(j, self.n)                 # x slowest
         else:
             idx = np.unravel_index(j, self.n[::-1])[::-1]     # x fastest
         return np.stack(idx, axis=1)
+
+    def global_ids(self):
+        """(J,) GlobalID of every cell in local order: ``ix + iy*nX + iz*nX*nY`` in 3D
+        (``Grid3D.cs:248``), ``ix*nY + iy`` in 2D (``Grid2D.cs:182``)."""
+        ijk = self.cell_ijk().astype(np.int64)
+        if self.dim == 2:
+            return ijk[:, 0] * self.n[1] + ijk[:, 1]
+        return ijk[:, 0] + self.n[0] * (ijk[:, 1] + self.n[1] * ijk[:, 2])
 
 
 def Cartesian2DGrid(xNodes, yNodes, periodicX=False, periodicY=False, cell_order=C.CELLS_GENERATOR):

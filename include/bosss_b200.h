@@ -130,7 +130,8 @@ enum bosss_cell_order {
     /* the generator's local order on one process: x slowest, last axis fastest
      * (Grid3D.cs:232-249: j = (ix*nY + iy)*nZ + iz; Grid2D: j = ix*nY + iy) */
     BOSSS_CELLS_GENERATOR = 0,
-    /* GlobalID order: x fastest (GlobalID = ix + iy*nX + iz*nX*nY) */
+    /* GlobalID order: 3D x fastest (GlobalID = ix + iy*nX + iz*nX*nY, Grid3D.cs:248);
+     * 2D GlobalID = ix*nY + iy (Grid2D.cs:182), the same as the generator order */
     BOSSS_CELLS_GLOBALID = 1
 };
 

@@ -370,26 +370,26 @@ static int np_of(int D, int k) {
     return (k + 1) * (k + 2) * (k + 3) / 6;
 }
 
+// 2D GlobalIDs (Grid2D.cs:182: ix*nY + iy) coincide with the generator order
 static void cell_ijk(const Problem& P, int j, int* ijk) {
     const int* n = P.g.n;
-    if (P.g.cell_order == BOSSS_CELLS_GENERATOR) {
+    if (P.g.cell_order == BOSSS_CELLS_GENERATOR || P.D == 2) {
         if (P.D == 2) { ijk[0] = j / n[1]; ijk[1] = j % n[1]; ijk[2] = 0; }
         else { ijk[2] = j % n[2]; int r = j / n[2]; ijk[1] = r % n[1]; ijk[0] = r / n[1]; }
     } else {
         ijk[0] = j % n[0];
         int r = j / n[0];
-        if (P.D == 2) { ijk[1] = r; ijk[2] = 0; }
-        else { ijk[1] = r % n[1]; ijk[2] = r / n[1]; }
+        ijk[1] = r % n[1];
+        ijk[2] = r / n[1];
     }
 }
 
 static int cell_index(const Problem& P, const int* ijk) {
     const int* n = P.g.n;
-    if (P.g.cell_order == BOSSS_CELLS_GENERATOR) {
+    if (P.g.cell_order == BOSSS_CELLS_GENERATOR || P.D == 2) {
         if (P.D == 2) return ijk[0] * n[1] + ijk[1];
         return (ijk[0] * n[1] + ijk[1]) * n[2] + ijk[2];
     }
-    if (P.D == 2) return ijk[0] + ijk[1] * n[0];
     return ijk[0] + n[0] * (ijk[1] + n[1] * ijk[2]);
 }
 
