@@ -130,6 +130,46 @@ static void block_pattern(const GridConst& g, std::vector<int64_t>& rowptr, std:
 
 static int grid_of(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 16); }
 
+// A += sigma I on the self blocks (the first block of every row, block_pattern); blocks
+// column-major, so entry (r, r) of block b sits at b*nb*nb + r*(nb+1)
+__global__ void k_shift_diag(long long nbr, int nb, const long long* __restrict__ rowptr, double* __restrict__ vals,
+                             double sigma) {
+    const long long n = nbr * nb;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long i = t / nb;
+        const int r = (int)(t - i * nb);
+        vals[rowptr[i] * (long long)nb * nb + (long long)r * (nb + 1)] += sigma;
+    }
+}
+
+// out = A^T for a structurally symmetric block pattern (the face-neighbour pattern of
+// block_pattern): block (j, i) of the result is block (i, j) of A transposed. One warp per
+// block row; a missing mirror block sets *bad
+__global__ void k_transpose_sym(long long nbr, int nb, const long long* __restrict__ rowptr,
+                                const int* __restrict__ colidx, const double* __restrict__ vals,
+                                double* __restrict__ out, int* bad) {
+    const int lane = threadIdx.x & 31;
+    const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long bs = (long long)nb * nb;
+    for (long long i = w0; i < nbr; i += nw) {
+        for (long long b = rowptr[i]; b < rowptr[i + 1]; ++b) {
+            const int j = colidx[b];
+            long long q = -1;
+            for (long long c = rowptr[j]; c < rowptr[j + 1]; ++c)
+                if (colidx[c] == (int)i) q = c;
+            if (q < 0) {
+                if (lane == 0) atomicExch(bad, 1);
+                continue;
+            }
+            for (long long e = lane; e < bs; e += 32) {
+                const long long c = e / nb, r = e - c * nb;   // entry (r, c) of the result block
+                out[q * bs + e] = vals[b * bs + r * nb + c];
+            }
+        }
+    }
+}
+
 // assemble J(U_dev) into a new bosss_bsr (values on the device)
 static int assemble(bosss_handle* h, const double* U_dev, double time, bosss_bsr** out) {
     const GridConst& g = h->base.g;
@@ -629,7 +669,11 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
     }
     bosss_solver_opts o;
     fill_defaults(opt, o, 1e-10, 30);
-    if (o.precond != 0 && o.precond != 1) return fail(BOSSS_ERR_BAD_ARG, "batch solve: preconditioner 0 or 1");
+    if (o.precond < 0 || o.precond > 2) return fail(BOSSS_ERR_BAD_ARG, "batch solve: preconditioner 0, 1 or 2");
+    if (o.precond == 2)
+        for (int i = 0; i < B->n; ++i)
+            if (B->h[i]->ndom != (int64_t)B->h[i]->base.g.J * np_of(B->h[i]->D, B->h[i]->K))
+                return fail(BOSSS_ERR_BAD_ARG, "batch solve: the multigrid preconditioner needs scalar operators");
     CUDA_TRY(cudaSetDevice(B->device));
     cudaStream_t s = B->stream;
     long long nmax = 0, bmax = 0;
@@ -639,7 +683,8 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
         nmax = std::max<long long>(nmax, h->ndom);
         bmax = std::max<long long>(bmax, (long long)h->base.g.J * nb * nb);
     }
-    double *r64 = nullptr, *t64 = nullptr, *y64 = nullptr, *u0 = nullptr, *blk = nullptr;
+    double *r64 = nullptr, *t64 = nullptr, *y64 = nullptr, *z64 = nullptr, *u0 = nullptr, *blk = nullptr;
+    bosss_pmg* mg = nullptr;
     float *r32 = nullptr, *c32 = nullptr, *t32 = nullptr, *inv = nullptr;
     long long* rp = nullptr;
     int* sing = nullptr;
@@ -648,6 +693,9 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
         cudaFree(r64);
         cudaFree(t64);
         cudaFree(y64);
+        cudaFree(z64);
+        pmg_destroy(mg);
+        mg = nullptr;
         cudaFree(u0);
         cudaFree(blk);
         cudaFree(r32);
@@ -661,6 +709,7 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
     if (e == cudaSuccess) e = cudaMalloc(&t64, sizeof(double) * nmax);
     if (e == cudaSuccess) e = cudaMalloc(&y64, sizeof(double) * nmax);
     if (e == cudaSuccess && !U_dev) e = cudaMalloc(&u0, sizeof(double) * nmax);
+    if (e == cudaSuccess && o.precond == 2) e = cudaMalloc(&z64, sizeof(double) * nmax);
     if (e == cudaSuccess) e = cudaMalloc(&r32, sizeof(float) * nmax);
     if (e == cudaSuccess) e = cudaMalloc(&c32, sizeof(float) * nmax);
     if (e == cudaSuccess) e = cudaMalloc(&t32, sizeof(float) * nmax);
@@ -727,6 +776,46 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
                 break;
             }
         }
+        // multigrid: V-cycle on the assembled I/dt + J (transpose: its transpose)
+        pmg_destroy(mg);
+        mg = nullptr;
+        if (o.precond == 2) {
+            if (!cu(cudaStreamSynchronize(s), "synchronize")) break;
+            bosss_bsr* A = nullptr;
+            rc = assemble(h, U, 0.0, &A);
+            if (rc) break;
+            const long long bsz = (long long)nb * nb;
+            k_shift_diag<<<grid_of((long long)g.J * nb), 256, 0, s>>>(g.J, nb, (const long long*)A->d_rowptr,
+                                                                      A->d_vals, idt);
+            bool ok = cu(cudaGetLastError(), "diagonal shift");
+            if (ok && transpose) {
+                double* tv = nullptr;
+                ok = cu(cudaMalloc(&tv, sizeof(double) * bsz * A->nnzb), "transpose alloc") &&
+                     cu(cudaMemsetAsync(sing, 0, sizeof(int), s), "memset");
+                if (ok) {
+                    k_transpose_sym<<<grid_of((long long)g.J * 32), 256, 0, s>>>(
+                        g.J, nb, (const long long*)A->d_rowptr, A->d_colidx, A->d_vals, tv, sing);
+                    int flag = 0;
+                    ok = cu(cudaGetLastError(), "transpose") &&
+                         cu(cudaMemcpyAsync(&flag, sing, sizeof(int), cudaMemcpyDeviceToHost, s), "copy") &&
+                         cu(cudaStreamSynchronize(s), "synchronize");
+                    if (ok && flag) {
+                        rc = fail(BOSSS_ERR_BAD_ARG, "batch solve: block pattern is not symmetric");
+                        ok = false;
+                    }
+                }
+                if (ok) {
+                    cudaFree(A->d_vals);
+                    A->d_vals = tv;
+                } else {
+                    cudaFree(tv);
+                }
+            }
+            if (ok) ok = cu(cudaStreamSynchronize(s), "synchronize");
+            if (ok) rc = pmg_create(h, A, &mg);
+            bosss_b200_bsr_destroy(A);
+            if (!ok || rc) break;
+        }
         const double bnorm = norm2(bi, n, kw.partials, s);
         for (int it = 0; it <= o.max_outer; ++it) {
             // r = b - (I/dt + J) x in FP64
@@ -752,6 +841,17 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
             int inner_rc = 0;
             auto apply = [&](const float* v, float* y) -> cudaError_t {
                 const float* vin = v;
+                if (mg) {
+                    k_convert<float, double><<<grid_of(n), 256, 0, s>>>(n, v, t64);
+                    int r2 = pmg_apply(mg, t64, z64, s);
+                    if (!r2) r2 = op64(z64, y64);
+                    if (r2) {
+                        inner_rc = r2;
+                        return cudaErrorUnknown;
+                    }
+                    k_convert<double, float><<<grid_of(n), 256, 0, s>>>(n, y64, y);
+                    return cudaGetLastError();
+                }
                 if (inv) {
                     k_apply_blockdiag<float><<<grid_of(n), 256, 0, s>>>(g.J, nb, inv, v, t32);
                     vin = t32;
@@ -782,7 +882,13 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
                 corr = t32;
             }
             k_convert<float, double><<<grid_of(n), 256, 0, s>>>(n, corr, t64);
-            k_axpby<double><<<grid_of(n), 256, 0, s>>>(n, 1.0, t64, 1.0, xi);
+            if (mg) {
+                rc = pmg_apply(mg, t64, z64, s);
+                if (rc) break;
+                k_axpby<double><<<grid_of(n), 256, 0, s>>>(n, 1.0, z64, 1.0, xi);
+            } else {
+                k_axpby<double><<<grid_of(n), 256, 0, s>>>(n, 1.0, t64, 1.0, xi);
+            }
             if (!cu(cudaGetLastError(), "update")) break;
         }
         if (reports) reports[i] = r;

@@ -287,8 +287,8 @@ typedef struct bosss_solver_opts {
     int32_t restart;        /* GMRES restart length m (<= 200) */
     int32_t max_krylov;     /* GMRES iterations per outer step */
     int32_t precond;        /* 0 = none, 1 = block-Jacobi on the cell blocks of the Jacobian,
-                               2 = multigrid V-cycle (bosss_b200_pmg_create; newton_solve with
-                               scalar operators only) */
+                               2 = multigrid V-cycle (bosss_b200_pmg_create; newton_solve and
+                               batch_solve with scalar operators only) */
     double inner_rtol;      /* relative tolerance of each inner (Krylov) solve */
     int32_t precond_update; /* newton_solve: rebuild the preconditioner (Jacobian assembly +
                                setup) every this many Newton steps, the reference's
@@ -386,7 +386,9 @@ int bosss_b200_batch_tiles(const bosss_batch* b, int32_t K, int32_t Q, int32_t* 
  * ||b_i - A_i x_i|| <= max(rtol ||b_i||, atol) (defaults: rtol 1e-10, 30 refinement steps,
  * inner tolerance 1e-3; SoftGMRES.cs on a BlockMsrMatrix in the reference, here
  * matrix-free); precond 1 (default): block-Jacobi on the diagonal cell blocks of
- * I/dt + J_i, probed with a face-neighbour colouring; 0: none. Device vectors (concatenated
+ * I/dt + J_i, probed with a face-neighbour colouring; 2: one multigrid V-cycle
+ * (bosss_b200_pmg_create) on the assembled I/dt + J_i, or its transpose for the adjoint
+ * systems (scalar operators); 0: none. Device vectors (concatenated
  * instance vectors, bosss_b200_batch_get_sizes offsets): U the state of the linearisation
  * (NULL: zero; the Jacobian of the linear advection-diffusion family does not depend on it),
  * b the right-hand sides, x the initial guesses in and the solutions out. reports: NULL or

@@ -31,7 +31,7 @@ def _dt(probs):
     return np.array([(1.0 / p.grid.n[0]) / np.linalg.norm(p.config["velocity"]) for p in probs])
 
 
-@pytest.mark.parametrize("precond", [1, 0], ids=["block_jacobi", "none"])
+@pytest.mark.parametrize("precond", [1, 0, 2], ids=["block_jacobi", "none", "multigrid"])
 def test_batch_solve_forward_and_adjoint(precond):
     import torch
     probs = _batch()
@@ -70,7 +70,7 @@ def test_batch_solve_rejects_bad_arguments():
     n = sum(p.n_dofs for p in probs)
     with O.BatchEvaluator(probs) as B:
         bt = torch.ones(n, dtype=torch.float64, device="cuda")
-        for dt, kw in ((-1.0, {}), (0.1, {"precond": 2})):
+        for dt, kw in ((-1.0, {}), (0.1, {"precond": 3})):
             with pytest.raises(C.BosssError) as ei:
                 B.solve(dt, bt, **kw)
             assert ei.value.code == C.ERR_BAD_ARG
