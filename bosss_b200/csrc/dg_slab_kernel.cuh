@@ -95,7 +95,7 @@ struct SlabCfg {
     static constexpr int MINB_VJP = K <= 1 ? 5 : (K <= 3 ? 4 : 3);
 #endif
     static constexpr int CPB_THR = ((MODE == MODE_VJP) ? BOSSS_SLAB_THREADS_VJP : BOSSS_SLAB_THREADS) / TPC;
-    static constexpr int MINB = (MODE == MODE_VJP) ? MINB_VJP : MINB_FWD;
+    static constexpr int MINB_REQ = (MODE == MODE_VJP) ? MINB_VJP : MINB_FWD;
     static constexpr int CPB_MAX = (CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR) < 1 ? 1
                                    : (CPB_SMEM < CPB_THR ? CPB_SMEM : CPB_THR);
     static constexpr int CPB = CPB_MAX;
@@ -104,6 +104,11 @@ struct SlabCfg {
     static constexpr int HALFP = (SPLIT > 1) ? (HALF + 31) / 32 * 32 : HALF;
     static constexpr int NT = SPLIT * HALFP;
     static constexpr size_t SMEM_BYTES = (size_t)CPB * S_CELL * 8;
+    // resident blocks the shared memory admits (228 KB per SM, 1 KB reserved per block): asking
+    // the register allocator for more than these only forces spills (the scalar family's tiles
+    // are shared-memory bound at 2 blocks: k=4 VJP 168 registers with spills under a 3-block cap)
+    static constexpr int BLK_SMEM = (int)(233472 / (SMEM_BYTES + 1024)) < 1 ? 1 : (int)(233472 / (SMEM_BYTES + 1024));
+    static constexpr int MINB = MINB_REQ < BLK_SMEM ? MINB_REQ : BLK_SMEM;
     // offset of field f's first comp block
     __host__ __device__ static constexpr int vnode(int f) { return f < NV ? f * NCI0 * FV : (NV * NCI0 + (f - NV) * NCI1V) * FV; }
     __host__ __device__ static constexpr int fnode(int f) { return f < NV ? f * NCI0 * FF : (NV * NCI0 + (f - NV) * NCI1F) * FF; }
