@@ -21,6 +21,13 @@
 
 namespace bosss {
 
+// Row strides of the node blocks in shared memory: odd, so that the threads of a warp (one
+// slab row each, cells S_CELL apart) spread their 8-byte accesses over all bank pairs; with
+// Q odd the unpadded Q^2 / Q are odd already (an even stride left half the banks unused:
+// 5.7 wavefronts per store in the k = 4 scalar VJP)
+__host__ __device__ constexpr int slab_slv(int Q) { return (Q * Q) | 1; }
+__host__ __device__ constexpr int slab_slf(int Q) { return Q | 1; }
+
 // PASS: 0 = volume and face terms (runtime flags may skip either), 1 = volume terms only
 // (compiled without the face passes: the volume pass of the face-once path)
 template <class Phys, int K, int Q, int MODE, int PASS = 0>
@@ -41,9 +48,9 @@ struct SlabCfg {
     static constexpr int NCI1F = G_SECOND_FACE ? 4 : 1;
     static constexpr int NCOV = (VOL_OV ? 1 : 0) + (VOL_OG ? 3 : 0);
     static constexpr int NCOF = (FACE_OV ? 1 : 0) + (FACE_OG ? 3 : 0);
-    static constexpr int SLV = Q * Q + 1;          // padded volume slab
+    static constexpr int SLV = slab_slv(Q);        // padded volume slab
     static constexpr int FV = Q * SLV;             // one (field, comp) volume block
-    static constexpr int SLF = Q + 1;              // padded face row
+    static constexpr int SLF = slab_slf(Q);        // padded face row
     static constexpr int FF = Q * SLF;             // one (field, comp) face block
     // work split of a slab over SPLIT warp-uniform parts: volume rows qy = part mod SPLIT,
     // faces: part s handles the lower (s=0) / upper (s=1) face. Measured on B200 (Euler
@@ -70,7 +77,9 @@ struct SlabCfg {
     static constexpr int S_RED = NO * SPLIT * Q * NP;
     static constexpr int S_W0 = (PASS == 1 || S_VOL > S_FACE) ? S_VOL : S_FACE;
     static constexpr int S_WORK = S_W0 > S_RED ? S_W0 : S_RED;
-    static constexpr int S_CELL = S_CIN + S_WORK;
+    // one field (the scalar family): the per-cell stride is odd as well (the threads of a warp
+    // span several cells); the multi-field tiles keep their measured layout
+    static constexpr int S_CELL = (NV == 1) ? ((S_CIN + S_WORK) | 1) : S_CIN + S_WORK;
     static constexpr int BUDGET = 110 * 1024 / 8;
     static constexpr int CPB_SMEM = BUDGET / S_CELL;
     // threads per block target and minimum resident blocks per SM (register budget):
@@ -350,7 +359,7 @@ template <int K, int Q, bool GRAD, int PART, int SPLIT>
 __device__ __forceinline__ void slab_interp(const Tables1D& T, const double* cf, const double* Az, const double* dAz,
                                             int q, double scaling, const double* twoh, double* nb) {
     constexpr int NPAIR = (K + 1) * (K + 2) / 2;
-    constexpr int SLV = Q * Q + 1, FV = Q * SLV;
+    constexpr int SLV = slab_slv(Q), FV = Q * SLV;
     double T1[NPAIR], T1z[NPAIR];
 #pragma unroll
     for (int a = 0; a <= K; ++a)
@@ -413,7 +422,7 @@ template <int K, int Q, bool OV, bool OG, int PART, int SPLIT, int CS>
 __device__ __forceinline__ void slab_project(const Tables1D& T, const double* ob, const double* Az, const double* dAz,
                                              int q, double* R) {
     constexpr int NPAIR = (K + 1) * (K + 2) / 2;
-    constexpr int SLV = Q * Q + 1, FV = Q * SLV;
+    constexpr int SLV = slab_slv(Q), FV = Q * SLV;
     constexpr int G0 = OV ? 1 : 0;
     double P2[NPAIR], P2z[NPAIR];
 #pragma unroll
@@ -460,7 +469,7 @@ template <int DIR, int K, int Q, bool GRAD>
 __device__ __forceinline__ void face_interp(const Tables1D& T, const double* cf, int fs, const double* A2,
                                             const double* dA2, double scaling, const double* twoh, double* tb) {
     constexpr int t1 = FaceDirs<DIR>::t1, t2 = FaceDirs<DIR>::t2;
-    constexpr int SLF = Q + 1, FF = Q * SLF;
+    constexpr int SLF = slab_slf(Q), FF = Q * SLF;
     double Tv[K + 1], Tn[K + 1], Tt2[K + 1];
 #pragma unroll
     for (int p = 0; p <= K; ++p) {
@@ -509,7 +518,7 @@ template <int DIR, int K, int Q, bool OV, bool OG>
 __device__ __forceinline__ void face_project(const Tables1D& T, const double* ob, int fs, const double* A2,
                                              const double* dA2, double* R) {
     constexpr int t1 = FaceDirs<DIR>::t1, t2 = FaceDirs<DIR>::t2;
-    constexpr int SLF = Q + 1, FF = Q * SLF;
+    constexpr int SLF = slab_slf(Q), FF = Q * SLF;
     constexpr int G0 = OV ? 1 : 0;
     double P[K + 1], Pn[K + 1], Pt2[K + 1];
 #pragma unroll
