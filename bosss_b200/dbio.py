@@ -462,7 +462,9 @@ def LoadFieldData(db, id, fields, stored_fields, part=None, device=None):
     gids, i0 = _local_cells(grid, part)
     J = len(gids)
     items = db.LoadVector(id, (i0, J))
-    # resort by GlobalID: the loaded slice may hold other ranks' cells
+    # resort by GlobalID: the loaded slice may hold other ranks' cells, so every rank's slice
+    # is gathered on every rank (host memory of the whole vector per rank; the reference
+    # exchanges only the permuted items)
     pairs = [(it.GlobalID, it.DGData) for it in items]
     everything = _allgather(pairs, db.group)
     where = {int(g): j for j, g in enumerate(gids)}

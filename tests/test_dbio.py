@@ -234,3 +234,13 @@ def test_several_ranks_save_and_load_over_gloo(tmp_path):
     # three ranks read the vector two ranks wrote (slices cross the stored parts)
     out3 = _spawn(3, str(tmp_path), vid)
     assert all(ok for _, _, ok in out3)
+
+
+def test_2d_round_trip(tmp_path):
+    g = O.Cartesian2DGrid(np.linspace(0, 1, 5), np.linspace(0, 1, 4))
+    fs = [O.DGField(g, 3, "T")]
+    x = np.random.default_rng(6).standard_normal(g.NoOfCells * fs[0].Np)
+    vid = dbio.SaveFieldData(tmp_path, fs, x)
+    items = dbio.DatabaseDriver(tmp_path).LoadVector(vid)
+    assert [it.GlobalID for it in items] == list(range(g.NoOfCells))   # ix*nY + iy
+    assert np.array_equal(dbio.LoadFieldData(tmp_path, vid, fs, ["T"]), x)
