@@ -14,9 +14,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <numeric>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "batch.h"
@@ -129,6 +133,9 @@ static void block_pattern(const GridConst& g, std::vector<int64_t>& rowptr, std:
 }
 
 static int grid_of(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 16); }
+
+// host threads of bosss_b200_batch_solve (one stream and one set of work arrays each)
+static constexpr int BATCH_SOLVE_THREADS = 4;
 
 // A += sigma I on the self blocks (the first block of every row, block_pattern); blocks
 // column-major, so entry (r, r) of block b sits at b*nb*nb + r*(nb+1)
@@ -675,7 +682,20 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
             if (B->h[i]->ndom != (int64_t)B->h[i]->base.g.J * np_of(B->h[i]->D, B->h[i]->K))
                 return fail(BOSSS_ERR_BAD_ARG, "batch solve: the multigrid preconditioner needs scalar operators");
     CUDA_TRY(cudaSetDevice(B->device));
-    cudaStream_t s = B->stream;
+    // instances largest first, taken by a few host threads with their own streams and work
+    // arrays, so that the launch-bound solves of the small instances overlap the large ones
+    std::vector<int> order(B->n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return B->h[a]->ndom > B->h[b]->ndom; });
+    std::atomic<int> next{0};
+    std::atomic<bool> abort_all{false};
+    const int nworkers = std::max(1, std::min(B->n, BATCH_SOLVE_THREADS));
+    std::vector<int> wrc(nworkers, 0);
+    std::vector<std::string> wmsg(nworkers);
+    auto worker = [&]() -> int {
+    CUDA_TRY(cudaSetDevice(B->device));
+    cudaStream_t s = nullptr;
+    CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     long long nmax = 0, bmax = 0;
     for (int i = 0; i < B->n; ++i) {
         const bosss_handle* h = B->h[i];
@@ -704,6 +724,7 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
         cudaFree(inv);
         cudaFree(rp);
         cudaFree(sing);
+        cudaStreamDestroy(s);
     };
     cudaError_t e = cudaMalloc(&r64, sizeof(double) * nmax);
     if (e == cudaSuccess) e = cudaMalloc(&t64, sizeof(double) * nmax);
@@ -730,7 +751,8 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
         return rc == 0;
     };
     const int mode = transpose ? MODE_VJP : MODE_JVP;
-    for (int i = 0; i < B->n && !rc; ++i) {
+    for (int it = next++; it < B->n && !rc && !abort_all; it = next++) {
+        const int i = order[it];
         bosss_handle* h = B->h[i];
         const GridConst& g = h->base.g;
         const long long n = h->ndom, off = B->dom_off[i];
@@ -899,6 +921,25 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
     }
     cleanup();
     return rc;
+    };
+    // errors are thread-local: each worker keeps its message for the calling thread
+    auto run_worker = [&](int wid) {
+        const int r = worker();
+        if (r) {
+            char buf[512];
+            bosss_b200_last_error(buf, sizeof(buf));
+            wrc[wid] = r;
+            wmsg[wid] = buf;
+            abort_all = true;
+        }
+    };
+    std::vector<std::thread> threads;
+    for (int w = 1; w < nworkers; ++w) threads.emplace_back(run_worker, w);
+    run_worker(0);
+    for (auto& t : threads) t.join();
+    for (int w = 0; w < nworkers; ++w)
+        if (wrc[w]) return fail(wrc[w], wmsg[w]);
+    return BOSSS_OK;
 }
 
 }  // extern "C"

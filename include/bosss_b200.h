@@ -392,7 +392,8 @@ int bosss_b200_batch_tiles(const bosss_batch* b, int32_t K, int32_t Q, int32_t* 
  * instance vectors, bosss_b200_batch_get_sizes offsets): U the state of the linearisation
  * (NULL: zero; the Jacobian of the linear advection-diffusion family does not depend on it),
  * b the right-hand sides, x the initial guesses in and the solutions out. reports: NULL or
- * n entries. Returns after the solves have completed. */
+ * n entries. The instances are solved largest first by 4 host threads, each on its own
+ * stream with its own work arrays. Returns after the solves have completed. */
 int bosss_b200_batch_solve(bosss_batch* b, int32_t transpose, const double* dt, const double* U_dev,
                            const double* b_dev, double* x_dev, const bosss_solver_opts* opt,
                            bosss_solver_report* reports);
