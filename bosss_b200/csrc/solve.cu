@@ -317,12 +317,14 @@ struct KrylovWork {
     T* z = nullptr;
     double* partials = nullptr;
     double* hbuf = nullptr;
+    double* pinned = nullptr;   // host slots of the lagged residual checks
     ~KrylovWork() {
         cudaFree(V);
         cudaFree(w);
         cudaFree(z);
         cudaFree(partials);
         cudaFree(hbuf);
+        if (pinned) cudaFreeHost(pinned);
     }
     cudaError_t alloc(long long n, int m) {
         cudaError_t e = cudaMalloc(&V, sizeof(T) * (size_t)(m + 1) * n);
@@ -330,6 +332,7 @@ struct KrylovWork {
         if (e == cudaSuccess) e = cudaMalloc(&z, sizeof(T) * n);
         if (e == cudaSuccess) e = cudaMalloc(&partials, sizeof(double) * RED_BLOCKS * (m + 1));
         if (e == cudaSuccess) e = cudaMalloc(&hbuf, sizeof(double) * gmres_dev_doubles(m));
+        if (e == cudaSuccess) e = cudaMallocHost(&pinned, sizeof(double) * 8);
         return e;
     }
 };
@@ -507,7 +510,7 @@ int bosss_b200_newton_solve(bosss_handle* h, double* U, double time, const bosss
             return rr ? cudaErrorUnknown : cudaGetLastError();
         };
         GmresResult g = gmres<double>(n, apply, dW, dX, o.restart, o.max_krylov, o.inner_rtol, 0.0, kw.V, kw.w,
-                                      kw.partials, kw.hbuf, s);
+                                      kw.partials, kw.hbuf, s, kw.pinned);
         r.krylov_iters += g.iters;
         if (inner_rc) {
             rc = inner_rc;
@@ -638,7 +641,7 @@ int bosss_b200_bsr_solve(bosss_bsr* A, const double* b, double* x, const bosss_s
             return cudaGetLastError();
         };
         GmresResult g = gmres<float>(n, apply, rf, cf, o.restart, o.max_krylov, o.inner_rtol, 0.0, kw.V, kw.w,
-                                     kw.partials, kw.hbuf, s);
+                                     kw.partials, kw.hbuf, s, kw.pinned);
         r.krylov_iters += g.iters;
         if (g.error) {
             rc = fail(BOSSS_ERR_CUDA, "GMRES: " + std::string(cudaGetErrorString((cudaError_t)g.error)));
@@ -888,7 +891,7 @@ int bosss_b200_batch_solve(bosss_batch* B, int32_t transpose, const double* dt, 
                 return cudaGetLastError();
             };
             GmresResult gr = gmres<float>(n, apply, r32, c32, o.restart, o.max_krylov, o.inner_rtol, 0.0, kw.V, kw.w,
-                                          kw.partials, kw.hbuf, s);
+                                          kw.partials, kw.hbuf, s, kw.pinned);
             r.krylov_iters += gr.iters;
             if (inner_rc) {
                 rc = inner_rc;

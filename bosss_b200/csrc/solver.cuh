@@ -275,7 +275,7 @@ struct GmresResult {
 template <class T>
 GmresResult gmres(long long n, const std::function<cudaError_t(const T*, T*)>& apply, const T* b, T* x, int m,
                   int max_iters, double rtol, double atol, T* V, T* w, double* partials, double* work,
-                  cudaStream_t s) {
+                  cudaStream_t s, double* pinned = nullptr) {
     GmresResult R;
     if (m > 254) m = 254;
     auto grid = [&]() { return (int)std::min<long long>((n + 255) / 256, 148LL * 8); };
@@ -296,15 +296,16 @@ GmresResult gmres(long long n, const std::function<cudaError_t(const T*, T*)>& a
         k_finish_partials<<<1, 256, 0, s>>>(partials, dv.sc);
         chk(cudaGetLastError());
     };
-    // pinned host slots for the lagged residual checks
-    double* hres = nullptr;
+    // pinned host slots for the lagged residual checks: the caller's (8 doubles, kept across
+    // calls: freeing pinned memory synchronises the device), else allocated here
+    double* hres = pinned;
     cudaEvent_t ev[2] = {nullptr, nullptr};
-    chk(cudaMallocHost(&hres, sizeof(double) * 8));
+    if (!hres) chk(cudaMallocHost(&hres, sizeof(double) * 8));
     for (int i = 0; i < 2; ++i) chk(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
     auto cleanup = [&]() {
         for (int i = 0; i < 2; ++i)
             if (ev[i]) cudaEventDestroy(ev[i]);
-        if (hres) cudaFreeHost(hres);
+        if (hres && !pinned) cudaFreeHost(hres);
     };
     if (R.error) {
         cleanup();
